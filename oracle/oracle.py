@@ -1,0 +1,254 @@
+"""ctypes front-end of the checkers — TEST INFRASTRUCTURE ONLY.
+
+`Oracle` wraps oracle/liboracle.so, the project's CPU restatement of the
+reference's reconstruction path (FP32 in the reference's operation order, and
+FP64).  `RefHost` wraps oracle/_ref/libxrref.so, the reference's own
+reconstruct/src/ir.cu compiled for the host through oracle/ref_shim.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module, and only to check or to time the reference; the product never
+does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_F = ctypes.POINTER(ctypes.c_float)
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def build(ref: bool = False) -> None:
+    """Build liboracle.so (and, with ref=True, the reference host build)."""
+    targets = ["all"] + (["ref"] if ref else [])
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+@dataclass
+class Scan:
+    """A scan description: the reference's Geometry plus its per-axis globals
+    (elemR, elemT, INIT_OFFSET) and the scattering basis (params.cu:14-40)."""
+    sdd: float
+    sod: float
+    det: float
+    N: int
+    Nd: int
+    V: int
+    rot: np.ndarray            # (C, 9)
+    trans: np.ndarray          # (C, 3)
+    offset: np.ndarray         # (C, 3)
+    basis: np.ndarray          # (K, 3)
+    _keep: list = field(default_factory=list, repr=False)
+
+    def __post_init__(self):
+        self.rot = np.ascontiguousarray(np.asarray(self.rot, np.float32).reshape(-1, 9))
+        self.trans = np.ascontiguousarray(np.asarray(self.trans, np.float32).reshape(-1, 3))
+        self.offset = np.ascontiguousarray(np.asarray(self.offset, np.float32).reshape(-1, 3))
+        self.basis = np.ascontiguousarray(np.asarray(self.basis, np.float32).reshape(-1, 3))
+
+    @property
+    def C(self) -> int:
+        return self.rot.shape[0]
+
+    @property
+    def K(self) -> int:
+        return self.basis.shape[0]
+
+    @property
+    def vs(self) -> float:
+        return float(np.float32(np.float32(self.sod) * np.float32(self.det)) / np.float32(self.sdd))
+
+
+class _OrScan(ctypes.Structure):
+    _fields_ = [("sdd", ctypes.c_float), ("sod", ctypes.c_float), ("det", ctypes.c_float),
+                ("N", ctypes.c_int), ("Nd", ctypes.c_int), ("V", ctypes.c_int),
+                ("C", ctypes.c_int), ("K", ctypes.c_int),
+                ("rot", _F), ("trans", _F), ("offset", _F), ("basis", _F)]
+
+
+def _p(a: np.ndarray, dt=np.float32):
+    assert a.dtype == dt and a.flags.c_contiguous
+    return a.ctypes.data_as(_F if dt == np.float32 else _D)
+
+
+def _ptr_array(arrs, dt):
+    t = _F if dt == np.float32 else _D
+    return (t * len(arrs))(*[a.ctypes.data_as(t) for a in arrs])
+
+
+class Oracle:
+    """The project's CPU restatement (liboracle.so)."""
+
+    def __init__(self):
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        self.lib = ctypes.CDLL(path)
+
+    def _scan(self, s: Scan) -> _OrScan:
+        return _OrScan(s.sdd, s.sod, s.det, s.N, s.Nd, s.V, s.C, s.K,
+                       _p(s.rot), _p(s.trans), _p(s.offset), _p(s.basis))
+
+    def _fn(self, name, dt):
+        return getattr(self.lib, ("or32_" if dt == np.float32 else "or64_") + name)
+
+    def forward_view(self, s, cond, n, vol, proj, factor, xtt, dt=np.float32):
+        self._fn("forward_view", dt)(ctypes.byref(self._scan(s)), cond, n, _p(vol, dt), _p(proj, dt),
+                                     _p(factor, dt), int(xtt))
+
+    def correlation(self, s, cond, n, proj, factor, dt=np.float32):
+        self._fn("correlation", dt)(ctypes.byref(self._scan(s)), cond, n, _p(proj, dt), _p(factor, dt))
+
+    def ratio(self, s, n, proj, sino, art, dt=np.float32):
+        acc = np.zeros(1, dt)
+        self._fn("ratio", dt)(ctypes.byref(self._scan(s)), n, _p(proj, dt), _p(sino, dt), int(art), _p(acc, dt))
+        return float(acc[0])
+
+    def backward_slab(self, s, cond, y, n, proj, tmp, factor, xtt, dt=np.float32):
+        self._fn("backward_slab", dt)(ctypes.byref(self._scan(s)), cond, y, n, _p(proj, dt), _p(tmp, dt),
+                                      _p(factor, dt), int(xtt))
+
+    def forward_all(self, s, vol, rotate_ccw=0, xtt=False, dt=np.float32):
+        vol = np.ascontiguousarray(vol, dt)
+        proj = np.zeros(s.C * s.V * s.Nd * s.Nd, dt)
+        self._fn("forward_all", dt)(ctypes.byref(self._scan(s)), _p(vol, dt), _p(proj, dt), int(rotate_ccw),
+                                    int(xtt))
+        return proj.reshape(s.C, s.V, s.Nd, s.Nd)
+
+    def subset_orders(self, batch, rows, fresh_engine_each_row):
+        out = np.zeros(rows * batch, np.int32)
+        self.lib.or_subset_orders(batch, rows, int(fresh_engine_each_row), out.ctypes.data_as(_I))
+        return out.reshape(rows, batch)
+
+    def ir_reconstruct(self, s, sino, vol, epoch, batch, rotate_ccw=0, art=False, lam=1e-2, dt=np.float32):
+        """sino: (C, V, Nd, Nd); vol: (C, N, N, N) initial volumes (copied).
+        Returns (volumes, losses[C, epoch])."""
+        sino = [np.ascontiguousarray(x, dt).ravel() for x in sino]
+        vols = [np.ascontiguousarray(x, dt).ravel().copy() for x in vol]
+        orders = self.subset_orders(batch, s.C * epoch, False)
+        losses = np.zeros(s.C * epoch, dt)
+        self._fn("ir_reconstruct", dt)(ctypes.byref(self._scan(s)), _ptr_array(sino, dt), _ptr_array(vols, dt),
+                                       epoch, batch, int(rotate_ccw), int(art),
+                                       (ctypes.c_float if dt == np.float32 else ctypes.c_double)(lam),
+                                       _p(losses, dt), orders.ctypes.data_as(_I))
+        return np.stack(vols).reshape(s.C, s.N, s.N, s.N), losses.reshape(s.C, epoch)
+
+    def xtt_reconstruct(self, s, sino, vol, epoch, batch, rotate_ccw=0, art=False, lam=1e-2, dt=np.float32):
+        """sino: (C, V, Nd, Nd); vol: (K, N, N, N).  Returns (vol after sqrt,
+        last ratio images (C, V, Nd, Nd), losses[epoch])."""
+        sino = np.ascontiguousarray(sino, dt).ravel()
+        vol = np.ascontiguousarray(vol, dt).ravel().copy()
+        proj = np.zeros_like(sino)
+        orders = self.subset_orders(batch, epoch, True)
+        losses = np.zeros(epoch, dt)
+        self._fn("xtt_reconstruct", dt)(ctypes.byref(self._scan(s)), _p(sino, dt), _p(vol, dt), _p(proj, dt),
+                                        epoch, batch, int(rotate_ccw), int(art),
+                                        (ctypes.c_float if dt == np.float32 else ctypes.c_double)(lam),
+                                        _p(losses, dt), orders.ctypes.data_as(_I))
+        return (vol.reshape(s.K, s.N, s.N, s.N), proj.reshape(s.C, s.V, s.Nd, s.Nd), losses)
+
+    def fdk_reconstruct(self, s, sino, rotate_ccw=0, ramlak=False, block0=True, dt=np.float32):
+        sino = np.ascontiguousarray(sino, dt).ravel()
+        vol = np.zeros(s.C * s.N ** 3, dt)
+        filt = np.zeros_like(sino)
+        self._fn("fdk_reconstruct", dt)(ctypes.byref(self._scan(s)), _p(sino, dt), _p(vol, dt), _p(filt, dt),
+                                        int(rotate_ccw), int(ramlak), int(block0))
+        return vol.reshape(s.C, s.N, s.N, s.N), filt.reshape(s.C, s.V, s.Nd, s.Nd)
+
+    def fdk_filter(self, s, ramlak=False, dt=np.float32):
+        f = np.zeros(s.Nd, dt)
+        self._fn("fdk_filter", dt)(ctypes.byref(self._scan(s)), int(ramlak), _p(f, dt))
+        return f
+
+    def fdk_weight(self, s, dt=np.float32):
+        w = np.zeros(s.Nd * s.Nd, dt)
+        self._fn("fdk_weight", dt)(ctypes.byref(self._scan(s)), _p(w, dt))
+        return w.reshape(s.Nd, s.Nd)
+
+    def orientation(self, basis, mu):
+        """mu: (K, ...) float32.  Returns md (3, ...), evalue (3, ...)."""
+        K = mu.shape[0]
+        shp = mu.shape[1:]
+        mu = np.ascontiguousarray(mu, np.float32).reshape(K, -1)
+        nv = mu.shape[1]
+        md = np.zeros((3, nv), np.float32)
+        ev = np.zeros((3, nv), np.float32)
+        b = np.ascontiguousarray(np.asarray(basis, np.float32).ravel())
+        self.lib.or_orientation(ctypes.c_long(nv), K, _p(b), _p(mu), _p(md), _p(ev))
+        return md.reshape((3,) + shp), ev.reshape((3,) + shp)
+
+    def jacobi3(self, A):
+        A = np.ascontiguousarray(A, np.float64).ravel()
+        w = np.zeros(3)
+        V = np.zeros(9)
+        self.lib.or_jacobi3(_p(A, np.float64), _p(w, np.float64), _p(V, np.float64))
+        return w, V.reshape(3, 3)
+
+
+class RefHost:
+    """The reference's own ir.cu kernels compiled for the host (libxrref.so)."""
+
+    def __init__(self, parallel: bool = False):
+        path = os.path.join(HERE, "_ref", "libxrref.so")
+        if not os.path.exists(path):
+            build(ref=True)
+        self.lib = ctypes.CDLL(path)
+        self.lib.xr_ref_ratio.restype = ctypes.c_float
+        self.lib.xr_ref_vox_size.restype = ctypes.c_float
+        self.lib.xr_ref_set_parallel(1 if parallel else 0)
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(os.path.join(HERE, "_ref", "libxrref.so"))
+
+    def setup(self, s: Scan):
+        self.s = s
+        self.lib.xr_ref_setup(ctypes.c_float(s.sdd), ctypes.c_float(s.sod), ctypes.c_float(s.det), s.N, s.Nd,
+                              s.V, s.C, s.K, _p(s.rot), _p(s.trans), _p(s.offset), _p(s.basis))
+
+    def set_parallel(self, on: bool):
+        self.lib.xr_ref_set_parallel(1 if on else 0)
+
+    def forward_view(self, cond, n, vol, proj, factor, xtt):
+        self.lib.xr_ref_forward_view(cond, n, _p(vol), _p(proj), _p(factor), int(xtt))
+
+    def correlation(self, cond, n, proj, factor):
+        self.lib.xr_ref_correlation(cond, n, _p(proj), _p(factor))
+
+    def ratio(self, n, proj, sino, art):
+        return float(self.lib.xr_ref_ratio(n, _p(proj), _p(sino), int(art)))
+
+    def backward_slab(self, cond, y, n, proj, tmp, factor, xtt):
+        self.lib.xr_ref_backward_slab(cond, y, n, _p(proj), _p(tmp), _p(factor), int(xtt))
+
+    def forward_all(self, vol, rotate_ccw=0, xtt=False):
+        s = self.s
+        vol = np.ascontiguousarray(vol, np.float32).ravel().copy()
+        proj = np.zeros(s.C * s.V * s.Nd * s.Nd, np.float32)
+        self.lib.xr_ref_forward_all(_p(vol), _p(proj), int(rotate_ccw), int(xtt))
+        return proj.reshape(s.C, s.V, s.Nd, s.Nd)
+
+    def ir_reconstruct(self, sino, vol, epoch, batch, rotate_ccw=0, art=False, lam=1e-2):
+        s = self.s
+        sino = [np.ascontiguousarray(x, np.float32).ravel().copy() for x in sino]
+        vols = [np.ascontiguousarray(x, np.float32).ravel().copy() for x in vol]
+        losses = np.zeros(epoch, np.float32)
+        self.lib.xr_ref_ir_reconstruct(_ptr_array(sino, np.float32), _ptr_array(vols, np.float32), epoch, batch,
+                                       int(rotate_ccw), int(art), ctypes.c_float(lam), _p(losses))
+        return np.stack(vols).reshape(s.C, s.N, s.N, s.N), losses
+
+    def xtt_reconstruct(self, sino, vol, epoch, batch, rotate_ccw=0, art=False, lam=1e-2):
+        s = self.s
+        sino = [np.ascontiguousarray(x, np.float32).ravel().copy() for x in sino]
+        vols = [np.ascontiguousarray(x, np.float32).ravel().copy() for x in vol]
+        losses = np.zeros(epoch, np.float32)
+        self.lib.xr_ref_xtt_reconstruct(_ptr_array(sino, np.float32), _ptr_array(vols, np.float32), epoch, batch,
+                                        int(rotate_ccw), int(art), ctypes.c_float(lam), _p(losses))
+        return (np.stack(vols).reshape(s.K, s.N, s.N, s.N), np.stack(sino).reshape(s.C, s.V, s.Nd, s.Nd),
+                losses)

@@ -1,0 +1,535 @@
+/*
+ * CPU restatement of the reference's reconstruction hot path — TEST
+ * INFRASTRUCTURE ONLY (the oracle).  Only tests/, __graft_entry__.smoke() and
+ * bench.py's CPU-baseline leg may load it, and only as the checker.
+ *
+ * This file is included twice by xr_oracle.c: once with real = float (the
+ * reference's FP32 arithmetic, operation by operation, so that per-voxel
+ * detector coordinates and weights are bit-identical to the reference compiled
+ * for the host) and once with real = double (the FP64 oracle used to state the
+ * error of every GPU result).
+ *
+ * Pinned against: oracle/_ref/libxrref.so, the reference's own
+ * reconstruct/src/ir.cu compiled through oracle/ref_shim, via the golden
+ * vectors in tests/golden (tests/golden/make_golden.py).  The FDK part
+ * (reconstruct/src/fdk.cu) cannot be compiled for the host (fdk.cu:330 holds a
+ * kernel launch) and the orientation part needs Eigen, which is absent: those
+ * two are restatements without a reference-run pin.
+ *
+ * Layouts follow the reference: volumes x-fastest (idx = x + N*y + N*N*z,
+ * volume.h:65-71), K channels of N^3 back to back (ir.cu:1788-1790);
+ * projections u-fastest, then v, then view (ir.cu:1518), C blocks of V views.
+ */
+
+#define RV(name) OR_CAT(OR_PFX, name)
+
+typedef struct {
+    real R[9];      /* Rotate = elemR[cond] * Rz(theta)          ir.cu:1865-1872 */
+    real off[3];    /* Rotate * INIT_OFFSET[cond]                ir.cu:1873       */
+    real t[3];      /* elemT[cond]                               ir.cu:1870       */
+    real src[3];    /* Rotate * (0, sod, 0)                      ir.cu:1874,1879  */
+    real eu[3];     /* Rotate * (1, 0, 0)                        ir.cu:1875,1896  */
+    real ev[3];     /* Rotate * (0, 0, 1)                        ir.cu:1876,1897  */
+    real ss;        /* src . src                                 ir.cu:1893       */
+} RV(frame);
+
+/* Matrix3X::operator*(Matrix3X) (vec.h:171-181): w = 0; w += a*b over k. */
+static void RV(mat3mul)(const real *a, const real *b, real *w) {
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            real s = (real)0;
+            for (int k = 0; k < 3; k++) s += a[3 * i + k] * b[3 * k + j];
+            w[3 * i + j] = s;
+        }
+}
+
+/* Matrix3X::operator*(Vector3X) (vec.h:193-201). */
+static void RV(mat3vec)(const real *a, const real *v, real *w) {
+    for (int i = 0; i < 3; i++) {
+        real s = (real)0;
+        for (int j = 0; j < 3; j++) s += a[3 * i + j] * v[j];
+        w[i] = s;
+    }
+}
+
+/* Vector3X::operator*(Vector3X) (vec.h:66-68). */
+static real RV(dot3)(const real *a, const real *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+/* The per-(axis, view) part of rayCasting, ir.cu:1860-1879 (also the head of
+ * correlationProjByLength ir.cu:1541-1553 and FDK's backwardonDevice
+ * fdk.cu:111-130, which differs only in the source sign). */
+void RV(view_frame)(const or_scan *s, int cond, int n, int fdk_frame, RV(frame) * f) {
+    const real theta = (real)2.0 * (real)M_PI * (real)n / (real)s->V;
+    const real c = RCOS(theta), sn = RSIN(theta);
+    const real Rz[9] = {c, -sn, (real)0, sn, c, (real)0, (real)0, (real)0, (real)1};
+    real cR[9], off0[3];
+    for (int i = 0; i < 9; i++) cR[i] = (real)s->rot[9 * cond + i];
+    for (int i = 0; i < 3; i++) {
+        off0[i] = (real)s->offset[3 * cond + i];
+        f->t[i] = (real)s->trans[3 * cond + i];
+    }
+    RV(mat3mul)(cR, Rz, f->R);
+    RV(mat3vec)(f->R, off0, f->off);
+    const real o2s[3] = {(real)0, fdk_frame ? -(real)s->sod : (real)s->sod, (real)0};
+    const real bu[3] = {(real)1, (real)0, (real)0}, bv[3] = {(real)0, (real)0, (real)1};
+    RV(mat3vec)(f->R, o2s, f->src);
+    RV(mat3vec)(f->R, bu, f->eu);
+    RV(mat3vec)(f->R, bv, f->ev);
+    f->ss = RV(dot3)(f->src, f->src);
+}
+
+static real RV(vox_size)(const or_scan *s) { return (real)s->sod * (real)s->det / (real)s->sdd; } /* geometry.h:13 */
+
+/* rayCasting, ir.cu:1852-1902 (per voxel).  fdk_frame selects FDK's centred
+ * voxel grid (fdk.cu:132-135).  Returns u, v, the unit ray B and, through o,
+ * origin2voxel (FDK's magnification weight needs its y). */
+void RV(raycast)(const or_scan *s, const RV(frame) * f, int fdk_frame, int x, int y, int z, real *u,
+                 real *v, real *B, real *o) {
+    const real vs = RV(vox_size)(s);
+    const real N = (real)s->N;
+    const int xyz[3] = {x, y, z};
+    real org[3], d[3], p[3];
+    for (int i = 0; i < 3; i++) {
+        if (fdk_frame)
+            org[i] = ((real)2.0 * (real)xyz[i] - N + (real)1.0) * (real)0.5 * vs - f->off[i] - f->t[i];
+        else
+            org[i] = ((real)2.0 * (real)xyz[i] - N - (real)1.0) * (real)0.5 * vs - f->off[i] - f->t[i];
+    }
+    for (int i = 0; i < 3; i++) d[i] = org[i] - f->src[i];
+    const real coeff = -(f->ss) / RV(dot3)(f->src, d);
+    for (int i = 0; i < 3; i++) p[i] = f->src[i] + coeff * d[i];
+    const real mag = (real)s->sdd / (real)s->sod;
+    *u = RV(dot3)(p, f->eu) * mag / (real)s->det + (real)0.5 * (real)s->Nd;
+    *v = RV(dot3)(p, f->ev) * mag / (real)s->det + (real)0.5 * (real)s->Nd;
+    if (B) { /* Vector3X::normalize(1e-8), vec.h:93-105 */
+        const real val = RSQRT(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        for (int i = 0; i < 3; i++) B[i] = (val > (real)1e-8f) ? d[i] / val : (real)0;
+    }
+    if (o)
+        for (int i = 0; i < 3; i++) o[i] = org[i];
+}
+
+/* Detector window and bilinear taps, e.g. ir.cu:1501-1509. Returns 0 outside. */
+static int RV(taps)(const or_scan *s, real u, real v, long *iu, long *iv, real c[4]) {
+    const real lim = (real)s->Nd - (real)0.55f;
+    if (!((real)0.55f < u && u < lim && (real)0.55f < v && v < lim)) return 0;
+    const real ut = u - (real)0.5, vt = v - (real)0.5;
+    *iu = (long)RFLOOR(ut);
+    *iv = (long)RFLOOR(vt);
+    const real fu = ut - (real)*iu, fv = vt - (real)*iv;
+    c[0] = ((real)1 - fu) * fv;          /* (iu,   iv+1) */
+    c[1] = fu * fv;                      /* (iu+1, iv+1) */
+    c[2] = fu * ((real)1 - fv);          /* (iu+1, iv)   */
+    c[3] = ((real)1 - fu) * ((real)1 - fv); /* (iu, iv)  */
+    return 1;
+}
+
+/* (|B x S_k| * |S_k . G|)^2, ir.cu:1785-1786. */
+static real RV(xtt_weight)(const real *B, const real *S, const real *G) {
+    const real cx = B[1] * S[2] - B[2] * S[1];
+    const real cy = B[2] * S[0] - B[0] * S[2];
+    const real cz = B[0] * S[1] - B[1] * S[0];
+    const real vkm = RSQRT(cx * cx + cy * cy + cz * cz) * RFABS(RV(dot3)(S, G));
+    return vkm * vkm;
+}
+
+/* forwardProj/forwardonDevice (ir.cu:1480-1531, xtt == 0) or
+ * forwardProjXTT/forwardXTTonDevice (ir.cu:133-141,1753-1804, xtt != 0) for
+ * one view over every y slab, in the reference's launch order (y, then z, then
+ * x).  proj is the axis block base (all views); factor is the per-view weight
+ * image, accumulated (the caller zeroes it, reconstruct.cu:88/:866). */
+void RV(forward_view)(const or_scan *s, int cond, int n, const real *vol, real *proj, real *factor,
+                      int xtt) {
+    RV(frame) f;
+    RV(view_frame)(s, cond, n, 0, &f);
+    const long N = s->N, Nd = s->Nd;
+    const long nn = n < 0 ? -n : n;
+    const real vs = RV(vox_size)(s);
+    const real ratio = (vs * vs) / ((real)s->det * ((real)s->sod / (real)s->sdd) * (real)s->det *
+                                    ((real)s->sod / (real)s->sdd));
+    real G[3];
+    { const real bz[3] = {(real)0, (real)0, (real)1}; RV(mat3vec)(f.R, bz, G); }
+    for (long y = 0; y < N; y++)
+        for (long z = 0; z < N; z++)
+            for (long x = 0; x < N; x++) {
+                real u, v, B[3], c[4];
+                long iu, iv;
+                RV(raycast)(s, &f, 0, (int)x, (int)y, (int)z, &u, &v, xtt ? B : 0, 0);
+                if (!RV(taps)(s, u, v, &iu, &iv, c)) continue;
+                const long idx = x + N * y + N * N * z;
+                real val[4];
+                if (!xtt) {
+                    for (int i = 0; i < 4; i++) val[i] = c[i] * ratio * vol[idx];
+                } else {
+                    real pr = (real)0;
+                    for (int k = 0; k < s->K; k++) {
+                        real S[3] = {(real)s->basis[3 * k], (real)s->basis[3 * k + 1], (real)s->basis[3 * k + 2]};
+                        const real w = RV(xtt_weight)(B, S, G);
+                        pr += w * vs * ratio * vol[idx + (long)k * N * N * N];
+                    }
+                    for (int i = 0; i < 4; i++) val[i] = c[i] * pr;
+                }
+                const long base = Nd * Nd * nn;
+                proj[iu + Nd * (iv + 1) + base] += val[0];
+                proj[(iu + 1) + Nd * (iv + 1) + base] += val[1];
+                proj[(iu + 1) + Nd * iv + base] += val[2];
+                proj[iu + Nd * iv + base] += val[3];
+                factor[iu + Nd * (iv + 1)] += c[0];
+                factor[(iu + 1) + Nd * (iv + 1)] += c[1];
+                factor[(iu + 1) + Nd * iv] += c[2];
+                factor[iu + Nd * iv] += c[3];
+            }
+}
+
+/* correlationProjByLength, ir.cu:1533-1603: the chord length L of the ray
+ * through the (shifted) volume box, and proj *= L / (factor + 1e-5).  Only the
+ * first two face hits are stored (the reference's coord[6] overflows past two,
+ * ir.cu:1576-1595).  The reference indexes the view with the signed n
+ * (ir.cu:1601); this restatement uses |n| (identical for clockwise scans). */
+void RV(correlation)(const or_scan *s, int cond, int n, real *proj, const real *factor) {
+    RV(frame) f;
+    RV(view_frame)(s, cond, n, 0, &f);
+    const long N = s->N, Nd = s->Nd;
+    const long nn = n < 0 ? -n : n;
+    const real vs = RV(vox_size)(s);
+    const real src[3] = {(real)0, (real)s->sod, (real)0};
+    real o2s[3];
+    RV(mat3vec)(f.R, src, o2s);
+    real plane[6];
+    for (int a = 0; a < 3; a++) {
+        plane[2 * a] = -((real)(N + 1) / (real)2.0) * vs - f.off[a] - f.t[a];
+        plane[2 * a + 1] = ((real)(N + 1) / (real)2.0) * vs - f.off[a] - f.t[a];
+    }
+    for (long v = 0; v < Nd; v++)
+        for (long u = 0; u < Nd; u++) {
+            const real pix[3] = {((real)u - ((real)Nd - (real)1.0) * (real)0.5) * (real)s->det,
+                                 -((real)s->sdd - (real)s->sod),
+                                 ((real)v - ((real)Nd - (real)1.0) * (real)0.5) * (real)s->det};
+            real o2p[3], s2p[3];
+            RV(mat3vec)(f.R, pix, o2p);
+            for (int i = 0; i < 3; i++) s2p[i] = o2s[i] - o2p[i];
+            int cnt = 0;
+            real coord[6] = {0, 0, 0, 0, 0, 0};
+            for (int p = 0; p < 3; p++)
+                for (int sg = 0; sg < 2; sg++) {
+                    const real tt = (plane[2 * p + sg] - o2s[p]) / s2p[p];
+                    real pl[3];
+                    for (int i = 0; i < 3; i++) pl[i] = tt * s2p[i] + o2s[i];
+                    const int p1 = (p + 1) % 3, p2 = (p + 2) % 3;
+                    if (plane[2 * p1] < pl[p1] && pl[p1] < plane[2 * p1 + 1] && plane[2 * p2] < pl[p2] &&
+                        pl[p2] < plane[2 * p2 + 1]) {
+                        if (cnt < 2)
+                            for (int i = 0; i < 3; i++) coord[i + 3 * cnt] = pl[i];
+                        cnt++;
+                    }
+                }
+            const real L = RSQRT((coord[0] - coord[3]) * (coord[0] - coord[3]) +
+                                 (coord[1] - coord[4]) * (coord[1] - coord[4]) +
+                                 (coord[2] - coord[5]) * (coord[2] - coord[5]));
+            const long idx = u + Nd * v + Nd * Nd * nn;
+            proj[idx] *= L / (factor[u + Nd * v] + (real)1e-5f);
+        }
+}
+
+/* projRatio (ir.cu:1616-1635, art == 0) / projSubtract (ir.cu:1656-1666).
+ * Adds every |b - p| to *loss in the reference's serial order (one running
+ * sum over all views, as the reference's single loss1 accumulator). */
+void RV(ratio)(const or_scan *s, int n, real *proj, const real *sino, int art, real *loss) {
+    const long Nd = s->Nd;
+    const long nn = n < 0 ? -n : n;
+    for (long v = 0; v < Nd; v++)
+        for (long u = 0; u < Nd; u++) {
+            const long idx = u + Nd * v + Nd * Nd * nn;
+            *loss += RFABS(sino[idx] - proj[idx]);
+            if (art) {
+                proj[idx] = sino[idx] - proj[idx];
+            } else {
+                if (proj[idx] != (real)0) proj[idx] = sino[idx] / proj[idx];
+                if (proj[idx] > (real)2.0) proj[idx] = (real)2.0;
+            }
+        }
+}
+
+/* backwardProj/backwardonDevice (ir.cu:1605-1614,1720-1751, xtt == 0) or
+ * backwardProjXTT/backwardXTTonDevice (ir.cu:143-152,1807-1850) for one y slab
+ * and one view; tmp/factor are the slab accumulators (K planes of N*N). */
+void RV(backward_slab)(const or_scan *s, int cond, int y, int n, const real *proj, real *tmp,
+                       real *factor, int xtt) {
+    RV(frame) f;
+    RV(view_frame)(s, cond, n, 0, &f);
+    const long N = s->N, Nd = s->Nd;
+    const long nn = n < 0 ? -n : n;
+    real G[3];
+    { const real bz[3] = {(real)0, (real)0, (real)1}; RV(mat3vec)(f.R, bz, G); }
+    for (long z = 0; z < N; z++)
+        for (long x = 0; x < N; x++) {
+            real u, v, B[3], c[4];
+            long iu, iv;
+            RV(raycast)(s, &f, 0, (int)x, y, (int)z, &u, &v, xtt ? B : 0, 0);
+            if (!RV(taps)(s, u, v, &iu, &iv, c)) continue;
+            const long base = Nd * Nd * nn;
+            const real p0 = proj[iu + Nd * (iv + 1) + base], p1 = proj[(iu + 1) + Nd * (iv + 1) + base];
+            const real p2 = proj[(iu + 1) + Nd * iv + base], p3 = proj[iu + Nd * iv + base];
+            const long idx = x + N * z;
+            if (!xtt) {
+                const real nb = c[0] * p0 + c[1] * p1 + c[2] * p2 + c[3] * p3;
+                factor[idx] += (real)1.0;
+                tmp[idx] += nb;
+            } else {
+                for (int k = 0; k < s->K; k++) {
+                    real S[3] = {(real)s->basis[3 * k], (real)s->basis[3 * k + 1], (real)s->basis[3 * k + 2]};
+                    const real w = RV(xtt_weight)(B, S, G);
+                    const real bf = w * c[0] * p0 + w * c[1] * p1 + w * c[2] * p2 + w * c[3] * p3;
+                    factor[idx + (long)k * N * N] += w;
+                    tmp[idx + (long)k * N * N] += bf;
+                }
+            }
+        }
+}
+
+/* voxelProduct (ir.cu:1637-1654, MLEM) or voxelPlus (ir.cu:1682-1693, ART)
+ * on slab y of one channel. */
+void RV(voxel_update)(const or_scan *s, int y, real *vol, const real *tmp, const real *factor, int art,
+                      real alpha) {
+    const long N = s->N;
+    for (long z = 0; z < N; z++)
+        for (long x = 0; x < N; x++) {
+            const long iv = x + N * y + N * N * z, ip = x + N * z;
+            if (art)
+                vol[iv] = vol[iv] + alpha * tmp[ip];
+            else
+                vol[iv] = (factor[ip] == (real)0) ? (real)0 : vol[iv] * tmp[ip] / factor[ip];
+        }
+}
+
+/* voxelSqrt, ir.cu:1707-1717, over all K channels. */
+void RV(voxel_sqrt)(const or_scan *s, real *vol) {
+    const long n = (long)s->N * s->N * s->N * s->K;
+    for (long i = 0; i < n; i++) vol[i] = vol[i] < (real)0 ? RSQRT(-vol[i]) : RSQRT(vol[i]);
+}
+
+/* The normalised forward operator A of the reconstruction loops: forward +
+ * correlation for every axis and view (what the loops compare with b). */
+void RV(forward_all)(const or_scan *s, const real *vol, real *proj, int rotate_ccw, int xtt) {
+    const long Nd = s->Nd, V = s->V;
+    const long lenD = Nd * Nd * V;
+    const int rotation = rotate_ccw ? -1 : 1;
+    real *factor = (real *)malloc(sizeof(real) * Nd * Nd);
+    memset(proj, 0, sizeof(real) * lenD * s->C);
+    for (int cond = 0; cond < s->C; cond++)
+        for (long w = 0; w < V; w++) {
+            const int n = rotation * (int)w;
+            memset(factor, 0, sizeof(real) * Nd * Nd);
+            RV(forward_view)(s, cond, n, vol, proj + lenD * cond, factor, xtt);
+            RV(correlation)(s, cond, n, proj + lenD * cond, factor);
+        }
+    free(factor);
+}
+
+/* IR::reconstruct, reconstruct.cu:23-156.  orders holds C*epoch rows of the
+ * subset order (the reference shuffles one std::mt19937_64 stream, :75,81);
+ * losses receives C*epoch raw loss sums. */
+void RV(ir_reconstruct)(const or_scan *s, real **sino, real **vol, int epoch, int batch, int rotate_ccw,
+                        int art, real lambda, real *losses, const int *orders) {
+    const long N = s->N, Nd = s->Nd, V = s->V;
+    const long lenD = Nd * Nd * V;
+    const int rotation = rotate_ccw ? -1 : 1;
+    const int subsetSize = (int)((V + batch - 1) / batch);
+    real *proj = (real *)malloc(sizeof(real) * lenD);
+    real *pf = (real *)malloc(sizeof(real) * Nd * Nd);
+    real *tmp = (real *)malloc(sizeof(real) * N * N);
+    real *fac = (real *)malloc(sizeof(real) * N * N);
+    for (int cond = 0; cond < s->C; cond++) {
+        for (int ep = 0; ep < epoch; ep++) {
+            const int *order = orders + ((long)cond * epoch + ep) * batch;
+            real loss = (real)0;
+            memset(proj, 0, sizeof(real) * lenD);
+            for (int b = 0; b < batch; b++) {
+                const int sub = order[b];
+                for (int j = 0; j < subsetSize; j++) {
+                    memset(pf, 0, sizeof(real) * Nd * Nd);
+                    const int n = rotation * (int)((sub + batch * j) % V);
+                    RV(forward_view)(s, cond, n, vol[cond], proj, pf, 0);
+                    RV(correlation)(s, cond, n, proj, pf);
+                    RV(ratio)(s, n, proj, sino[cond], art, &loss);
+                }
+                for (int y = 0; y < N; y++) {
+                    memset(tmp, 0, sizeof(real) * N * N);
+                    memset(fac, 0, sizeof(real) * N * N);
+                    for (int j = 0; j < subsetSize; j++) {
+                        const int n = rotation * (int)((sub + batch * j) % V);
+                        RV(backward_slab)(s, cond, y, n, proj, tmp, fac, 0);
+                    }
+                    RV(voxel_update)(s, y, vol[cond], tmp, fac, art, lambda / (real)subsetSize);
+                }
+            }
+            if (losses) losses[(long)cond * epoch + ep] = loss;
+        }
+    }
+    free(proj); free(pf); free(tmp); free(fac);
+}
+
+/* XTT::reconstruct, reconstruct.cu:799-927 (without the orientation step;
+ * see orientation below).  vol is ONE buffer of K*N^3 (the device layout,
+ * reconstruct.cu:819,828-829); proj (C*lenD) receives the last ratio images
+ * (the reference copies them over the sinograms, :924-925).  orders holds
+ * epoch rows (a fresh engine shuffles a persistent order each epoch, :858-859). */
+void RV(xtt_reconstruct)(const or_scan *s, const real *sino, real *vol, real *proj, int epoch, int batch,
+                         int rotate_ccw, int art, real lambda, real *losses, const int *orders) {
+    const long N = s->N, Nd = s->Nd, V = s->V, K = s->K;
+    const long lenD = Nd * Nd * V, lenV = N * N * N, lenP = N * N;
+    const int rotation = rotate_ccw ? -1 : 1;
+    const int subsetSize = (int)((V + batch - 1) / batch);
+    real *pf = (real *)malloc(sizeof(real) * Nd * Nd);
+    real *tmp = (real *)malloc(sizeof(real) * lenP * K);
+    real *fac = (real *)malloc(sizeof(real) * lenP * K);
+    for (int ep = 0; ep < epoch; ep++) {
+        const int *order = orders + (long)ep * batch;
+        real loss = (real)0;
+        memset(proj, 0, sizeof(real) * lenD * s->C);
+        for (int b = 0; b < batch; b++) {
+            const int sub = order[b];
+            for (int cond = 0; cond < s->C; cond++)
+                for (int j = 0; j < subsetSize; j++) {
+                    memset(pf, 0, sizeof(real) * Nd * Nd);
+                    const int n = rotation * (int)((sub + batch * j) % V);
+                    RV(forward_view)(s, cond, n, vol, proj + lenD * cond, pf, 1);
+                    RV(correlation)(s, cond, n, proj + lenD * cond, pf);
+                    RV(ratio)(s, n, proj + lenD * cond, sino + lenD * cond, art, &loss);
+                }
+            for (int y = 0; y < N; y++) {
+                memset(tmp, 0, sizeof(real) * lenP * K);
+                memset(fac, 0, sizeof(real) * lenP * K);
+                for (int cond = 0; cond < s->C; cond++)
+                    for (int j = 0; j < subsetSize; j++) {
+                        const int n = rotation * (int)((sub + batch * j) % V);
+                        RV(backward_slab)(s, cond, y, n, proj + lenD * cond, tmp, fac, 1);
+                    }
+                for (long k = 0; k < K; k++)
+                    RV(voxel_update)(s, y, vol + lenV * k, tmp + lenP * k, fac + lenP * k, art,
+                                     lambda / (real)subsetSize);
+            }
+        }
+        if (losses) losses[ep] = loss;
+    }
+    RV(voxel_sqrt)(s, vol);
+    free(pf); free(tmp); free(fac);
+}
+
+/* ---------------------------------------------------------------- FDK ---- */
+
+/* calcWeight, fdk.cu:13-26. */
+void RV(fdk_weight)(const or_scan *s, real *w) {
+    const long Nd = s->Nd;
+    for (long v = 0; v < Nd; v++)
+        for (long u = 0; u < Nd; u++) {
+            const real ur = ((real)u + (real)0.5 - (real)Nd / (real)2.0) * (real)s->det;
+            const real vr = ((real)v + (real)0.5 - (real)Nd / (real)2.0) * (real)s->det;
+            w[u + Nd * v] = (real)s->sdd / RSQRT((real)s->sdd * (real)s->sdd + ur * ur + vr * vr);
+        }
+}
+
+/* The filter table built on the host, reconstruct.cu:1694-1698 (ramlak=0), or
+ * a Ram-Lak (band-limited ramp) table in the same scaling (the sample spacing d
+ * and the 1/2 of a full 360-degree scan folded in): h[0] = 1/(8d),
+ * h[odd k] = -1/(2 pi^2 k^2 d), h[even k > 0] = 0 (ramlak=1; the reference has
+ * no Ram-Lak). */
+void RV(fdk_filter)(const or_scan *s, int ramlak, real *filt) {
+    const real d = (real)s->det * ((real)s->sod / (real)s->sdd);
+    for (long k = 0; k < s->Nd; k++) {
+        if (!ramlak) {
+#if OR_IS_FLOAT
+            filt[k] = 1.0f / (float)(M_PI * M_PI * d * (1.0f - 4.0f * (float)(k * k)));
+#else
+            filt[k] = 1.0 / (M_PI * M_PI * d * (1.0 - 4.0 * (double)(k * k)));
+#endif
+        } else {
+            if (k == 0) filt[k] = (real)1 / ((real)8 * d);
+            else if (k % 2) filt[k] = -(real)1 / ((real)2 * (real)(M_PI * M_PI) * (real)(k * k) * d);
+            else filt[k] = (real)0;
+        }
+    }
+}
+
+/* projConv, fdk.cu:28-43, for view |n|: dst += sum_j filt[|u-j|] src[j] w[j]
+ * along each detector row (dst starts at zero: the reference never clears it,
+ * reconstruct.cu:1669, which is taken as zero). */
+void RV(fdk_conv)(const or_scan *s, int n, const real *src, const real *filt, const real *w, real *dst) {
+    const long Nd = s->Nd;
+    const long nn = n < 0 ? -n : n;
+    for (long v = 0; v < Nd; v++)
+        for (long u = 0; u < Nd; u++) {
+            const long idx = u + Nd * v + Nd * Nd * nn;
+            real acc = dst[idx];
+            for (long j = 0; j < Nd; j++) {
+                const real fk = (u > j) ? filt[u - j] : filt[j - u];
+                acc += fk * src[Nd * v + j + Nd * Nd * nn] * w[Nd * v + j];
+            }
+            dst[idx] = acc;
+        }
+}
+
+/* filteredBackProj/backwardonDevice (FDK), fdk.cu:51-170: for one signed view
+ * n, vol[x,y,z] += (sod/(sod+o_y))^2 * (2 pi / V) * bilinear(proj). */
+void RV(fdk_backproject_view)(const or_scan *s, int cond, int n, const real *proj, real *vol) {
+    RV(frame) f;
+    RV(view_frame)(s, cond, n, 1, &f);
+    const long N = s->N, Nd = s->Nd;
+    const long nn = n < 0 ? -n : n;
+    const real Cw = (real)2.0 * (real)M_PI / (real)s->V;
+    for (long y = 0; y < N; y++)
+        for (long z = 0; z < N; z++)
+            for (long x = 0; x < N; x++) {
+                real u, v, c[4], o[3];
+                long iu, iv;
+                RV(raycast)(s, &f, 1, (int)x, (int)y, (int)z, &u, &v, 0, o);
+                if (!RV(taps)(s, u, v, &iu, &iv, c)) continue;
+                const real U = (real)s->sod / ((real)s->sod + o[1]);
+                const long base = Nd * Nd * nn;
+                const real nb = c[0] * proj[iu + Nd * (iv + 1) + base] + c[1] * proj[(iu + 1) + Nd * (iv + 1) + base] +
+                                c[2] * proj[(iu + 1) + Nd * iv + base] + c[3] * proj[iu + Nd * iv + base];
+                vol[x + N * y + N * N * z] += U * U * Cw * nb;
+            }
+}
+
+/* FDK::reconstruct, reconstruct.cu:1651-1724.  sino: C blocks; vol: C
+ * channels of N^3 (the reference writes channel `cond`, fdk.cu:163); filt_out
+ * (C blocks, may be NULL) receives the filtered projections (the reference
+ * copies them over the sinograms, :1713-1714).  block0 != 0 reproduces the
+ * reference's back-projection of axis 0's filtered block for every axis
+ * (:1708 passes devSinoFilt without the axis offset). */
+void RV(fdk_reconstruct)(const or_scan *s, const real *sino, real *vol, real *filt_out, int rotate_ccw,
+                         int ramlak, int block0) {
+    const long N = s->N, Nd = s->Nd, V = s->V;
+    const long lenD = Nd * Nd * V, lenV = N * N * N;
+    const int rotation = rotate_ccw ? -1 : 1;
+    real *w = (real *)malloc(sizeof(real) * Nd * Nd);
+    real *filt = (real *)malloc(sizeof(real) * Nd);
+    real *sf = (real *)calloc((size_t)(lenD * s->C), sizeof(real));
+    RV(fdk_weight)(s, w);
+    RV(fdk_filter)(s, ramlak, filt);
+    memset(vol, 0, sizeof(real) * lenV * s->C);
+    for (int cond = 0; cond < s->C; cond++)
+        for (long n = 0; n < V; n++) {
+            RV(fdk_conv)(s, (int)n, sino + lenD * cond, filt, w, sf + lenD * cond);
+            RV(fdk_backproject_view)(s, cond, rotation * (int)n, sf + (block0 ? 0 : lenD * cond), vol + lenV * cond);
+        }
+    if (filt_out) memcpy(filt_out, sf, sizeof(real) * lenD * s->C);
+    free(w); free(filt); free(sf);
+}
+
+/* Data residual in FP64 over all axes, views and pixels:
+ * out[0] = ||p - b||_2 / ||b||_2, out[1] = sum |b - p| (the reference's loss). */
+void RV(residual)(long n, const real *p, const real *b, double *out) {
+    double num = 0, den = 0, l1 = 0;
+    for (long i = 0; i < n; i++) {
+        const double d = (double)p[i] - (double)b[i];
+        num += d * d;
+        den += (double)b[i] * (double)b[i];
+        l1 += fabs(d);
+    }
+    out[0] = den > 0 ? sqrt(num / den) : 0.0;
+    out[1] = l1;
+}
+
+#undef RV
