@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Benchmark: XTT reconstruction throughput on B200.
+
+Workload (the XTT 256^3 x 13 configuration): 256^3 voxels x K = 13 scattering
+channels, 3 sample-rotation axes x 180 views over 360 degrees, 384 x 384
+detector, SOD 500 / SDD 1000 / 1 mm voxels, 12 seeded straight fiber
+cylinders; OS-EM (the reference's XTT::reconstruct, method MLEM, 5 subsets as
+main.cu:60) from mu = 0.01.  One step = one OS-EM epoch: forward + ratio +
+back-projection/update of every view of every axis.
+
+metric  effective projector bandwidth: every epoch applies the forward and
+        the back projector once to each of the C*V views, each charged
+        bytes_view = K*N^3*4 + Nd^2*4 (the volume streamed once plus one
+        detector image), so value = 2*C*V*bytes_view / epoch time.
+e2e     the same metric through the public host-buffer call
+        (xr_xtt_reconstruct, one epoch, pinned host buffers, including the
+        H2D of sinograms + initial volume and the D2H of volume, ratio
+        images and orientation).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib.util
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "xray-directional-reconstruction_b200")
+
+W = dict(N=256, Nd=384, V=180, C=3, K=13, batch=5, sdd=1000.0, sod=500.0, det=2.0, n_fibers=12, seed=5)
+WORKLOAD = ("XTT 256^3 x K13, 3 axes x 180 views, 384^2 detector, OS-EM 5 subsets, FP32 "
+            "(12 seeded fiber cylinders, SOD 500 / SDD 1000 mm, 1 mm voxels)")
+METRIC = "XTT 256^3x13 projector GB/s (effective, forward+back per OS-EM epoch)"
+
+
+def load_pkg():
+    if "xrd" in sys.modules:
+        return sys.modules["xrd"]
+    spec = importlib.util.spec_from_file_location("xrd", os.path.join(PKG, "__init__.py"),
+                                                  submodule_search_locations=[PKG])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["xrd"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def three_axes():
+    return np.array([[1, 0, 0, 0, 1, 0, 0, 0, 1], [0, 0, -1, 0, 1, 0, 1, 0, 0], [1, 0, 0, 0, 0, -1, 0, 1, 0]],
+                    np.float32)
+
+
+def basis13():
+    d = [(1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (1, -1, 0), (1, 0, 1), (1, 0, -1), (0, 1, 1), (0, 1, -1),
+         (1, 1, 1), (1, 1, -1), (1, -1, 1), (-1, 1, 1)]
+    return np.array([np.asarray(v, np.float64) / np.linalg.norm(v) for v in d], np.float32)
+
+
+def fiber_phantom(N, n_fib, seed, basis):
+    """Fibers of radius U[2,5] voxels with unit direction f uniform on the
+    sphere; channel k = |S_k x f|^2 inside, 0 outside.  (K, N, N, N) float32."""
+    rng = np.random.default_rng(seed)
+    c = (np.arange(N, dtype=np.float32) - (N - 1) / 2.0)
+    vol = np.zeros((basis.shape[0], N, N, N), np.float32)
+    for _ in range(n_fib):
+        f = rng.normal(size=3)
+        f /= np.linalg.norm(f)
+        p0 = rng.uniform(-0.3 * N, 0.3 * N, 3)
+        r = rng.uniform(2.0, 5.0)
+        eta = np.sum(np.cross(basis.astype(np.float64), f[None, :]) ** 2, axis=1).astype(np.float32)
+        for z in range(N):
+            dz = c[z] - p0[2]
+            dy = (c - p0[1])[:, None]
+            dx = (c - p0[0])[None, :]
+            t = dx * f[0] + dy * f[1] + dz * f[2]
+            d2 = dx * dx + dy * dy + dz * dz - t * t
+            inside = d2 <= r * r
+            if inside.any():
+                for k in range(basis.shape[0]):
+                    vol[k, z][inside] = eta[k]
+    return vol
+
+
+def bytes_view(K, N, Nd, s=4):
+    return K * N ** 3 * s + Nd * Nd * s
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` at this workload from the committed
+    ncu summary, if present (profiles/*.md line 'traffic_per_launch <kernel> <bytes>')."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for fn in sorted(os.listdir(d)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(d, fn)):
+            m = re.match(r"\s*traffic_per_launch\s+(\S+)\s+([0-9.eE+]+)", line)
+            if m and m.group(1) == kernel:
+                return float(m.group(2))
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap,utilization.gpu",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.proc is None:
+            return out
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7 and parts[0].replace(".", "").isdigit():
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        loaded = [r for r in rows if r[6].isdigit() and int(r[6]) > 0] or rows
+        out["sm_mhz"] = statistics.median(float(r[0]) for r in loaded)
+        out["sm_max_mhz"] = max(float(r[1]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        out["reasons"] = [n for i, n in enumerate(names) if any(r[2 + i].lower() == "active" for r in loaded)]
+        out["samples"] = len(loaded)
+        return out
+
+
+def cpu_reference_sample(mu_host: np.ndarray, b_host: np.ndarray, n_views: int, warm: int = 0):
+    """Time the reference's own projector kernels (reconstruct/src/ir.cu built
+    for the host, OpenMP over detector/voxel rows) on n_views views of the
+    same workload: forward + correlation + ratio, then the back-projection of
+    every y slab.  Returns (seconds, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefHost, Scan
+    s = Scan(sdd=W["sdd"], sod=W["sod"], det=W["det"], N=W["N"], Nd=W["Nd"], V=W["V"], rot=three_axes(),
+             trans=np.zeros((3, 3)), offset=np.zeros((3, 3)), basis=basis13())
+    R = RefHost(parallel=True)
+    R.setup(s)
+    N, Nd, K = s.N, s.Nd, s.K
+    vol = np.ascontiguousarray(mu_host.reshape(-1))
+    proj = np.zeros(s.V * Nd * Nd, np.float32)
+    fac = np.zeros(Nd * Nd, np.float32)
+    tmp = np.zeros(N * N * K, np.float32)
+    bfac = np.zeros(N * N * K, np.float32)
+    views = [(c, (v * 37) % s.V) for c in range(s.C) for v in range(s.V)]
+    t_total = 0.0
+    for i in range(warm + n_views):
+        cond, n = views[i % len(views)]
+        sino = np.ascontiguousarray(b_host[cond].reshape(-1))
+        t0 = time.perf_counter()
+        R.forward_view(cond, n, vol, proj, fac, 1)
+        R.correlation(cond, n, proj, fac)
+        R.ratio(n, proj, sino, 0)
+        for y in range(N):
+            tmp[:] = 0
+            bfac[:] = 0
+            R.backward_slab(cond, y, n, proj, tmp, bfac, 1)
+        dt = time.perf_counter() - t0
+        if i >= warm:
+            t_total += dt
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return t_total, threads
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference's CPU implementation of the path on
+    the host cores (oracle/_ref, its own ir.cu), same metric and config."""
+    if rank != 0:
+        return
+    bv = bytes_view(W["K"], W["N"], W["Nd"])
+    mu = fiber_phantom(W["N"], W["n_fibers"], W["seed"], basis13())
+    rng = np.random.default_rng(1)
+    b = rng.uniform(0.0, 50.0, (W["C"], W["V"], W["Nd"], W["Nd"])).astype(np.float32)
+    per_step_views = 1
+    times = []
+    threads = 1
+    for i in range(args.warmup + args.steps):
+        t, threads = cpu_reference_sample(mu, b, per_step_views, 0)
+        if i >= args.warmup:
+            times.append(t)
+    t_step = float(np.mean(times))
+    value = 2 * per_step_views * bv / t_step / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": f"{per_step_views} view (forward+ratio+back, all K) per step"},
+            "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "reference",
+                             "sample": f"{per_step_views} of {W['C'] * W['V']} views per step, reference ir.cu "
+                                       "kernels compiled for the host, OpenMP"},
+            "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    xr = load_pkg()
+    s_basis = basis13()
+    ctx = xr.Context.create(W["sdd"], W["sod"], W["det"], W["N"], W["Nd"], W["V"], three_axes(), None, None,
+                            s_basis, device=local)
+    # one non-default stream shared by torch and the library, so the CUDA
+    # events below bracket the library's kernels
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+
+    N, Nd, V, C, K = W["N"], W["Nd"], W["V"], W["C"], W["K"]
+    mu_true = fiber_phantom(N, W["n_fibers"], W["seed"] + rank, s_basis)
+    d_true = torch.from_numpy(mu_true).cuda()
+    d_b = torch.empty((C, V, Nd, Nd), dtype=torch.float32, device="cuda")
+    ctx.dev_forward(d_true.data_ptr(), d_b.data_ptr(), True)           # b = A mu_true
+    d_vol = torch.full((K, N, N, N), 0.01, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+
+    ctx.dev_session_begin(d_b.data_ptr(), d_vol.data_ptr(), True, args.warmup + args.steps, W["batch"])
+    for _ in range(args.warmup):
+        ctx.dev_session_epoch()
+    torch.cuda.synchronize()
+    ctx.set_option(xr.Option.TIMING, 1)
+    ctx.reset_timings()
+
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        ctx.dev_session_epoch()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    t_ms = ev0.elapsed_time(ev1) / args.steps
+    tim = ctx.timings()
+    ctx.set_option(xr.Option.TIMING, 0)
+    rel, _ = ctx.dev_residual(d_vol.data_ptr(), d_b.data_ptr(), True)   # ||A mu - b|| / ||b|| after the epochs
+    ctx.dev_session_end(0, 0)
+
+    bv = bytes_view(K, N, Nd)
+    per_gpu_bytes = 2 * C * V * bv
+    value = world * per_gpu_bytes / (t_ms / 1e3) / 1e9
+
+    # roofline of the dominant kernel (forward or back), per launch
+    views_per_launch = C * ((V + W["batch"] - 1) // W["batch"])
+    fwd_ms, fwd_n = tim["forward"]
+    back_ms, back_n = tim["back"]
+    dom, dom_ms, dom_n = ("k_forward<1>", fwd_ms, fwd_n) if fwd_ms >= back_ms else ("k_back_update<true>", back_ms,
+                                                                                     back_n)
+    peak, peak_kind = measured_peaks()
+    avg_launch_s = dom_ms / max(dom_n, 1) / 1e3
+    achieved = views_per_launch * bv / avg_launch_s / 1e9
+    traffic = profile_traffic(dom)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": dom, "peak_kind": peak_kind,
+                "avg_launch_ms": avg_launch_s * 1e3, "units_per_launch": views_per_launch,
+                "bytes_per_unit": bv,
+                "note": "effective: the kernel reads the volume once per launch for all its views"}
+    launches = int(sum(n for _, n in tim.values()))
+
+    # e2e through the public host-buffer API (pinned host memory), every rank
+    e2e = None
+    e2e_ms = None
+    if not args.no_e2e:
+        h_b = d_b.cpu().pin_memory()
+        h_v0 = torch.full((K, N, N, N), 0.01, dtype=torch.float32).pin_memory()
+        h_vol = torch.empty((K, N, N, N), dtype=torch.float32).pin_memory()
+        h_sino = torch.empty((C, V, Nd, Nd), dtype=torch.float32).pin_memory()
+        h_md = torch.empty((6, N, N, N), dtype=torch.float32).pin_memory()
+        FP = ctypes.POINTER(ctypes.c_float)
+
+        def ptrs(t, n):
+            base = t.data_ptr()
+            step = t[0].numel() * 4
+            return (FP * n)(*[ctypes.cast(base + i * step, FP) for i in range(n)])
+
+        L = xr.lib()
+        times = []
+        for i in range(3 + args.steps):
+            h_vol.copy_(h_v0)
+            h_sino.copy_(h_b)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = L.xr_xtt_reconstruct(ctx._h, ptrs(h_sino, C), ptrs(h_vol, K), ptrs(h_md, 3),
+                                      ptrs(h_md[3:], 3), 1, W["batch"], 0, 1, ctypes.c_float(1e-2), None)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if st:
+                raise RuntimeError(L.xr_last_error(ctx._h).decode())
+            if i >= 3:
+                times.append(e0.elapsed_time(e1))
+        e2e_ms = float(np.mean(times))
+
+    if world > 1:
+        t = torch.tensor([t_ms, e2e_ms or 0.0], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms, e2e_ms = float(t[0].item()), (float(t[1].item()) if e2e_ms else None)
+        value = world * per_gpu_bytes / (t_ms / 1e3) / 1e9
+        if dist.get_rank() != 0:
+            dist.barrier()
+            dist.destroy_process_group()
+            return
+    if e2e_ms:
+        h2d = C * V * Nd * Nd * 4 + K * N ** 3 * 4
+        d2h = K * N ** 3 * 4 + C * V * Nd * Nd * 4 + 6 * N ** 3 * 4
+        e2e = {"value": world * per_gpu_bytes / (e2e_ms / 1e3) / 1e9, "unit": "GB/s",
+               "ms_per_step": e2e_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "call": "xr_xtt_reconstruct(epoch=1) with pinned host buffers, incl. sqrt + orientation"}
+
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        n_views = 2
+        t, threads = cpu_reference_sample(mu_true, d_b.cpu().numpy(), n_views, 0)
+        cpu = {"value": 2 * n_views * bv / t / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
+               "sample": f"{n_views} of {C * V} views (forward+ratio+back, all K), reference ir.cu kernels "
+                         "compiled for the host, OpenMP"}
+
+    line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "N": N, "K": K, "axes": C, "views": V, "detector": Nd,
+                       "subsets": W["batch"], "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (volume 872 MB, sinograms 318 MB)",
+                       "residual_rel_l2_after": rel},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in tim.items() if v[1]}}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

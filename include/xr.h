@@ -1,0 +1,211 @@
+/*
+ * xr.h — C ABI of the B200 (sm_100a) reconstruction library libxr.so.
+ *
+ * Drop-in boundary for the reference's reconstruction hot path
+ * (ixactly/Xray-directional-reconstruction): every entry point below names the
+ * reference interface it replaces.  Plain pointers and sizes only; the caller
+ * owns every buffer and the library keeps no host pointer after a call.
+ *
+ * Layouts are the reference's:
+ *   volume     N*N*N floats, x fastest: idx = x + N*y + N*N*z   (volume.h:65-71)
+ *   sinogram   V views of Nd*Nd, u fastest, then v, then view   (ir.cu:1518)
+ * Host-buffer entry points take one pointer per axis / per basis channel, as
+ * the reference's Volume<float> arrays (reconstruct.cuh:27-45).  Device-buffer
+ * entry points (xr_dev_*) take contiguous device memory: K channels of N^3
+ * back to back and C axis blocks of V*Nd*Nd back to back
+ * (reconstruct.cu:816-829).
+ *
+ * Every call returns an xr_status; xr_last_error() gives the message.  A
+ * context is not thread-safe: use one context per host thread.  Work runs on
+ * the context's stream (xr_set_stream), host-buffer calls synchronize it
+ * before returning.
+ */
+#ifndef XR_H
+#define XR_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum xr_status {
+    XR_OK = 0,
+    XR_ERR_ARG = 1,      /* bad argument (null pointer, size, enum)         */
+    XR_ERR_OOM = 2,      /* device allocation failed                         */
+    XR_ERR_CUDA = 3,     /* CUDA runtime / launch error                      */
+    XR_ERR_TIMEOUT = 4,  /* a bounded device wait gave up                    */
+    XR_ERR_IO = 5,       /* file could not be read / written                 */
+    XR_ERR_CONFIG = 6,   /* settings file malformed or key missing           */
+    XR_ERR_NODEV = 7,    /* no CUDA device, or not an sm_100 device          */
+    XR_ERR_STATE = 8     /* call out of order (e.g. epoch before begin)      */
+} xr_status;
+
+/* enum class Method, reconstruct.cuh:14-19 */
+typedef enum xr_method { XR_METHOD_XTT = 0, XR_METHOD_MLEM = 1, XR_METHOD_ART = 2, XR_METHOD_FDK = 3 } xr_method;
+/* enum class Rotate, reconstruct.cuh:21-24 (CW: view n at +2*pi*n/V) */
+typedef enum xr_rotate { XR_ROTATE_CW = 0, XR_ROTATE_CCW = 1 } xr_rotate;
+/* FDK filter tables: the reference's (reconstruct.cu:1692-1698) or Ram-Lak */
+typedef enum xr_filter { XR_FILTER_REFERENCE = 0, XR_FILTER_RAMLAK = 1 } xr_filter;
+
+/* Scan description: Geometry (geometry.h:8-25) plus the globals init_params
+ * fills (params.cu:14-40).  voxSize is derived, sod*det_size/sdd
+ * (geometry.h:13).  Arrays are read at xr_create and copied. */
+typedef struct xr_scan {
+    float sdd;          /* source-detector distance  (SRC_DETECT_DISTANCE)       */
+    float sod;          /* source-object distance    (SRC_OBJ_DISTANCE)          */
+    float det_size;     /* detector pixel pitch      (DETECTOR_SIZE)             */
+    int num_voxel;      /* N, voxels per side        (NUM_VOXEL)                 */
+    int num_detect;     /* Nd, pixels per side       (NUM_DETECT_U == _V)        */
+    int num_proj;       /* V, views per axis over 360 degrees (NUM_PROJ)         */
+    int num_cond;       /* C, sample rotation axes   (NUM_PROJ_COND)             */
+    int num_basis;      /* K, scattering vectors     (NUM_BASIS_VECTOR)          */
+    const float *rot;   /* 9*C  elemR, row-major per axis                        */
+    const float *trans; /* 3*C  elemT (areaTrans already added, params.cu:74-78) */
+    const float *offset;/* 3*C  INIT_OFFSET                                      */
+    const float *basis; /* 3*K  basisVector                                      */
+} xr_scan;
+
+typedef struct xr_ctx xr_ctx;
+
+/* Per-kernel-class device time, accumulated while XR_OPT_TIMING is on
+ * (CUDA events on the context stream).  Classes: */
+enum {
+    XR_T_FORWARD = 0,   /* forward splat (plain / XTT)                  */
+    XR_T_RATIO = 1,     /* normalisation + ratio/subtract + loss        */
+    XR_T_BACK = 2,      /* back-projection fused with the voxel update  */
+    XR_T_SETUP = 3,     /* normaliser precompute (weights + chord)      */
+    XR_T_ORIENT = 4,    /* sqrt + per-voxel eigen                       */
+    XR_T_FDK = 5,       /* FDK weight/convolution/back-projection       */
+    XR_T_OTHER = 6,     /* residual, memsets, copies                    */
+    XR_T_COUNT = 7
+};
+typedef struct xr_timings {
+    double ms[XR_T_COUNT];
+    long launches[XR_T_COUNT];
+} xr_timings;
+
+/* Options (xr_set_option) */
+enum {
+    XR_OPT_TIMING = 1,        /* 1: record per-class device times                 */
+    XR_OPT_FDK_AXIS_BLOCKS = 2,/* 1: FDK back-projects each axis's own filtered
+                                  block; 0 (default): axis 0's block for every
+                                  axis, as the reference (reconstruct.cu:1708)   */
+    XR_OPT_VIEWS_PER_CTA = 3,  /* forward splat: views per CTA (0 = automatic)    */
+    XR_OPT_STORAGE = 4         /* 0: FP32 storage; 1: BF16 volume+sinogram storage
+                                  with FP32 accumulation (device-session calls)   */
+};
+
+/* ---- context ----------------------------------------------------------- */
+
+/* Replaces Geometry(sdd, sod, detSize, voxel, detect, nProj) + the globals of
+ * init_params (geometry.h:10-14, params.cu:42-104).  device: CUDA ordinal. */
+xr_status xr_create(const xr_scan *scan, int device, xr_ctx **out);
+
+/* init_params(tag), params.cu:42-104: reads `tag` from a settings.json of the
+ * reference's schema (utility/settings.json), including the sorting/index
+ * axis permutation (:80-95) and areaTrans (:74-78).  The path is an argument
+ * (the reference hard-codes it, :43); a preset without "sorting" reads as
+ * sorting=false. */
+xr_status xr_init_params(const char *json_path, const char *tag, int device, xr_ctx **out);
+
+void xr_destroy(xr_ctx *ctx);
+const char *xr_last_error(const xr_ctx *ctx);
+/* Scan as stored (pointers valid while ctx lives). */
+xr_status xr_get_scan(const xr_ctx *ctx, xr_scan *out);
+/* PROJ_PATH, VOLUME_PATH, DIRECTION_PATH and LOAD_INDEX (params.cu:46-95);
+ * load_index receives C ints (1-based file indices). */
+xr_status xr_get_paths(const xr_ctx *ctx, const char **proj_path, const char **vol_path,
+                       const char **direc_path, int *load_index);
+/* Use `stream` (a cudaStream_t) for all device work; NULL = the context's own. */
+xr_status xr_set_stream(xr_ctx *ctx, void *stream);
+xr_status xr_set_option(xr_ctx *ctx, int key, int value);
+xr_status xr_get_timings(const xr_ctx *ctx, xr_timings *out);
+xr_status xr_reset_timings(xr_ctx *ctx);
+
+/* ---- host-buffer entry points (the reference's call surface) ------------ */
+
+/* forwardProjOnly, reconstruct.cu:1890-1949: the raw voxel-driven splat of
+ * channel 0 (forwardProj, ir.cu:1480-1531) for every axis and view, without
+ * the chord-length normalisation.  voxel[1], sino[C]. */
+xr_status xr_forward_proj_only(xr_ctx *ctx, const float *const *voxel, float *const *sino, xr_rotate dir);
+
+/* The normalised forward operator of the reconstruction loops (forward splat +
+ * correlationProjByLength, ir.cu:1480-1603 / :1753-1804): what the loops
+ * compare with the measured sinogram.  xtt=0: channel 0, plain weights;
+ * xtt=1: K channels, dark-field weights.  voxel[1 or K], sino[C]. */
+xr_status xr_forward(xr_ctx *ctx, const float *const *voxel, float *const *sino, xr_rotate dir, int xtt);
+
+/* IR::reconstruct, reconstruct.cu:23-156 (reconstruct.cuh:27-28): OS-EM
+ * (XR_METHOD_MLEM) or OS-ART (XR_METHOD_ART, step lambda/subsetSize) of each
+ * axis independently into voxel[cond].  sino[C], voxel[C] (in: initial
+ * volume, out: result).  losses: NULL or C*epoch raw sums of |b - Ax| per
+ * epoch (the reference keeps the last axis's, :131). */
+xr_status xr_ir_reconstruct(xr_ctx *ctx, float *const *sino, float *const *voxel, int epoch, int batch,
+                            xr_rotate dir, xr_method method, float lambda, float *losses);
+
+/* XTT::reconstruct, reconstruct.cu:799-954 (reconstruct.cuh:42-45): joint
+ * OS-EM / OS-ART of the K scattering channels over all axes, then
+ * mu_k = sqrt|mu_k| and, when md != NULL, the per-voxel orientation
+ * (calcEigenVector, direction/src/pca.cu:12-55) into md[3] (and evalue[3]
+ * when evalue != NULL).  sino[C] is overwritten with the last ratio images,
+ * as the reference does (:924-925).  losses: NULL or epoch raw sums. */
+xr_status xr_xtt_reconstruct(xr_ctx *ctx, float *const *sino, float *const *voxel, float *const *md,
+                             float *const *evalue, int epoch, int batch, xr_rotate dir, xr_method method,
+                             float lambda, float *losses);
+
+/* FDK::reconstruct, reconstruct.cu:1651-1724: cosine weight (fdk.cu:13-26),
+ * row convolution (fdk.cu:28-43) and weighted back-projection
+ * (fdk.cu:51-170) of each axis into voxel[cond] (zeroed first).  sino[C] is
+ * overwritten with the filtered projections (:1713-1714). */
+xr_status xr_fdk_reconstruct(xr_ctx *ctx, float *const *sino, float *const *voxel, xr_rotate dir,
+                             xr_filter filter);
+
+/* calcEigenVector over every voxel (pca.cu:12-55, called at
+ * reconstruct.cu:935-942), in FP64 on the GPU.  mu[K] in, md[3] out,
+ * evalue[3] out (may be NULL). */
+xr_status xr_orientation(xr_ctx *ctx, const float *const *mu, float *const *md, float *const *evalue);
+
+/* calcAngleFromMD (pca.cu:67-83): angle[0] = phi, angle[1] = theta. */
+xr_status xr_angle_from_md(xr_ctx *ctx, const float *const *md, float *const *angle);
+/* directionNormalization (pca.cu:85-106): unit vectors where |md| > 0.65, else 0. */
+xr_status xr_direction_normalization(xr_ctx *ctx, float *const *md);
+
+/* Data residual (no reference counterpart; the reference logs only the L1
+ * sum, reconstruct.cu:951-953): rel_l2 = ||A x - b||_2 / ||b||_2 and
+ * l1 = sum |A x - b| over all axes, views and pixels, in FP64. */
+xr_status xr_residual(xr_ctx *ctx, const float *const *voxel, const float *const *sino, xr_rotate dir,
+                      int xtt, double *rel_l2, double *l1);
+
+/* ---- device-buffer entry points (no host copies) ------------------------ */
+
+xr_status xr_dev_forward(xr_ctx *ctx, const float *d_vol, float *d_sino, xr_rotate dir, int xtt);
+xr_status xr_dev_residual(xr_ctx *ctx, const float *d_vol, const float *d_sino, xr_rotate dir, int xtt,
+                          double *rel_l2, double *l1);
+xr_status xr_dev_orientation(xr_ctx *ctx, const float *d_mu, float *d_md, float *d_evalue);
+
+/* An XTT / IR reconstruction session on device buffers, split so a caller
+ * (or a CUDA graph) can drive epochs one at a time:
+ *   begin: geometry tables, normaliser and subset lists (iteration-invariant);
+ *          `epochs` is the planned epoch count (IR draws every axis's subset
+ *          orders from one engine, axis-major, reconstruct.cu:75-81, so the
+ *          order of (axis, epoch) depends on it; XTT ignores it);
+ *   epoch: one OS-EM/OS-ART epoch over all subsets; *loss = raw |b - Ax| sum
+ *          (may be NULL; reading it synchronizes the stream);
+ *   end:   XTT only — mu_k = sqrt|mu_k| and, when d_md != NULL, orientation.
+ * d_sino: C*V*Nd^2; d_vol: K*N^3 (XTT) or C*N^3 (IR).  Both stay owned by
+ * the caller and must outlive the session. */
+xr_status xr_dev_session_begin(xr_ctx *ctx, const float *d_sino, float *d_vol, int xtt, int epochs,
+                               int batch, xr_rotate dir, xr_method method, float lambda);
+xr_status xr_dev_session_epoch(xr_ctx *ctx, double *loss);
+xr_status xr_dev_session_end(xr_ctx *ctx, float *d_md, float *d_evalue);
+/* The session's current ratio images (C*V*Nd^2 floats, device pointer). */
+xr_status xr_dev_session_proj(xr_ctx *ctx, const float **d_proj);
+
+/* Library version string. */
+const char *xr_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XR_H */

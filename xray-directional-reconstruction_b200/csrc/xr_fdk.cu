@@ -1,0 +1,171 @@
+/*
+ * FDK on the GPU (FDK::reconstruct, reconstruct.cu:1651-1724).
+ *
+ * The reference launches calcWeight once, then per view one projConv over the
+ * detector followed by N filteredBackProj launches (one per y slab).  Here:
+ *   k_fdk_weight  cosine weight sdd / sqrt(sdd^2 + u^2 + v^2) (fdk.cu:13-26)
+ *   k_fdk_conv    every view's rows in one launch; a CTA stages one detector
+ *                 row of the projection and of the weight in shared memory
+ *                 and each thread sums filt[|u-j|] * src[j] * w[j] over j in
+ *                 the reference's order (fdk.cu:28-43)
+ *   k_fdk_bp      one thread per voxel loops over all views, gathering the
+ *                 bilinear taps and adding (sod/(sod+o_y))^2 * (2 pi/V) * tap
+ *                 sum in the reference's view order (fdk.cu:62-170), one store
+ *                 per voxel.
+ * FP32 operations on the per-voxel path are explicitly rounded (no FMA
+ * contraction), matching the reference's arithmetic.
+ */
+#include <cuda_runtime.h>
+
+#include "xr_internal.h"
+
+namespace xr {
+namespace {
+
+constexpr int kBpThreads = 256;
+constexpr int kFrameChunk = 128;
+
+__device__ __forceinline__ float dot_rn(float a0, float a1, float a2, float b0, float b1, float b2) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a0, b0), __fmul_rn(a1, b1)), __fmul_rn(a2, b2));
+}
+
+/* ((2i - N + 1) * 0.5) * vs: FDK's centred voxel grid (fdk.cu:132-135). */
+__device__ __forceinline__ float vox_base_fdk(int i, int N, float vs) {
+    const float a = __fadd_rn(__fsub_rn(__fmul_rn(2.0f, (float)i), (float)N), 1.0f);
+    return __fmul_rn(__fmul_rn(a, 0.5f), vs);
+}
+
+__global__ void k_fdk_weight(GeomConst g, float *w) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = blockIdx.y * blockDim.y + threadIdx.y;
+    if (u >= g.Nd || v >= g.Nd) return;
+    const float hn = __fdiv_rn((float)g.Nd, 2.0f);
+    const float ur = __fmul_rn(__fsub_rn(__fadd_rn((float)u, 0.5f), hn), g.det);
+    const float vr = __fmul_rn(__fsub_rn(__fadd_rn((float)v, 0.5f), hn), g.det);
+    const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(g.sdd, g.sdd), __fmul_rn(ur, ur)), __fmul_rn(vr, vr));
+    w[u + g.Nd * v] = __fdiv_rn(g.sdd, __fsqrt_rn(r2));
+}
+
+/* grid (row v, view, axis); dst row = sum_j filt[|u-j|] src[j] w[j]. */
+__global__ void k_fdk_conv(GeomConst g, const float *sino, float *dst, const float *filt, const float *w) {
+    extern __shared__ float sm[];
+    const int Nd = g.Nd;
+    float *srow = sm, *wrow = sm + Nd, *ft = sm + 2 * Nd;
+    const int v = blockIdx.x, view = blockIdx.y, cond = blockIdx.z;
+    const size_t off = ((size_t)cond * g.V + view) * (size_t)Nd * Nd + (size_t)Nd * v;
+    for (int j = threadIdx.x; j < Nd; j += blockDim.x) {
+        srow[j] = sino[off + j];
+        wrow[j] = w[(size_t)Nd * v + j];
+        ft[j] = filt[j];
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < Nd; u += blockDim.x) {
+        float acc = 0.0f;
+        for (int j = 0; j < Nd; j++) {
+            const float fk = ft[u > j ? u - j : j - u];
+            acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(fk, srow[j]), wrow[j]));
+        }
+        dst[off + u] = acc;
+    }
+}
+
+struct BpArgs {
+    GeomConst g;
+    const ViewFrame *frames;   /* FDK frames [C][V] (source at -sod)          */
+    const float *filt_sino;    /* C blocks of filtered projections            */
+    float *vol;                /* C channels of N^3                           */
+    int cond, src_block;
+};
+
+__global__ void __launch_bounds__(kBpThreads) k_fdk_bp(BpArgs a) {
+    __shared__ ViewFrame fr[kFrameChunk];
+    const GeomConst &g = a.g;
+    const int N = g.N, Nd = g.Nd;
+    const int nbx = (N + 7) / 8, nby = (N + 3) / 4;
+    const int b = blockIdx.x;
+    const int x = (b % nbx) * 8 + (threadIdx.x & 7);
+    const int y = ((b / nbx) % nby) * 4 + ((threadIdx.x >> 3) & 3);
+    const int z = (b / (nbx * nby)) * 8 + (threadIdx.x >> 5);
+    const bool ok = x < N && y < N && z < N;
+    const float bx = vox_base_fdk(x, N, g.vs), by = vox_base_fdk(y, N, g.vs), bz = vox_base_fdk(z, N, g.vs);
+    const size_t NdNd = (size_t)Nd * Nd;
+    const float *P = a.filt_sino + (size_t)a.src_block * g.V * NdNd;
+    const float Cw = __fdiv_rn(__fmul_rn(2.0f, (float)M_PI), (float)g.V);
+    float acc = 0.0f;
+    for (int c0 = 0; c0 < g.V; c0 += kFrameChunk) {
+        const int nc = min(kFrameChunk, g.V - c0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < nc * 5; i += kBpThreads) {
+            const int jj = i / 5, q = i % 5;
+            reinterpret_cast<float4 *>(&fr[jj])[q] =
+                reinterpret_cast<const float4 *>(&a.frames[(size_t)a.cond * g.V + c0 + jj])[q];
+        }
+        __syncthreads();
+        if (!ok) continue;
+        for (int jj = 0; jj < nc; jj++) {
+            const ViewFrame &f = fr[jj];
+            const float ox = __fsub_rn(__fsub_rn(bx, f.off[0]), f.t[0]);
+            const float oy = __fsub_rn(__fsub_rn(by, f.off[1]), f.t[1]);
+            const float oz = __fsub_rn(__fsub_rn(bz, f.off[2]), f.t[2]);
+            const float d0 = __fsub_rn(ox, f.src[0]), d1 = __fsub_rn(oy, f.src[1]), d2 = __fsub_rn(oz, f.src[2]);
+            const float coeff = __fdiv_rn(-f.ss, dot_rn(f.src[0], f.src[1], f.src[2], d0, d1, d2));
+            const float p0 = __fadd_rn(f.src[0], __fmul_rn(coeff, d0));
+            const float p1 = __fadd_rn(f.src[1], __fmul_rn(coeff, d1));
+            const float p2 = __fadd_rn(f.src[2], __fmul_rn(coeff, d2));
+            const float u = __fadd_rn(__fdiv_rn(__fmul_rn(dot_rn(p0, p1, p2, f.eu[0], f.eu[1], f.eu[2]), g.mag), g.det),
+                                      g.half);
+            const float v = __fadd_rn(__fdiv_rn(__fmul_rn(dot_rn(p0, p1, p2, f.ev[0], f.ev[1], f.ev[2]), g.mag), g.det),
+                                      g.half);
+            if (!(0.55f < u && u < g.lim && 0.55f < v && v < g.lim)) continue;
+            const float ut = __fsub_rn(u, 0.5f), vt = __fsub_rn(v, 0.5f);
+            const float fiu = floorf(ut), fiv = floorf(vt);
+            const int iu = (int)fiu, iv = (int)fiv;
+            const float fu = __fsub_rn(ut, fiu), fv = __fsub_rn(vt, fiv);
+            const float gu = __fsub_rn(1.0f, fu), gv = __fsub_rn(1.0f, fv);
+            const float c1 = __fmul_rn(gu, fv), c2 = __fmul_rn(fu, fv), c3 = __fmul_rn(fu, gv), c4 = __fmul_rn(gu, gv);
+            const float U = __fdiv_rn(g.sod, __fadd_rn(g.sod, oy));
+            const float *pp = P + (size_t)f.view * NdNd + iu + (size_t)Nd * iv;
+            const float p4 = __ldg(pp), p3 = __ldg(pp + 1), p1v = __ldg(pp + Nd), p2v = __ldg(pp + Nd + 1);
+            const float nb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(c1, p1v), __fmul_rn(c2, p2v)), __fmul_rn(c3, p3)),
+                                       __fmul_rn(c4, p4));
+            acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(__fmul_rn(U, U), Cw), nb));
+        }
+    }
+    if (ok) a.vol[(size_t)a.cond * N * N * N + (size_t)x + (size_t)N * y + (size_t)N * N * z] = acc;
+}
+
+}  // namespace
+
+cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_cond, const float *sino,
+                       float *sino_filt, float *vol, const float *filt, float *weight, int axis_blocks,
+                       cudaStream_t s) {
+    {
+        const dim3 blk(32, 8), grid((g.Nd + 31) / 32, (g.Nd + 7) / 8);
+        k_fdk_weight<<<grid, blk, 0, s>>>(g, weight);
+    }
+    {
+        const dim3 grid((unsigned)g.Nd, (unsigned)g.V, (unsigned)n_cond);
+        const size_t smem = 3 * (size_t)g.Nd * sizeof(float);
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(k_fdk_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        k_fdk_conv<<<grid, 128, smem, s>>>(g, sino, sino_filt, filt, weight);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const long nb = (long)((g.N + 7) / 8) * ((g.N + 3) / 4) * ((g.N + 7) / 8);
+    for (int c = 0; c < n_cond; c++) {
+        BpArgs a;
+        a.g = g;
+        a.frames = fdk_frames;
+        a.filt_sino = sino_filt;
+        a.vol = vol;
+        a.cond = c;
+        a.src_block = axis_blocks ? c : 0;
+        k_fdk_bp<<<(unsigned)nb, kBpThreads, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace xr

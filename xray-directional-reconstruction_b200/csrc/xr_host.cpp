@@ -1,0 +1,1014 @@
+/*
+ * Host side of libxr: context, settings reader, per-view geometry tables,
+ * the OS-EM / OS-ART / FDK schedulers and the C ABI of include/xr.h.
+ *
+ * Compiled with g++ -ffp-contract=off and no -march flags: the per-view
+ * tables are computed with the same float operations, in the same order and
+ * the same rounding as the reference's rayCasting (ir.cu:1860-1879), so the
+ * kernels see bit-identical rotation, source and offset vectors.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <random>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "xr_internal.h"
+#include "xr_json.h"
+
+namespace xr {
+
+constexpr int kMaxBasisXTT = 16; /* XTT back-projection keeps 2 accumulators per channel in registers */
+
+xr_status fail(xr_ctx *c, xr_status st, const std::string &msg) {
+    if (c) c->err = msg;
+    return st;
+}
+
+xr_status cuda_check(xr_ctx *c, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return XR_OK;
+    const xr_status st = (e == cudaErrorMemoryAllocation) ? XR_ERR_OOM : XR_ERR_CUDA;
+    return fail(c, st, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+xr_status ensure(xr_ctx *c, DevBuf &b, size_t bytes, const char *what) {
+    if (b.bytes >= bytes && b.p) return XR_OK;
+    if (b.p) {
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    if (bytes == 0) return XR_OK;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, XR_ERR_OOM, std::string("cudaMalloc(") + what + ", " + std::to_string(bytes) +
+                                       " bytes): " + cudaGetErrorString(e));
+    }
+    b.bytes = bytes;
+    return XR_OK;
+}
+
+static void release(DevBuf &b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+void timing_begin(xr_ctx *c, int cls, cudaEvent_t *ev) {
+    *ev = nullptr;
+    if (!c->timing.on) return;
+    (void)cls;
+    std::pair<cudaEvent_t, cudaEvent_t> pr{nullptr, nullptr};
+    if (!c->timing.pool.empty()) {
+        pr = c->timing.pool.back();
+        c->timing.pool.pop_back();
+    } else {
+        cudaEventCreate(&pr.first);
+        cudaEventCreate(&pr.second);
+    }
+    cudaEventRecord(pr.first, c->stream);
+    *ev = pr.first;
+    c->timing.pending[cls].push_back(pr);
+}
+
+void timing_end(xr_ctx *c, int cls, cudaEvent_t ev) {
+    if (!c->timing.on || !ev) return;
+    auto &v = c->timing.pending[cls];
+    if (!v.empty() && v.back().first == ev) {
+        cudaEventRecord(v.back().second, c->stream);
+        c->timing.launches[cls]++;
+    }
+}
+
+static void timing_collect(xr_ctx *c) {
+    for (int k = 0; k < XR_T_COUNT; k++) {
+        for (auto &pr : c->timing.pending[k]) {
+            cudaEventSynchronize(pr.second);
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) c->timing.ms[k] += ms;
+            c->timing.pool.push_back(pr);
+        }
+        c->timing.pending[k].clear();
+    }
+    cudaGetLastError();
+}
+
+/* RAII helper: time one launch of class `cls` on the context stream. */
+struct Timed {
+    xr_ctx *c;
+    int cls;
+    cudaEvent_t ev;
+    Timed(xr_ctx *c_, int cls_) : c(c_), cls(cls_) { timing_begin(c, cls, &ev); }
+    ~Timed() { timing_end(c, cls, ev); }
+};
+
+/* ---------------------------------------------------------------- geometry */
+
+/* Matrix3X::operator*(Matrix3X), vec.h:171-181. */
+static void mat3mul(const float *a, const float *b, float *w) {
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            float s = 0.0f;
+            for (int k = 0; k < 3; k++) s += a[3 * i + k] * b[3 * k + j];
+            w[3 * i + j] = s;
+        }
+}
+
+/* Matrix3X::operator*(Vector3X), vec.h:193-201. */
+static void mat3vec(const float *a, const float *v, float *w) {
+    for (int i = 0; i < 3; i++) {
+        float s = 0.0f;
+        for (int j = 0; j < 3; j++) s += a[3 * i + j] * v[j];
+        w[i] = s;
+    }
+}
+
+/* Per-(axis, signed view n) part of rayCasting (ir.cu:1860-1879); fdk selects
+ * the FDK source position (0, -sod, 0) (fdk.cu:125). */
+static ViewFrame make_frame(const xr_ctx *c, int cond, int n, bool fdk) {
+    ViewFrame f;
+    std::memset(&f, 0, sizeof(f));
+    const float theta = 2.0f * (float)M_PI * (float)n / (float)c->V;
+    const float cs = cosf(theta), sn = sinf(theta);
+    const float Rz[9] = {cs, -sn, 0.0f, sn, cs, 0.0f, 0.0f, 0.0f, 1.0f};
+    float R[9];
+    mat3mul(&c->rot[9 * cond], Rz, R);
+    mat3vec(R, &c->offset[3 * cond], f.off);
+    const float o2s[3] = {0.0f, fdk ? -c->sod : c->sod, 0.0f};
+    const float bu[3] = {1.0f, 0.0f, 0.0f}, bv[3] = {0.0f, 0.0f, 1.0f};
+    mat3vec(R, o2s, f.src);
+    mat3vec(R, bu, f.eu);
+    mat3vec(R, bv, f.ev);
+    f.e1x = R[1];
+    f.e1y = R[4];
+    f.e1z = R[7];
+    f.ss = f.src[0] * f.src[0] + f.src[1] * f.src[1] + f.src[2] * f.src[2];
+    for (int i = 0; i < 3; i++) f.t[i] = c->trans[3 * cond + i];
+    f.view = n < 0 ? -n : n;
+    return f;
+}
+
+static void fill_consts(xr_ctx *c) {
+    GeomConst &g = c->gc;
+    g.N = c->N;
+    g.Nd = c->Nd;
+    g.V = c->V;
+    g.C = c->C;
+    g.K = c->K;
+    g.vs = c->sod * c->det / c->sdd;                 /* geometry.h:13 */
+    g.mag = c->sdd / c->sod;                         /* ir.cu:1896    */
+    g.det = c->det;
+    g.half = 0.5f * (float)c->Nd;
+    g.lim = (float)c->Nd - 0.55f;                    /* ir.cu:1501    */
+    g.ratio = (g.vs * g.vs) / (c->det * (c->sod / c->sdd) * c->det * (c->sod / c->sdd)); /* ir.cu:1513 */
+    g.sod = c->sod;
+    g.sdd = c->sdd;
+    BasisConst &b = c->bc;
+    std::memset(&b, 0, sizeof(b));
+    for (int k = 0; k < c->K; k++) {
+        const float s0 = c->basis[3 * k], s1 = c->basis[3 * k + 1], s2 = c->basis[3 * k + 2];
+        b.S[3 * k] = s0;
+        b.S[3 * k + 1] = s1;
+        b.S[3 * k + 2] = s2;
+        b.S2[k] = s0 * s0 + s1 * s1 + s2 * s2;
+    }
+    for (int cond = 0; cond < c->C; cond++) {
+        /* G = Rotate * e_z = elemR[cond] * e_z for every view (Rz fixes e_z);
+         * |S . G| as ir.cu:1786, squared. */
+        const ViewFrame f = make_frame(c, cond, 0, false);
+        for (int k = 0; k < c->K; k++) {
+            const float h = std::fabs(b.S[3 * k] * f.ev[0] + b.S[3 * k + 1] * f.ev[1] + b.S[3 * k + 2] * f.ev[2]);
+            b.g[cond * c->K + k] = h * h;
+        }
+    }
+}
+
+/* Select the device, create the stream and upload the basis constants. */
+static xr_status ensure_device(xr_ctx *c) {
+    if (c->dev_ready) return cuda_check(c, cudaSetDevice(c->device), "cudaSetDevice");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= c->device) {
+        cudaGetLastError();
+        return fail(c, XR_ERR_NODEV, "no CUDA device available (libxr needs a B200, sm_100a)");
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess)
+        return fail(c, XR_ERR_NODEV, "cudaGetDeviceProperties failed");
+    if (prop.major != 10)
+        return fail(c, XR_ERR_NODEV, std::string("libxr is built for sm_100a; device is ") + prop.name + " sm_" +
+                                         std::to_string(prop.major) + std::to_string(prop.minor));
+    xr_status st = cuda_check(c, cudaSetDevice(c->device), "cudaSetDevice");
+    if (st) return st;
+    if (!c->own_stream) {
+        st = cuda_check(c, cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        if (st) return st;
+    }
+    if (!c->stream) c->stream = c->own_stream;
+    if ((st = ensure(c, c->basis_dev, sizeof(BasisConst), "basis"))) return st;
+    st = cuda_check(c, cudaMemcpy(c->basis_dev.p, &c->bc, sizeof(BasisConst), cudaMemcpyHostToDevice),
+                    "upload basis");
+    if (st) return st;
+    if (!c->h_loss) {
+        st = cuda_check(c, cudaMallocHost(&c->h_loss, kLossSlots * sizeof(double)), "cudaMallocHost");
+        if (st) return st;
+    }
+    if ((st = ensure(c, c->loss, kLossSlots * sizeof(double), "loss"))) return st;
+    c->dev_ready = true;
+    return XR_OK;
+}
+
+static const BasisConst *dbasis(xr_ctx *c) { return (const BasisConst *)c->basis_dev.p; }
+
+/* Frame table for the rotation direction and the normaliser L/(sum c + 1e-5)
+ * for every axis and view (geometry only; computed once per context). */
+static xr_status ensure_frames(xr_ctx *c, int rotation) {
+    xr_status st;
+    const size_t nf = (size_t)c->C * c->V;
+    if (c->frames_rotation != rotation) {
+        std::vector<ViewFrame> h(nf);
+        for (int cond = 0; cond < c->C; cond++)
+            for (int v = 0; v < c->V; v++) h[(size_t)cond * c->V + v] = make_frame(c, cond, rotation * v, false);
+        if ((st = ensure(c, c->frames, nf * sizeof(ViewFrame), "frames"))) return st;
+        st = cuda_check(c, cudaMemcpyAsync(c->frames.p, h.data(), nf * sizeof(ViewFrame), cudaMemcpyHostToDevice,
+                                           c->stream), "upload frames");
+        if (st) return st;
+        st = cuda_check(c, cudaStreamSynchronize(c->stream), "upload frames");
+        if (st) return st;
+        c->frames_rotation = rotation;
+        c->norm_valid = false;
+    }
+    if (!c->norm_valid) {
+        const size_t npx = nf * (size_t)c->Nd * c->Nd;
+        if ((st = ensure(c, c->norm, npx * sizeof(float), "normaliser"))) return st;
+        std::vector<int> all(c->V);
+        for (int v = 0; v < c->V; v++) all[v] = v;
+        DevBuf lst;
+        if ((st = ensure(c, lst, all.size() * sizeof(int), "view list"))) return st;
+        cudaMemcpyAsync(lst.p, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+        {
+            Timed t(c, XR_T_SETUP);
+            cudaMemsetAsync(c->norm.p, 0, npx * sizeof(float), c->stream);
+            st = cuda_check(c, launch_forward(c->gc, dbasis(c), (const ViewFrame *)c->frames.p, (const int *)lst.p,
+                                              c->V, 0, c->C, nullptr, (float *)c->norm.p, 2, c->views_per_cta,
+                                              c->stream), "weight splat");
+        }
+        if (!st) {
+            Timed t(c, XR_T_SETUP);
+            st = cuda_check(c, launch_chord(c->gc, (const ViewFrame *)c->frames.p, (float *)c->norm.p, c->C,
+                                            c->stream), "chord length");
+        }
+        cudaStreamSynchronize(c->stream);
+        release(lst);
+        if (st) return st;
+        c->norm_valid = true;
+    }
+    return XR_OK;
+}
+
+static xr_status check_xtt_k(xr_ctx *c) {
+    if (c->K > kMaxBasisXTT)
+        return fail(c, XR_ERR_ARG, "XTT paths support at most " + std::to_string(kMaxBasisXTT) +
+                                       " scattering vectors (got " + std::to_string(c->K) + ")");
+    return XR_OK;
+}
+
+static xr_status validate_scan(xr_ctx *c) {
+    if (!(c->sdd > 0 && c->sod > 0 && c->det > 0)) return fail(c, XR_ERR_ARG, "sdd, sod and det_size must be > 0");
+    if (c->N < 1 || c->N > 4096) return fail(c, XR_ERR_ARG, "num_voxel out of range [1, 4096]");
+    if (c->Nd < 2 || c->Nd > 16384) return fail(c, XR_ERR_ARG, "num_detect out of range [2, 16384]");
+    if (c->V < 1 || c->V > 65535) return fail(c, XR_ERR_ARG, "num_proj out of range [1, 65535]");
+    if (c->C < 1 || c->C > kMaxCond) return fail(c, XR_ERR_ARG, "num_cond out of range [1, 32]");
+    if (c->K < 1 || c->K > kMaxBasis) return fail(c, XR_ERR_ARG, "num_basis out of range [1, 32]");
+    if ((long)c->C * c->V > 65535) return fail(c, XR_ERR_ARG, "num_cond * num_proj must be <= 65535");
+    fill_consts(c);
+    return XR_OK;
+}
+
+/* ---------------------------------------------------------------- settings */
+
+static const JVal *need(const JVal *o, const char *key, std::string &err) {
+    const JVal *v = o ? o->get(key) : nullptr;
+    if (!v) err = std::string("settings: missing key \"") + key + "\"";
+    return v;
+}
+
+static bool floats(const JVal *v, std::vector<float> &out) {
+    if (!v || v->kind != JVal::Arr) return false;
+    out.clear();
+    for (const auto &e : v->a) {
+        if (e.kind != JVal::Num) return false;
+        out.push_back((float)e.n);
+    }
+    return true;
+}
+
+}  // namespace xr
+
+using namespace xr;
+
+extern "C" {
+
+const char *xr_version(void) { return "libxr 0.1 (sm_100a)"; }
+
+xr_status xr_create(const xr_scan *s, int device, xr_ctx **out) {
+    if (!s || !out) return XR_ERR_ARG;
+    *out = nullptr;
+    if (!s->rot || !s->trans || !s->offset || !s->basis) return XR_ERR_ARG;
+    if (s->num_cond < 1 || s->num_cond > kMaxCond || s->num_basis < 1 || s->num_basis > kMaxBasis) return XR_ERR_ARG;
+    xr_ctx *c = new xr_ctx();
+    c->device = device;
+    c->sdd = s->sdd;
+    c->sod = s->sod;
+    c->det = s->det_size;
+    c->N = s->num_voxel;
+    c->Nd = s->num_detect;
+    c->V = s->num_proj;
+    c->C = s->num_cond;
+    c->K = s->num_basis;
+    c->rot.assign(s->rot, s->rot + 9 * c->C);
+    c->trans.assign(s->trans, s->trans + 3 * c->C);
+    c->offset.assign(s->offset, s->offset + 3 * c->C);
+    c->basis.assign(s->basis, s->basis + 3 * c->K);
+    c->load_index.resize(c->C);
+    for (int i = 0; i < c->C; i++) c->load_index[i] = i + 1;
+    const xr_status st = validate_scan(c);
+    if (st) {
+        delete c;
+        return st;
+    }
+    *out = c;
+    return XR_OK;
+}
+
+/* init_params, params.cu:42-104. */
+xr_status xr_init_params(const char *json_path, const char *tag, int device, xr_ctx **out) {
+    if (!json_path || !tag || !out) return XR_ERR_ARG;
+    *out = nullptr;
+    std::ifstream f(json_path, std::ios::binary);
+    if (!f) return XR_ERR_IO;
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string text = ss.str();
+    JVal root;
+    std::string err;
+    JParser p(text.data(), text.data() + text.size());
+    if (!p.parse(root, err)) return XR_ERR_CONFIG;
+    const JVal *rv = need(&root, "recon_variable", err);
+    const JVal *t = need(&root, tag, err);
+    if (!rv || !t) return XR_ERR_CONFIG;
+    auto num = [&](const JVal *o, const char *k, double &d) -> bool {
+        const JVal *v = need(o, k, err);
+        if (!v || v->kind != JVal::Num) return false;
+        d = v->n;
+        return true;
+    };
+    auto str = [&](const JVal *o, const char *k, std::string &s) -> bool {
+        const JVal *v = need(o, k, err);
+        if (!v || v->kind != JVal::Str) return false;
+        s = v->s;
+        return true;
+    };
+    double vec, cond, sod, sdd, proj, ndu, ndv, det, nvox, rot;
+    std::string pp, vp, dp;
+    if (!str(t, "proj_path", pp) || !str(t, "vol_path", vp) || !str(t, "direc_path", dp)) return XR_ERR_CONFIG;
+    if (!num(rv, "vector", vec) || !num(rv, "condition", cond)) return XR_ERR_CONFIG;
+    if (!num(t, "sod", sod) || !num(t, "sdd", sdd) || !num(t, "proj", proj) || !num(t, "num_det_u", ndu) ||
+        !num(t, "num_det_v", ndv) || !num(t, "det_size", det) || !num(t, "num_voxel", nvox) || !num(t, "rot", rot))
+        return XR_ERR_CONFIG;
+    std::vector<float> mRot, vTrans, recon, offset, base;
+    if (!floats(need(t, "matrixRot", err), mRot) || !floats(need(t, "vecTrans", err), vTrans) ||
+        !floats(need(t, "areaTrans", err), recon) || !floats(need(t, "offset", err), offset) ||
+        !floats(need(rv, "base", err), base))
+        return XR_ERR_CONFIG;
+    const JVal *srt = t->get("sorting");
+    const bool sorting = srt && srt->kind == JVal::Bool && srt->b;
+    const int K = (int)vec, C = (int)cond, proj_cond = (int)rot;
+    if (K < 1 || K > kMaxBasis || C < 1 || C > kMaxCond || (int)base.size() < 3 * K || recon.size() < 3 ||
+        (int)vTrans.size() < 3 * proj_cond)
+        return XR_ERR_CONFIG;
+    for (int i = 0; i < proj_cond; i++)
+        for (int j = 0; j < 3; j++) vTrans[3 * i + j] += recon[j];
+    std::vector<float> R(9 * C), T(3 * C), O(3 * C);
+    std::vector<int> li(C);
+    if (sorting) {
+        std::vector<float> idx;
+        if (!floats(need(t, "index", err), idx) || (int)idx.size() < C) return XR_ERR_CONFIG;
+        for (int i = 0; i < C; i++) {
+            const int k = (int)idx[i];
+            if (k < 0 || 9 * k + 9 > (int)mRot.size() || 3 * k + 3 > (int)vTrans.size() ||
+                3 * k + 3 > (int)offset.size())
+                return XR_ERR_CONFIG;
+            li[i] = k + 1;
+            std::copy(&mRot[9 * k], &mRot[9 * k + 9], &R[9 * i]);
+            std::copy(&vTrans[3 * k], &vTrans[3 * k + 3], &T[3 * i]);
+            std::copy(&offset[3 * k], &offset[3 * k + 3], &O[3 * i]);
+        }
+    } else {
+        if ((int)mRot.size() < 9 * C || (int)vTrans.size() < 3 * C || (int)offset.size() < 3 * C)
+            return XR_ERR_CONFIG;
+        for (int i = 0; i < C; i++) li[i] = i + 1;
+        std::copy(mRot.begin(), mRot.begin() + 9 * C, R.begin());
+        std::copy(vTrans.begin(), vTrans.begin() + 3 * C, T.begin());
+        std::copy(offset.begin(), offset.begin() + 3 * C, O.begin());
+    }
+    xr_scan s;
+    s.sdd = (float)sdd;
+    s.sod = (float)sod;
+    s.det_size = (float)det;
+    s.num_voxel = (int)nvox;
+    s.num_detect = (int)ndu;
+    s.num_proj = (int)proj;
+    s.num_cond = C;
+    s.num_basis = K;
+    s.rot = R.data();
+    s.trans = T.data();
+    s.offset = O.data();
+    s.basis = base.data();
+    const xr_status st = xr_create(&s, device, out);
+    if (st) return st;
+    (*out)->proj_path = pp;
+    (*out)->vol_path = vp;
+    (*out)->direc_path = dp;
+    (*out)->load_index = li;
+    return XR_OK;
+}
+
+void xr_destroy(xr_ctx *c) {
+    if (!c) return;
+    if (c->dev_ready) {
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->stream);
+        timing_collect(c);
+        for (auto &pr : c->timing.pool) {
+            cudaEventDestroy(pr.first);
+            cudaEventDestroy(pr.second);
+        }
+    }
+    release(c->frames);
+    release(c->norm);
+    release(c->proj);
+    release(c->subsets);
+    release(c->loss);
+    release(c->scratch_vol);
+    release(c->scratch_sino);
+    release(c->scratch_md);
+    release(c->basis_dev);
+    release(c->fdk_frames);
+    release(c->fdk_filt);
+    release(c->fdk_weight);
+    release(c->fdk_sf);
+    if (c->h_loss) cudaFreeHost(c->h_loss);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+const char *xr_last_error(const xr_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+xr_status xr_get_scan(const xr_ctx *c, xr_scan *out) {
+    if (!c || !out) return XR_ERR_ARG;
+    out->sdd = c->sdd;
+    out->sod = c->sod;
+    out->det_size = c->det;
+    out->num_voxel = c->N;
+    out->num_detect = c->Nd;
+    out->num_proj = c->V;
+    out->num_cond = c->C;
+    out->num_basis = c->K;
+    out->rot = c->rot.data();
+    out->trans = c->trans.data();
+    out->offset = c->offset.data();
+    out->basis = c->basis.data();
+    return XR_OK;
+}
+
+xr_status xr_get_paths(const xr_ctx *c, const char **pp, const char **vp, const char **dp, int *li) {
+    if (!c) return XR_ERR_ARG;
+    if (pp) *pp = c->proj_path.c_str();
+    if (vp) *vp = c->vol_path.c_str();
+    if (dp) *dp = c->direc_path.c_str();
+    if (li) std::copy(c->load_index.begin(), c->load_index.end(), li);
+    return XR_OK;
+}
+
+xr_status xr_set_stream(xr_ctx *c, void *stream) {
+    if (!c) return XR_ERR_ARG;
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return XR_OK;
+}
+
+xr_status xr_set_option(xr_ctx *c, int key, int value) {
+    if (!c) return XR_ERR_ARG;
+    switch (key) {
+        case XR_OPT_TIMING: c->timing.on = value != 0; return XR_OK;
+        case XR_OPT_FDK_AXIS_BLOCKS: c->fdk_axis_blocks = value != 0; return XR_OK;
+        case XR_OPT_VIEWS_PER_CTA:
+            if (value < 0 || value > 64) return fail(c, XR_ERR_ARG, "views per CTA must be in [0, 64]");
+            c->views_per_cta = value;
+            return XR_OK;
+        case XR_OPT_STORAGE:
+            if (value != 0) return fail(c, XR_ERR_ARG, "only FP32 storage (0) is available");
+            c->storage = value;
+            return XR_OK;
+        default: return fail(c, XR_ERR_ARG, "unknown option " + std::to_string(key));
+    }
+}
+
+xr_status xr_get_timings(const xr_ctx *cc, xr_timings *out) {
+    xr_ctx *c = const_cast<xr_ctx *>(cc);
+    if (!c || !out) return XR_ERR_ARG;
+    if (c->dev_ready) timing_collect(c);
+    for (int k = 0; k < XR_T_COUNT; k++) {
+        out->ms[k] = c->timing.ms[k];
+        out->launches[k] = c->timing.launches[k];
+    }
+    return XR_OK;
+}
+
+xr_status xr_reset_timings(xr_ctx *c) {
+    if (!c) return XR_ERR_ARG;
+    if (c->dev_ready) timing_collect(c);
+    for (int k = 0; k < XR_T_COUNT; k++) {
+        c->timing.ms[k] = 0;
+        c->timing.launches[k] = 0;
+    }
+    return XR_OK;
+}
+
+/* ------------------------------------------------------------- sessions */
+
+xr_status xr_dev_session_begin(xr_ctx *c, const float *d_sino, float *d_vol, int xtt, int epochs, int batch,
+                               xr_rotate dir, xr_method method, float lambda) {
+    if (!c || !d_sino || !d_vol) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    if (batch < 1 || batch > c->V) return fail(c, XR_ERR_ARG, "batch must be in [1, num_proj]");
+    if (method != XR_METHOD_MLEM && method != XR_METHOD_ART && method != XR_METHOD_XTT)
+        return fail(c, XR_ERR_ARG, "method must be MLEM or ART");
+    if (dir != XR_ROTATE_CW && dir != XR_ROTATE_CCW) return fail(c, XR_ERR_ARG, "bad rotate");
+    if (epochs < 0) return fail(c, XR_ERR_ARG, "epochs must be >= 0");
+    xr_status st;
+    if (xtt && (st = check_xtt_k(c))) return st;
+    if ((st = ensure_device(c))) return st;
+    const int rotation = dir == XR_ROTATE_CW ? 1 : -1;
+    if ((st = ensure_frames(c, rotation))) return st;
+    Session &s = c->sess;
+    s = Session();
+    s.xtt = xtt != 0;
+    s.epochs = epochs;
+    s.batch = batch;
+    s.subset_size = (c->V + batch - 1) / batch;      /* reconstruct.cu:61 / :842 */
+    s.rotation = rotation;
+    s.art = method == XR_METHOD_ART;
+    s.lambda = lambda;
+    s.d_sino = d_sino;
+    s.d_vol = d_vol;
+    std::vector<int> lists((size_t)batch * s.subset_size);
+    for (int sub = 0; sub < batch; sub++)
+        for (int j = 0; j < s.subset_size; j++)   /* n = (sub + batch*j) % nProj, reconstruct.cu:89 */
+            lists[(size_t)sub * s.subset_size + j] = (int)(((long)sub + (long)batch * j) % c->V);
+    if ((st = ensure(c, c->subsets, lists.size() * sizeof(int), "subset lists"))) return st;
+    st = cuda_check(c, cudaMemcpyAsync(c->subsets.p, lists.data(), lists.size() * sizeof(int),
+                                       cudaMemcpyHostToDevice, c->stream), "upload subsets");
+    if (st) return st;
+    const size_t npx = (size_t)c->C * c->V * c->Nd * c->Nd;
+    if ((st = ensure(c, c->proj, npx * sizeof(float), "projections"))) return st;
+    s.order.resize(batch);
+    for (int i = 0; i < batch; i++) s.order[i] = i;
+    if (!s.xtt) {
+        /* IR: one engine for the whole run, shuffled once per (axis, epoch),
+         * axis-major (reconstruct.cu:75-81). */
+        std::mt19937_64 eng;
+        s.ir_orders.resize((size_t)c->C * epochs * batch);
+        std::vector<int> o = s.order;
+        for (long r = 0; r < (long)c->C * epochs; r++) {
+            std::shuffle(o.begin(), o.end(), eng);
+            std::copy(o.begin(), o.end(), s.ir_orders.begin() + r * batch);
+        }
+    }
+    st = cuda_check(c, cudaStreamSynchronize(c->stream), "session begin");
+    if (st) return st;
+    s.active = true;
+    return XR_OK;
+}
+
+xr_status xr_dev_session_epoch(xr_ctx *c, double *loss) {
+    if (!c) return XR_ERR_ARG;
+    Session &s = c->sess;
+    if (!s.active) return fail(c, XR_ERR_STATE, "no active session (call xr_dev_session_begin)");
+    if (!s.xtt && s.epoch_done >= s.epochs)
+        return fail(c, XR_ERR_STATE, "IR session: all planned epochs already run");
+    xr_status st;
+    cudaStream_t str = c->stream;
+    const size_t NdNd = (size_t)c->Nd * c->Nd;
+    const size_t blk = (size_t)c->V * NdNd;
+    const size_t N3 = (size_t)c->N * c->N * c->N;
+    const float alpha = s.lambda / (float)s.subset_size;   /* reconstruct.cu:124 / :906 */
+    const ViewFrame *fr = (const ViewFrame *)c->frames.p;
+    float *proj = (float *)c->proj.p;
+    const float *norm = (const float *)c->norm.p;
+    double *dl = (double *)c->loss.p;
+    cudaMemsetAsync(dl, 0, kMaxCond * sizeof(double), str);
+    if (s.xtt) {
+        /* XTT::reconstruct epoch, reconstruct.cu:857-917: a fresh default
+         * engine shuffles the persistent order; the ratio images of every
+         * axis are cleared once per epoch. */
+        std::mt19937_64 eng;
+        std::shuffle(s.order.begin(), s.order.end(), eng);
+        cudaMemsetAsync(proj, 0, (size_t)c->C * blk * sizeof(float), str);
+        for (int b = 0; b < s.batch; b++) {
+            const int *vl = (const int *)c->subsets.p + (size_t)s.order[b] * s.subset_size;
+            {
+                Timed t(c, XR_T_FORWARD);
+                if ((st = cuda_check(c, launch_forward(c->gc, dbasis(c), fr, vl, s.subset_size, 0, c->C, s.d_vol,
+                                                       proj, 1, c->views_per_cta, str), "XTT forward")))
+                    return st;
+            }
+            {
+                Timed t(c, XR_T_RATIO);
+                if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, norm, s.d_sino, s.art,
+                                                     dl, str), "ratio")))
+                    return st;
+            }
+            {
+                Timed t(c, XR_T_BACK);
+                if ((st = cuda_check(c, launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, 0, c->C, proj,
+                                                           s.d_vol, 1, s.art, alpha, str), "XTT back")))
+                    return st;
+            }
+        }
+    } else {
+        /* IR::reconstruct epoch (reconstruct.cu:80-132) of every axis. */
+        for (int cond = 0; cond < c->C; cond++) {
+            const int *order = &s.ir_orders[((size_t)cond * s.epochs + s.epoch_done) * s.batch];
+            float *pc = proj + (size_t)cond * blk;
+            float *vc = s.d_vol + (size_t)cond * N3;
+            cudaMemsetAsync(pc, 0, blk * sizeof(float), str);
+            for (int b = 0; b < s.batch; b++) {
+                const int *vl = (const int *)c->subsets.p + (size_t)order[b] * s.subset_size;
+                {
+                    Timed t(c, XR_T_FORWARD);
+                    if ((st = cuda_check(c, launch_forward(c->gc, dbasis(c), fr, vl, s.subset_size, cond, 1, vc,
+                                                           proj, 0, c->views_per_cta, str), "forward")))
+                        return st;
+                }
+                {
+                    Timed t(c, XR_T_RATIO);
+                    if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, 1, pc, norm + (size_t)cond * blk,
+                                                         s.d_sino + (size_t)cond * blk, s.art, dl + cond,
+                                                         str), "ratio")))
+                        return st;
+                }
+                {
+                    Timed t(c, XR_T_BACK);
+                    if ((st = cuda_check(c, launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, cond, 1,
+                                                               proj, vc, 0, s.art, alpha, str), "back")))
+                        return st;
+                }
+            }
+        }
+    }
+    s.epoch_done++;
+    if (loss) {
+        st = cuda_check(c, cudaMemcpyAsync(c->h_loss, dl, kMaxCond * sizeof(double), cudaMemcpyDeviceToHost, str),
+                        "loss copy");
+        if (st) return st;
+        if ((st = cuda_check(c, cudaStreamSynchronize(str), "epoch"))) return st;
+        if (s.xtt) {
+            loss[0] = c->h_loss[0];
+        } else {
+            for (int cond = 0; cond < c->C; cond++) loss[cond] = c->h_loss[cond];
+        }
+    }
+    return cuda_check(c, cudaGetLastError(), "epoch");
+}
+
+xr_status xr_dev_session_end(xr_ctx *c, float *d_md, float *d_ev) {
+    if (!c) return XR_ERR_ARG;
+    Session &s = c->sess;
+    if (!s.active) return fail(c, XR_ERR_STATE, "no active session");
+    xr_status st = XR_OK;
+    if (s.xtt) {
+        const long nvox = (long)c->N * c->N * c->N;
+        {
+            Timed t(c, XR_T_ORIENT);
+            st = cuda_check(c, launch_sqrt_abs(nvox * c->K, s.d_vol, c->stream), "sqrt");   /* reconstruct.cu:919-922 */
+        }
+        if (!st && d_md) {
+            Timed t(c, XR_T_ORIENT);
+            st = cuda_check(c, launch_orientation(nvox, c->K, dbasis(c), s.d_vol, d_md, d_ev, c->stream),
+                            "orientation");
+        }
+    }
+    if (!st) st = cuda_check(c, cudaStreamSynchronize(c->stream), "session end");
+    s.active = false;
+    return st;
+}
+
+xr_status xr_dev_session_proj(xr_ctx *c, const float **d_proj) {
+    if (!c || !d_proj) return XR_ERR_ARG;
+    *d_proj = (const float *)c->proj.p;
+    return XR_OK;
+}
+
+/* ---------------------------------------------------- device-buffer calls */
+
+static xr_status forward_into(xr_ctx *c, const float *d_vol, float *d_out, int rotation, int mode, bool normalise) {
+    xr_status st;
+    if ((st = ensure_frames(c, rotation))) return st;
+    const size_t npx = (size_t)c->C * c->V * c->Nd * c->Nd;
+    std::vector<int> all(c->V);
+    for (int v = 0; v < c->V; v++) all[v] = v;
+    DevBuf lst;
+    if ((st = ensure(c, lst, all.size() * sizeof(int), "view list"))) return st;
+    cudaMemcpyAsync(lst.p, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    cudaMemsetAsync(d_out, 0, npx * sizeof(float), c->stream);
+    {
+        Timed t(c, XR_T_FORWARD);
+        st = cuda_check(c, launch_forward(c->gc, dbasis(c), (const ViewFrame *)c->frames.p, (const int *)lst.p,
+                                          c->V, 0, c->C, d_vol, d_out, mode, c->views_per_cta, c->stream),
+                        "forward");
+    }
+    if (!st && normalise) {
+        Timed t(c, XR_T_OTHER);
+        st = cuda_check(c, launch_normalize(c->gc, c->C, d_out, (const float *)c->norm.p, c->stream), "normalise");
+    }
+    cudaStreamSynchronize(c->stream);
+    release(lst);
+    return st;
+}
+
+xr_status xr_dev_forward(xr_ctx *c, const float *d_vol, float *d_sino, xr_rotate dir, int xtt) {
+    if (!c || !d_vol || !d_sino) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    xr_status st;
+    if (xtt && (st = check_xtt_k(c))) return st;
+    if ((st = ensure_device(c))) return st;
+    return forward_into(c, d_vol, d_sino, dir == XR_ROTATE_CCW ? -1 : 1, xtt ? 1 : 0, true);
+}
+
+xr_status xr_dev_residual(xr_ctx *c, const float *d_vol, const float *d_sino, xr_rotate dir, int xtt,
+                          double *rel_l2, double *l1) {
+    if (!c || !d_vol || !d_sino) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    xr_status st;
+    if (xtt && (st = check_xtt_k(c))) return st;
+    if ((st = ensure_device(c))) return st;
+    const size_t npx = (size_t)c->C * c->V * c->Nd * c->Nd;
+    if ((st = ensure(c, c->scratch_sino, npx * sizeof(float), "residual scratch"))) return st;
+    float *p = (float *)c->scratch_sino.p;
+    if ((st = forward_into(c, d_vol, p, dir == XR_ROTATE_CCW ? -1 : 1, xtt ? 1 : 0, true))) return st;
+    double *dl = (double *)c->loss.p + 40;
+    cudaMemsetAsync(dl, 0, 3 * sizeof(double), c->stream);
+    {
+        Timed t(c, XR_T_OTHER);
+        if ((st = cuda_check(c, launch_residual((long)npx, p, d_sino, dl, c->stream), "residual"))) return st;
+    }
+    if ((st = cuda_check(c, cudaMemcpyAsync(c->h_loss, dl, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+                         "residual copy")))
+        return st;
+    if ((st = cuda_check(c, cudaStreamSynchronize(c->stream), "residual"))) return st;
+    if (rel_l2) *rel_l2 = c->h_loss[1] > 0 ? std::sqrt(c->h_loss[0] / c->h_loss[1]) : 0.0;
+    if (l1) *l1 = c->h_loss[2];
+    return XR_OK;
+}
+
+xr_status xr_dev_orientation(xr_ctx *c, const float *d_mu, float *d_md, float *d_ev) {
+    if (!c || !d_mu || !d_md) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    {
+        Timed t(c, XR_T_ORIENT);
+        st = cuda_check(c, launch_orientation((long)c->N * c->N * c->N, c->K, dbasis(c), d_mu, d_md, d_ev,
+                                              c->stream), "orientation");
+    }
+    if (!st) st = cuda_check(c, cudaStreamSynchronize(c->stream), "orientation");
+    return st;
+}
+
+/* ------------------------------------------------------ host-buffer calls */
+
+static xr_status upload_planes(xr_ctx *c, DevBuf &b, const float *const *src, int planes, size_t plane_elems,
+                               const char *what) {
+    for (int i = 0; i < planes; i++)
+        if (!src[i]) return fail(c, XR_ERR_ARG, std::string("null host pointer: ") + what);
+    xr_status st;
+    if ((st = ensure(c, b, (size_t)planes * plane_elems * sizeof(float), what))) return st;
+    for (int i = 0; i < planes; i++) {
+        st = cuda_check(c, cudaMemcpyAsync((float *)b.p + i * plane_elems, src[i], plane_elems * sizeof(float),
+                                           cudaMemcpyHostToDevice, c->stream), what);
+        if (st) return st;
+    }
+    return XR_OK;
+}
+
+static xr_status download_planes(xr_ctx *c, const float *d, float *const *dst, int planes, size_t plane_elems,
+                                 const char *what) {
+    for (int i = 0; i < planes; i++) {
+        if (!dst[i]) return fail(c, XR_ERR_ARG, std::string("null host pointer: ") + what);
+        xr_status st = cuda_check(c, cudaMemcpyAsync(dst[i], d + i * plane_elems, plane_elems * sizeof(float),
+                                                     cudaMemcpyDeviceToHost, c->stream), what);
+        if (st) return st;
+    }
+    return cuda_check(c, cudaStreamSynchronize(c->stream), what);
+}
+
+xr_status xr_forward(xr_ctx *c, const float *const *voxel, float *const *sino, xr_rotate dir, int xtt) {
+    if (!c || !voxel || !sino) return c ? fail(c, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
+    xr_status st;
+    if (xtt && (st = check_xtt_k(c))) return st;
+    if ((st = ensure_device(c))) return st;
+    const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
+    if ((st = upload_planes(c, c->scratch_vol, voxel, xtt ? c->K : 1, N3, "volume"))) return st;
+    if ((st = ensure(c, c->scratch_sino, c->C * blk * sizeof(float), "sinogram"))) return st;
+    if ((st = forward_into(c, (const float *)c->scratch_vol.p, (float *)c->scratch_sino.p,
+                           dir == XR_ROTATE_CCW ? -1 : 1, xtt ? 1 : 0, true)))
+        return st;
+    return download_planes(c, (const float *)c->scratch_sino.p, sino, c->C, blk, "sinogram");
+}
+
+/* forwardProjOnly, reconstruct.cu:1890-1949: plain splat of channel 0, no
+ * normalisation (the reference passes a null weight buffer there, which
+ * faults; the weights are simply not accumulated here). */
+xr_status xr_forward_proj_only(xr_ctx *c, const float *const *voxel, float *const *sino, xr_rotate dir) {
+    if (!c || !voxel || !sino) return c ? fail(c, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
+    if ((st = upload_planes(c, c->scratch_vol, voxel, 1, N3, "volume"))) return st;
+    if ((st = ensure(c, c->scratch_sino, c->C * blk * sizeof(float), "sinogram"))) return st;
+    if ((st = forward_into(c, (const float *)c->scratch_vol.p, (float *)c->scratch_sino.p,
+                           dir == XR_ROTATE_CCW ? -1 : 1, 0, false)))
+        return st;
+    return download_planes(c, (const float *)c->scratch_sino.p, sino, c->C, blk, "sinogram");
+}
+
+xr_status xr_ir_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel, int epoch, int batch,
+                            xr_rotate dir, xr_method method, float lambda, float *losses) {
+    if (!c || !sino || !voxel) return c ? fail(c, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
+    if (epoch < 0) return fail(c, XR_ERR_ARG, "epoch must be >= 0");
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
+    if ((st = upload_planes(c, c->scratch_sino, sino, c->C, blk, "sinogram"))) return st;
+    if ((st = upload_planes(c, c->scratch_vol, voxel, c->C, N3, "volume"))) return st;
+    if ((st = xr_dev_session_begin(c, (const float *)c->scratch_sino.p, (float *)c->scratch_vol.p, 0, epoch, batch,
+                                   dir, method, lambda)))
+        return st;
+    std::vector<double> l(c->C);
+    for (int ep = 0; ep < epoch; ep++) {
+        if ((st = xr_dev_session_epoch(c, losses ? l.data() : nullptr))) return st;
+        if (losses)
+            for (int cond = 0; cond < c->C; cond++) losses[(size_t)cond * epoch + ep] = (float)l[cond];
+    }
+    if ((st = xr_dev_session_end(c, nullptr, nullptr))) return st;
+    return download_planes(c, (const float *)c->scratch_vol.p, voxel, c->C, N3, "volume");
+}
+
+xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel, float *const *md,
+                             float *const *evalue, int epoch, int batch, xr_rotate dir, xr_method method,
+                             float lambda, float *losses) {
+    if (!c || !sino || !voxel) return c ? fail(c, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
+    if (epoch < 0) return fail(c, XR_ERR_ARG, "epoch must be >= 0");
+    xr_status st;
+    if ((st = check_xtt_k(c))) return st;
+    if ((st = ensure_device(c))) return st;
+    const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
+    if ((st = upload_planes(c, c->scratch_sino, sino, c->C, blk, "sinogram"))) return st;
+    if ((st = upload_planes(c, c->scratch_vol, voxel, c->K, N3, "volume"))) return st;
+    if ((st = xr_dev_session_begin(c, (const float *)c->scratch_sino.p, (float *)c->scratch_vol.p, 1, epoch, batch,
+                                   dir, method, lambda)))
+        return st;
+    for (int ep = 0; ep < epoch; ep++) {
+        double l = 0;
+        if ((st = xr_dev_session_epoch(c, losses ? &l : nullptr))) return st;
+        if (losses) losses[ep] = (float)l;
+    }
+    float *d_md = nullptr, *d_ev = nullptr;
+    if (md) {
+        if ((st = ensure(c, c->scratch_md, 6 * N3 * sizeof(float), "orientation"))) return st;
+        d_md = (float *)c->scratch_md.p;
+        d_ev = evalue ? d_md + 3 * N3 : nullptr;
+    }
+    if ((st = xr_dev_session_end(c, d_md, d_ev))) return st;
+    if ((st = download_planes(c, (const float *)c->scratch_vol.p, voxel, c->K, N3, "volume"))) return st;
+    if ((st = download_planes(c, (const float *)c->proj.p, sino, c->C, blk, "ratio images"))) return st;
+    if (md) {
+        if ((st = download_planes(c, d_md, md, 3, N3, "md"))) return st;
+        if (evalue && (st = download_planes(c, d_ev, evalue, 3, N3, "evalue"))) return st;
+    }
+    return XR_OK;
+}
+
+xr_status xr_orientation(xr_ctx *c, const float *const *mu, float *const *md, float *const *evalue) {
+    if (!c || !mu || !md) return c ? fail(c, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    const size_t N3 = (size_t)c->N * c->N * c->N;
+    if ((st = upload_planes(c, c->scratch_vol, mu, c->K, N3, "mu"))) return st;
+    if ((st = ensure(c, c->scratch_md, 6 * N3 * sizeof(float), "orientation"))) return st;
+    float *d_md = (float *)c->scratch_md.p;
+    float *d_ev = evalue ? d_md + 3 * N3 : nullptr;
+    if ((st = xr_dev_orientation(c, (const float *)c->scratch_vol.p, d_md, d_ev))) return st;
+    if ((st = download_planes(c, d_md, md, 3, N3, "md"))) return st;
+    if (evalue) return download_planes(c, d_ev, evalue, 3, N3, "evalue");
+    return XR_OK;
+}
+
+xr_status xr_angle_from_md(xr_ctx *c, const float *const *md, float *const *angle) {
+    if (!c || !md || !angle) return c ? fail(c, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    const size_t N3 = (size_t)c->N * c->N * c->N;
+    if ((st = upload_planes(c, c->scratch_vol, md, 3, N3, "md"))) return st;
+    if ((st = ensure(c, c->scratch_md, 6 * N3 * sizeof(float), "angle"))) return st;
+    {
+        Timed t(c, XR_T_ORIENT);
+        if ((st = cuda_check(c, launch_angle_from_md((long)N3, (const float *)c->scratch_vol.p,
+                                                     (float *)c->scratch_md.p, c->stream), "angle")))
+            return st;
+    }
+    return download_planes(c, (const float *)c->scratch_md.p, angle, 2, N3, "angle");
+}
+
+xr_status xr_direction_normalization(xr_ctx *c, float *const *md) {
+    if (!c || !md) return c ? fail(c, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    const size_t N3 = (size_t)c->N * c->N * c->N;
+    if ((st = upload_planes(c, c->scratch_vol, (const float *const *)md, 3, N3, "md"))) return st;
+    {
+        Timed t(c, XR_T_ORIENT);
+        if ((st = cuda_check(c, launch_direction_normalization((long)N3, (float *)c->scratch_vol.p, c->stream),
+                             "normalise")))
+            return st;
+    }
+    return download_planes(c, (const float *)c->scratch_vol.p, md, 3, N3, "md");
+}
+
+xr_status xr_residual(xr_ctx *c, const float *const *voxel, const float *const *sino, xr_rotate dir, int xtt,
+                      double *rel_l2, double *l1) {
+    if (!c || !voxel || !sino) return c ? fail(c, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
+    xr_status st;
+    if (xtt && (st = check_xtt_k(c))) return st;
+    if ((st = ensure_device(c))) return st;
+    const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
+    if ((st = upload_planes(c, c->scratch_vol, voxel, xtt ? c->K : 1, N3, "volume"))) return st;
+    DevBuf b;
+    if ((st = upload_planes(c, b, sino, c->C, blk, "sinogram"))) return st;
+    st = xr_dev_residual(c, (const float *)c->scratch_vol.p, (const float *)b.p, dir, xtt, rel_l2, l1);
+    release(b);
+    return st;
+}
+
+/* FDK::reconstruct, reconstruct.cu:1651-1724. */
+xr_status xr_fdk_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel, xr_rotate dir, xr_filter filter) {
+    if (!c || !sino || !voxel) return c ? fail(c, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
+    if (filter != XR_FILTER_REFERENCE && filter != XR_FILTER_RAMLAK) return fail(c, XR_ERR_ARG, "bad filter");
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    xr_ctx &x = *c;
+    const int rotation = dir == XR_ROTATE_CCW ? -1 : 1;
+    const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
+    if (x.fdk_rotation != rotation) {
+        std::vector<ViewFrame> h((size_t)c->C * c->V);
+        for (int cond = 0; cond < c->C; cond++)
+            for (int v = 0; v < c->V; v++) h[(size_t)cond * c->V + v] = make_frame(c, cond, rotation * v, true);
+        if ((st = ensure(c, x.fdk_frames, h.size() * sizeof(ViewFrame), "fdk frames"))) return st;
+        cudaMemcpy(x.fdk_frames.p, h.data(), h.size() * sizeof(ViewFrame), cudaMemcpyHostToDevice);
+        x.fdk_rotation = rotation;
+    }
+    /* filter table, reconstruct.cu:1694-1698 (or Ram-Lak in the same scaling) */
+    std::vector<float> filt(c->Nd);
+    const float d = c->det * (c->sod / c->sdd);
+    for (int k = 0; k < c->Nd; k++) {
+        if (filter == XR_FILTER_REFERENCE) {
+            filt[k] = 1.0f / (float)(M_PI * M_PI * d * (1.0f - 4.0f * (float)(k * k)));
+        } else {
+            if (k == 0) filt[k] = 1.0f / (8.0f * d);
+            else if (k % 2) filt[k] = -1.0f / (2.0f * (float)(M_PI * M_PI) * (float)((long)k * k) * d);
+            else filt[k] = 0.0f;
+        }
+    }
+    if ((st = ensure(c, x.fdk_filt, filt.size() * sizeof(float), "filter"))) return st;
+    cudaMemcpyAsync(x.fdk_filt.p, filt.data(), filt.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+    if ((st = ensure(c, x.fdk_weight, (size_t)c->Nd * c->Nd * sizeof(float), "weight"))) return st;
+    if ((st = upload_planes(c, c->scratch_sino, (const float *const *)sino, c->C, blk, "sinogram"))) return st;
+    if ((st = ensure(c, x.fdk_sf, c->C * blk * sizeof(float), "filtered"))) return st;
+    if ((st = ensure(c, c->scratch_vol, c->C * N3 * sizeof(float), "volume"))) return st;
+    {
+        Timed t(c, XR_T_FDK);
+        st = cuda_check(c, launch_fdk(c->gc, (const ViewFrame *)x.fdk_frames.p, c->C,
+                                      (const float *)c->scratch_sino.p, (float *)x.fdk_sf.p,
+                                      (float *)c->scratch_vol.p, (const float *)x.fdk_filt.p,
+                                      (float *)x.fdk_weight.p, c->fdk_axis_blocks, c->stream), "fdk");
+    }
+    if (st) return st;
+    if ((st = download_planes(c, (const float *)c->scratch_vol.p, voxel, c->C, N3, "volume"))) return st;
+    return download_planes(c, (const float *)x.fdk_sf.p, sino, c->C, blk, "filtered sinogram");
+}
+
+}  // extern "C"

@@ -1,0 +1,176 @@
+/*
+ * Internal types of libxr: the context, the per-view geometry table and the
+ * kernel launchers shared by the host code (xr_host.cpp) and the device code
+ * (xr_kernels.cu, xr_fdk.cu, xr_orient.cu).
+ */
+#ifndef XR_INTERNAL_H
+#define XR_INTERNAL_H
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/xr.h"
+
+namespace xr {
+
+constexpr int kMaxCond = 32;
+constexpr int kMaxBasis = 32;
+constexpr int kLossSlots = 64;   /* [0, 32): per-axis epoch losses; [40, 43): residual sums */
+
+/* Per-(axis, view) constants of the reference's rayCasting (ir.cu:1860-1879),
+ * computed once on the host with the reference's float operations.  The
+ * kernels then repeat only the per-voxel part, op for op. */
+struct ViewFrame {
+    float src[3];  /* Rotate * (0, +-sod, 0)                        */
+    float ss;      /* src . src                                     */
+    float eu[3];   /* Rotate * (1,0,0): detector u axis (column 0)  */
+    float e1x;     /* column 1 of Rotate (x)                        */
+    float ev[3];   /* Rotate * (0,0,1): detector v axis == grating  */
+    float e1y;     /* column 1 of Rotate (y)                        */
+    float off[3];  /* Rotate * INIT_OFFSET[cond]                    */
+    float e1z;     /* column 1 of Rotate (z)                        */
+    float t[3];    /* elemT[cond]                                   */
+    int view;      /* |n|: the view's index in the sinogram         */
+};
+static_assert(sizeof(ViewFrame) == 80, "ViewFrame layout");
+
+/* Scalars every kernel needs (copied by value into kernel parameters). */
+struct GeomConst {
+    int N, Nd, V, C, K;
+    float vs;      /* voxSize = sod*det/sdd (geometry.h:13)          */
+    float mag;     /* sdd / sod                                      */
+    float det;     /* detector pitch                                 */
+    float half;    /* 0.5f * Nd                                      */
+    float lim;     /* (float)Nd - 0.55f: detector window             */
+    float ratio;   /* vs^2 / (det*(sod/sdd)*det*(sod/sdd)) (ir.cu:1513) */
+    float sod, sdd;
+};
+
+/* XTT basis constants: S_k, |S_k|^2 and g_kc = |S_k . G_c|^2 where
+ * G_c = elemR[c] * e_z is the grating axis of axis c (the same for every view
+ * of an axis: Rz(theta) leaves e_z fixed). */
+struct BasisConst {
+    float S[3 * kMaxBasis];
+    float S2[kMaxBasis];
+    float g[kMaxCond * kMaxBasis];  /* g[c*K + k] */
+};
+
+struct Timing {
+    bool on = false;
+    double ms[XR_T_COUNT] = {};
+    long launches[XR_T_COUNT] = {};
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[XR_T_COUNT];
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+};
+
+/* A device allocation owned by the context. */
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Session {
+    bool active = false;
+    bool xtt = true;
+    int epochs = 0, epoch_done = 0, batch = 1, subset_size = 1;
+    int rotation = 1;
+    bool art = false;
+    float lambda = 0.f;
+    const float *d_sino = nullptr;
+    float *d_vol = nullptr;
+    std::vector<int> order;            /* persistent subset order (XTT)     */
+    std::vector<int> ir_orders;        /* C*epochs rows (IR)                */
+};
+
+}  // namespace xr
+
+struct xr_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    std::string err;
+
+    float sdd = 0, sod = 0, det = 0;
+    int N = 0, Nd = 0, V = 0, C = 0, K = 0;
+    std::vector<float> rot, trans, offset, basis;
+    std::string proj_path, vol_path, direc_path;
+    std::vector<int> load_index;
+
+    int fdk_axis_blocks = 0;
+    int views_per_cta = 0;
+    int storage = 0;
+
+    xr::GeomConst gc{};
+    xr::BasisConst bc{};
+    xr::Timing timing;
+
+    /* device workspace */
+    int frames_rotation = 0;           /* rotation the frame table holds (0: none) */
+    xr::DevBuf frames;                 /* C*V ViewFrame, n = rotation * view        */
+    xr::DevBuf norm;                   /* C*V*Nd*Nd: L / (sum c + 1e-5)            */
+    bool norm_valid = false;
+    xr::DevBuf proj;                   /* C*V*Nd*Nd: forward / ratio images         */
+    xr::DevBuf subsets;                /* batch*subset_size view indices            */
+    xr::DevBuf loss;                   /* doubles: loss accumulators                */
+    xr::DevBuf scratch_vol, scratch_sino, scratch_md;
+    xr::DevBuf basis_dev;              /* BasisConst                                */
+    xr::DevBuf fdk_frames;             /* C*V ViewFrame with the FDK source         */
+    int fdk_rotation = 0;
+    xr::DevBuf fdk_filt, fdk_weight, fdk_sf;
+    bool dev_ready = false;
+    double *h_loss = nullptr;          /* pinned, kLossSlots doubles                */
+
+    xr::Session sess;
+};
+
+namespace xr {
+
+/* ---- host helpers (xr_host.cpp) ---- */
+xr_status fail(xr_ctx *c, xr_status st, const std::string &msg);
+xr_status cuda_check(xr_ctx *c, cudaError_t e, const char *what);
+xr_status ensure(xr_ctx *c, DevBuf &b, size_t bytes, const char *what);
+void timing_begin(xr_ctx *c, int cls, cudaEvent_t *ev);
+void timing_end(xr_ctx *c, int cls, cudaEvent_t ev);
+
+/* ---- kernel launchers (xr_kernels.cu) ---- */
+/* Forward splat of one set of views (all listed views of every listed axis).
+ * mode 0: plain, value = ratio * vol[0]; mode 1: XTT K channels; mode 2:
+ * weights only (value 1, the reference's devProjFactor).  out: C blocks of
+ * V*Nd*Nd, accumulated with float atomics. */
+cudaError_t launch_forward(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
+                           const int *view_list, int n_views, int cond0, int n_cond, const float *vol,
+                           float *out, int mode, int views_per_cta, cudaStream_t s);
+/* Chord-length normaliser: norm = L / (norm + 1e-5) in place, every view. */
+cudaError_t launch_chord(const GeomConst &g, const ViewFrame *frames, float *norm, int n_cond, cudaStream_t s);
+/* Normalise + ratio (MLEM) or subtract (ART) on listed views of every axis,
+ * FP64 loss sum added to *loss. */
+cudaError_t launch_ratio(const GeomConst &g, const int *view_list, int n_views, int n_cond, float *proj,
+                         const float *norm, const float *sino, int art, double *loss, cudaStream_t s);
+/* Normalise only (proj *= norm) on every view: the forward operator A. */
+cudaError_t launch_normalize(const GeomConst &g, int n_cond, float *proj, const float *norm, cudaStream_t s);
+/* Back-projection of the listed views fused with the MLEM / ART update. */
+cudaError_t launch_back_update(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
+                               const int *view_list, int n_views, int cond0, int n_cond, const float *proj,
+                               float *vol, int xtt, int art, float alpha, cudaStream_t s);
+/* FP64 sums: out[0] += sum (p-b)^2, out[1] += sum b^2, out[2] += sum |p-b|. */
+cudaError_t launch_residual(long n, const float *p, const float *b, double *out, cudaStream_t s);
+/* mu = sqrt|mu| over n values. */
+cudaError_t launch_sqrt_abs(long n, float *mu, cudaStream_t s);
+
+/* ---- xr_orient.cu ---- */
+cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, const float *mu, float *md,
+                               float *ev, cudaStream_t s);
+cudaError_t launch_angle_from_md(long nvox, const float *md, float *angle, cudaStream_t s);
+cudaError_t launch_direction_normalization(long nvox, float *md, cudaStream_t s);
+
+/* ---- xr_fdk.cu ---- */
+cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_cond, const float *sino,
+                       float *sino_filt, float *vol, const float *filt, float *weight, int axis_blocks,
+                       cudaStream_t s);
+
+}  // namespace xr
+
+#endif
