@@ -39,6 +39,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "xray-directional-reconstruction_b200")
 
 W = dict(N=256, Nd=384, V=180, C=3, K=13, batch=5, sdd=1000.0, sod=500.0, det=2.0, n_fibers=12, seed=5)
+# --size profile: the same kernels on a smaller case for ncu captures (volume
+# 192^3 x 13 = 368 MB, still larger than L2).
+W_PROFILE = dict(W, N=192, Nd=288, V=90)
 WORKLOAD = ("XTT 256^3 x K13, 3 axes x 180 views, 384^2 detector, OS-EM 5 subsets, FP32 "
             "(12 seeded fiber cylinders, SOD 500 / SDD 1000 mm, 1 mm voxels)")
 METRIC = "XTT 256^3x13 projector GB/s (effective, forward+back per OS-EM epoch)"
@@ -243,7 +246,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--size", default="full", choices=["full", "profile"])
     args = ap.parse_args()
+    if args.size == "profile":
+        W.update(W_PROFILE)
+        args.no_e2e = True
+        args.no_cpu_baseline = True
     if args.warmup < 3:
         args.warmup = 3
 
