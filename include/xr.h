@@ -202,6 +202,23 @@ xr_status xr_dev_session_end(xr_ctx *ctx, float *d_md, float *d_evalue);
 /* The session's current ratio images (C*V*Nd^2 floats, device pointer). */
 xr_status xr_dev_session_proj(xr_ctx *ctx, const float **d_proj);
 
+/* The raw forward splat of xr_forward_proj_only on device buffers, for
+ * callers that cannot allocate device memory: code whose device memory is
+ * all owned by another allocator (a framework's caching pool) or whose
+ * steady-state loop must not allocate.  No counterpart in the reference.
+ * Allocates nothing: its only scratch (the per-view geometry table and the
+ * view list) is a fixed array inside libxr of num_cond * num_proj <= 4096
+ * (axis, view) pairs, held by every GPU that loads the library until exit;
+ * larger scans get XR_ERR_ARG.  d_vol: N^3 floats (channel 0); d_sino:
+ * C*V*Nd^2 floats, cleared then accumulated.  Work is enqueued on `stream`
+ * (a cudaStream_t, NULL = legacy default) without synchronizing.  All calls
+ * share the scratch and it keeps the last call's contents, so calls that
+ * overlap on the GPU race; serialise them.  The first call on a device
+ * resolves the scratch address (cudaGetSymbolAddress): make it before any
+ * stream capture. */
+xr_status xr_dev_forward_proj_only_static(xr_ctx *ctx, const float *d_vol, float *d_sino, xr_rotate dir,
+                                          void *stream);
+
 /* Library version string. */
 const char *xr_version(void);
 

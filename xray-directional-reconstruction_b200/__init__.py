@@ -131,6 +131,8 @@ _SIGS = {
     "xr_dev_session_epoch": ([ctypes.c_void_p, _D], ctypes.c_int),
     "xr_dev_session_end": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "xr_dev_session_proj": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "xr_dev_forward_proj_only_static": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.c_void_p], ctypes.c_int),
 }
 
 _lib = None

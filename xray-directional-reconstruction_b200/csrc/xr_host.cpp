@@ -155,6 +155,8 @@ static ViewFrame make_frame(const xr_ctx *c, int cond, int n, bool fdk) {
     return f;
 }
 
+ViewFrame host_view_frame(const xr_ctx *c, int cond, int n, bool fdk) { return make_frame(c, cond, n, fdk); }
+
 static void fill_consts(xr_ctx *c) {
     GeomConst &g = c->gc;
     g.N = c->N;
