@@ -238,6 +238,53 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_ttr(args, local):
+    """Time to a relative data residual: OS-EM epochs (device-timed with CUDA
+    events) from the reference's MLEM start mu = 0.01 (main.cu:38-43), with
+    ||A mu - b|| / ||b|| checked every few epochs outside the timed work."""
+    import torch
+    xr = load_pkg()
+    torch.cuda.set_device(local)
+    ctx = xr.Context.create(W["sdd"], W["sod"], W["det"], W["N"], W["Nd"], W["V"], three_axes(), None, None,
+                            basis13(), device=local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    N, Nd, V, C, K = W["N"], W["Nd"], W["V"], W["C"], W["K"]
+    mu_true = fiber_phantom(N, W["n_fibers"], W["seed"], basis13())
+    d_true = torch.from_numpy(mu_true).cuda()
+    d_b = torch.empty((C, V, Nd, Nd), dtype=torch.float32, device="cuda")
+    ctx.dev_forward(d_true.data_ptr(), d_b.data_ptr(), True)
+    d_vol = torch.full((K, N, N, N), 0.01, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.dev_session_begin(d_b.data_ptr(), d_vol.data_ptr(), True, args.max_epochs, W["batch"])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    total_ms = e0.elapsed_time(e1)
+    hist = []
+    reached = None
+    for ep in range(1, args.max_epochs + 1):
+        e0.record(stream)
+        ctx.dev_session_epoch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        if ep % args.check_every == 0 or ep == args.max_epochs:
+            r, _ = ctx.dev_residual(d_vol.data_ptr(), d_b.data_ptr(), True)
+            hist.append((ep, r, total_ms))
+            if r <= args.target:
+                reached = (ep, r, total_ms)
+                break
+    line = {"mode": "time_to_residual", "workload": WORKLOAD, "target": args.target, "storage": "f32",
+            "start": "mu = 0.01", "reached": reached is not None,
+            "epochs": reached[0] if reached else None, "seconds": (reached[2] / 1e3) if reached else None,
+            "history": [{"epoch": e, "rel_l2": r, "ms": t} for e, r, t in hist]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -247,6 +294,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--size", default="full", choices=["full", "profile"])
+    ap.add_argument("--ttr", action="store_true",
+                    help="time-to-residual: OS-EM from mu = 0.01 until ||A mu - b|| / ||b|| <= --target")
+    ap.add_argument("--target", type=float, default=1e-3)
+    ap.add_argument("--max-epochs", type=int, default=300)
+    ap.add_argument("--check-every", type=int, default=2)
     args = ap.parse_args()
     if args.size == "profile":
         W.update(W_PROFILE)
@@ -271,6 +323,10 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+
+    if args.ttr:
+        run_ttr(args, local)
+        return
 
     xr = load_pkg()
     s_basis = basis13()
@@ -316,26 +372,64 @@ def main():
     rel, _ = ctx.dev_residual(d_vol.data_ptr(), d_b.data_ptr(), True)   # ||A mu - b|| / ||b|| after the epochs
     ctx.dev_session_end(0, 0)
 
+    def epoch_ms(storage, graphs, steps):
+        """Mean epoch time of a fresh session (same inputs) with the given
+        storage type and graph replay; warm-up epochs untimed."""
+        ctx.set_option(xr.Option.STORAGE, storage)
+        ctx.set_option(xr.Option.GRAPHS, graphs)
+        dt = {0: torch.float32, 1: torch.bfloat16, 2: torch.float16}[storage]
+        db = d_b.to(dt)
+        dv = torch.full((K, N, N, N), 0.01, dtype=dt, device="cuda")
+        torch.cuda.synchronize()
+        ctx.dev_session_begin(db.data_ptr(), dv.data_ptr(), True, args.warmup + steps, W["batch"])
+        for _ in range(args.warmup):
+            ctx.dev_session_epoch()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(steps):
+            ctx.dev_session_epoch()
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ctx.dev_session_end(0, 0)
+        ctx.set_option(xr.Option.GRAPHS, 0)
+        ctx.set_option(xr.Option.STORAGE, 0)
+        del db, dv
+        return a0.elapsed_time(a1) / steps
+
+    variants = {"f32_graphs": epoch_ms(0, 1, args.steps), "bf16": epoch_ms(1, 0, args.steps),
+                "bf16_graphs": epoch_ms(1, 1, args.steps)}
+
     bv = bytes_view(K, N, Nd)
     per_gpu_bytes = 2 * C * V * bv
     value = world * per_gpu_bytes / (t_ms / 1e3) / 1e9
 
-    # roofline of the dominant kernel (forward or back), per launch
-    views_per_launch = C * ((V + W["batch"] - 1) // W["batch"])
+    # roofline of the dominant kernel (forward or back), per launch.  The
+    # forward of a subset is one k_fwd_col launch per column axis g (the three
+    # axes here have g = z, x, y: 3 launches of V/batch views); the fused back
+    # projection + update is one k_back_col launch over all axes' views.
+    subset = (V + W["batch"] - 1) // W["batch"]
+    rot = three_axes().reshape(C, 3, 3)
+    n_groups = len({int(np.argmax(np.abs(r[:, 2]))) for r in rot})
     fwd_ms, fwd_n = tim["forward"]
     back_ms, back_n = tim["back"]
-    dom, dom_ms, dom_n = ("k_forward<1>", fwd_ms, fwd_n) if fwd_ms >= back_ms else ("k_back_update<true>", back_ms,
-                                                                                     back_n)
+    if fwd_ms >= back_ms:
+        dom, dom_ms, dom_n, units = "k_fwd_col<1,g,float>", fwd_ms, fwd_n * n_groups, C * subset // n_groups
+    else:
+        dom, dom_ms, dom_n, units = "k_back_col<1,float>", back_ms, back_n, C * subset
     peak, peak_kind = measured_peaks()
     avg_launch_s = dom_ms / max(dom_n, 1) / 1e3
-    achieved = views_per_launch * bv / avg_launch_s / 1e9
+    achieved = units * bv / avg_launch_s / 1e9
     traffic = profile_traffic(dom)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": dom, "peak_kind": peak_kind,
-                "avg_launch_ms": avg_launch_s * 1e3, "units_per_launch": views_per_launch,
+                "avg_launch_ms": avg_launch_s * 1e3, "units_per_launch": units,
                 "bytes_per_unit": bv,
-                "note": "effective: the kernel reads the volume once per launch for all its views"}
-    launches = int(sum(n for _, n in tim.values()))
+                "note": "effective: one launch reads the volume once for all its views; traffic = ncu DRAM "
+                        "bytes per launch"}
+    # kernels in the timed region: per subset n_groups forward launches, one
+    # ratio launch, one back launch
+    launches = int(fwd_n * n_groups + tim["ratio"][1] + back_n)
 
     # e2e through the public host-buffer API (pinned host memory), every rank
     e2e = None
@@ -404,7 +498,8 @@ def main():
                        "l2": "inputs larger than L2 (volume 872 MB, sinograms 318 MB)",
                        "residual_rel_l2_after": rel},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
-            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in tim.items() if v[1]}}
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in tim.items() if v[1]},
+            "variants_ms_per_step": variants}
     print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

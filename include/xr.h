@@ -92,8 +92,15 @@ enum {
                                   block; 0 (default): axis 0's block for every
                                   axis, as the reference (reconstruct.cu:1708)   */
     XR_OPT_VIEWS_PER_CTA = 3,  /* forward splat: views per CTA (0 = automatic)    */
-    XR_OPT_STORAGE = 4         /* 0: FP32 storage; 1: BF16 volume+sinogram storage
-                                  with FP32 accumulation (device-session calls)   */
+    XR_OPT_STORAGE = 4,        /* storage of volumes and measured sinograms in HBM:
+                                  0 FP32 (default), 1 BF16, 2 FP16; arithmetic
+                                  and accumulation stay FP32 (FP64 for losses and
+                                  residual norms).  Device-buffer calls then take
+                                  volumes / sinograms of that type; host-buffer
+                                  calls keep float arrays and convert on the GPU */
+    XR_OPT_GRAPHS = 5          /* 1: each session epoch runs as a CUDA graph, one
+                                  captured per distinct subset order and replayed
+                                  (ignored while XR_OPT_TIMING is on)            */
 };
 
 /* ---- context ----------------------------------------------------------- */
@@ -178,11 +185,14 @@ xr_status xr_residual(xr_ctx *ctx, const float *const *voxel, const float *const
                       int xtt, double *rel_l2, double *l1);
 
 /* ---- device-buffer entry points (no host copies) ------------------------ */
+/* Volumes (d_vol, d_mu) and measured sinograms (d_sino of the residual and
+ * of sessions) hold elements of the storage type (XR_OPT_STORAGE); forward
+ * projections, orientations and eigenvalues are FP32. */
 
-xr_status xr_dev_forward(xr_ctx *ctx, const float *d_vol, float *d_sino, xr_rotate dir, int xtt);
-xr_status xr_dev_residual(xr_ctx *ctx, const float *d_vol, const float *d_sino, xr_rotate dir, int xtt,
+xr_status xr_dev_forward(xr_ctx *ctx, const void *d_vol, float *d_sino, xr_rotate dir, int xtt);
+xr_status xr_dev_residual(xr_ctx *ctx, const void *d_vol, const void *d_sino, xr_rotate dir, int xtt,
                           double *rel_l2, double *l1);
-xr_status xr_dev_orientation(xr_ctx *ctx, const float *d_mu, float *d_md, float *d_evalue);
+xr_status xr_dev_orientation(xr_ctx *ctx, const void *d_mu, float *d_md, float *d_evalue);
 
 /* An XTT / IR reconstruction session on device buffers, split so a caller
  * (or a CUDA graph) can drive epochs one at a time:
@@ -195,7 +205,7 @@ xr_status xr_dev_orientation(xr_ctx *ctx, const float *d_mu, float *d_md, float 
  *   end:   XTT only — mu_k = sqrt|mu_k| and, when d_md != NULL, orientation.
  * d_sino: C*V*Nd^2; d_vol: K*N^3 (XTT) or C*N^3 (IR).  Both stay owned by
  * the caller and must outlive the session. */
-xr_status xr_dev_session_begin(xr_ctx *ctx, const float *d_sino, float *d_vol, int xtt, int epochs,
+xr_status xr_dev_session_begin(xr_ctx *ctx, const void *d_sino, void *d_vol, int xtt, int epochs,
                                int batch, xr_rotate dir, xr_method method, float lambda);
 xr_status xr_dev_session_epoch(xr_ctx *ctx, double *loss);
 xr_status xr_dev_session_end(xr_ctx *ctx, float *d_md, float *d_evalue);

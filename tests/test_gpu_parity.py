@@ -253,3 +253,148 @@ def test_errors_on_device():
     ctx2 = xr.Context.create(1000, 500, 2, 8, 12, 4, rot)
     with pytest.raises(xr.XRError):                            # batch > V
         ctx2.ir_reconstruct(np.zeros((1, 4, 12, 12)), np.ones((1, 8, 8, 8)), 1, 5)
+
+
+def _oblique_rot(seed, n):
+    """Rotation matrices in general position (not grid-aligned), like the
+    reference's measured presets (settings.json "matrixRot")."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        a, b, c, d = q
+        out.append([a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c),
+                    2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b),
+                    2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d])
+    return np.array(out, np.float32)
+
+
+def _make_rot(rot, N, Nd, V, K, seed, sdd=1000.0, sod=500.0, det=2.0):
+    rng = np.random.default_rng(seed)
+    C = rot.shape[0]
+    basis = basis13()[:K] if K > 1 else np.array([[0, 0, 1.0]])
+    s = Scan(sdd=sdd, sod=sod, det=det, N=N, Nd=Nd, V=V, rot=rot, trans=rng.normal(0, 0.3, (C, 3)),
+             offset=rng.normal(0, 0.2, (C, 3)), basis=basis)
+    xr = load_xr()
+    ctx = xr.Context.create(sdd, sod, det, N, Nd, V, s.rot, s.trans, s.offset, s.basis)
+    return s, ctx
+
+
+@pytest.mark.parametrize("xtt", [False, True])
+def test_forward_oblique_axes_odd_pitch(oracle, xtt):
+    """General (non grid-aligned) rotation axes take the general kernels; a
+    detector pitch that is not a power of two exercises the verified exact
+    division by the pitch (the reference's oilpan preset: 0.0581777777 mm)."""
+    rot = np.concatenate([_oblique_rot(41, 2), three_axes()[:1]])
+    s, ctx = _make_rot(rot, 20, 30, 12, 13 if xtt else 1, 42, sdd=1819.6, sod=1316.5, det=0.0581777777)
+    vol = np.random.default_rng(43).uniform(0, 1, (s.K if xtt else 1, s.N, s.N, s.N)).astype(np.float32)
+    got = ctx.forward(vol, xtt)
+    ref = oracle.forward_all(s, vol if xtt else vol[0], 0, xtt)
+    assert rel_err(got, ref) <= TOL
+
+
+@pytest.mark.parametrize("method", ["MLEM", "ART"])
+def test_xtt_mixed_axes(oracle, method):
+    """XTT with one grid-aligned and one oblique axis: column forward for the
+    first, general kernels for the rest of the path."""
+    xr = load_xr()
+    rot = np.concatenate([three_axes()[:1], _oblique_rot(44, 1)])
+    s, ctx = _make_rot(rot, 16, 24, 10, 13, 45)
+    truth = fiber_phantom(s.N, 3, 46, s.basis)
+    b = oracle.forward_all(s, truth, 0, True)
+    v0 = np.full((s.K, s.N, s.N, s.N), 0.01, np.float32)
+    mu, ratio, _, _, gl = ctx.xtt_reconstruct(b, v0, 2, 3, xr.Rotate.CW, xr.Method[method], 1e-3)
+    ref, rproj, rl = oracle.xtt_reconstruct(s, b, v0, 2, 3, art=method == "ART", lam=1e-3)
+    assert rel_err(mu, ref) <= TOL
+    assert rel_err(ratio, rproj) <= TOL
+
+
+def test_ir_oblique_axis_odd_pitch(oracle):
+    xr = load_xr()
+    s, ctx = _make_rot(_oblique_rot(47, 1), 20, 30, 12, 1, 48, sdd=1819.6, sod=1316.5, det=0.0581777777)
+    truth = ellipsoid_phantom(s.N, 4, 49)
+    b = oracle.forward_all(s, truth, 0, False)
+    v0 = np.ones((1, s.N, s.N, s.N), np.float32)
+    got, _ = ctx.ir_reconstruct(b, v0, 2, 3)
+    ref, _ = oracle.ir_reconstruct(s, b, v0, 2, 3)
+    assert rel_err(got, ref) <= TOL
+
+
+def test_ccw_rotation(oracle):
+    """Rotate::CCW (n = -view): the reference indexes correlationProjByLength
+    with the signed n, which writes before the buffer; the restatement and
+    libxr both use |n| and agree."""
+    xr = load_xr()
+    s, ctx = make(16, 24, 10, C=2, seed=50)
+    vol = np.random.default_rng(51).uniform(0, 1, (s.N, s.N, s.N)).astype(np.float32)
+    got = ctx.forward(vol[None], False, xr.Rotate.CCW)
+    ref = oracle.forward_all(s, vol, 1, False)
+    assert rel_err(got, ref) <= TOL
+
+
+def _bf16_round(a):
+    """Round float32 to bfloat16 (nearest even), returned as float32."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+@pytest.mark.parametrize("storage", [1, 2])
+def test_storage_forward_is_rounded_input(oracle, storage):
+    """16-bit storage only rounds the stored volume: the forward of a BF16 /
+    FP16 volume equals the FP32 forward of the rounded volume."""
+    xr = load_xr()
+    s, ctx = make(20, 30, 10, C=3, K=13, seed=60)
+    vol = np.random.default_rng(61).uniform(0, 1, (13, 20, 20, 20)).astype(np.float32)
+    ctx.set_option(xr.Option.STORAGE, storage)
+    got = ctx.forward(vol, True)
+    rounded = _bf16_round(vol) if storage == 1 else vol.astype(np.float16).astype(np.float32)
+    ref = oracle.forward_all(s, rounded, 0, True)
+    assert rel_err(got, ref) <= TOL
+
+
+@pytest.mark.parametrize("storage,bound", [(0, 1e-3), (1, 3e-2), (2, 5e-3)])
+def test_storage_xtt_error_vs_fp64(oracle, storage, bound):
+    """XTT OS-EM with FP32 / BF16 / FP16 storage of volume and sinogram (FP32
+    arithmetic): the error of each against the FP64 oracle is stated and
+    bounded (max |d| / max |ref| over the reconstructed coefficients)."""
+    xr = load_xr()
+    s, ctx = make(16, 24, 12, C=3, K=13, seed=62, shifts=False)
+    truth = fiber_phantom(s.N, 4, 63, s.basis)
+    b = oracle.forward_all(s, truth, 0, True)
+    v0 = np.full((s.K, s.N, s.N, s.N), 0.01, np.float32)
+    ctx.set_option(xr.Option.STORAGE, storage)
+    mu, _, _, _, _ = ctx.xtt_reconstruct(b, v0, 3, 3, orientation=False)
+    ref64, _, _ = oracle.xtt_reconstruct(s, b.astype(np.float64), v0.astype(np.float64), 3, 3, dt=np.float64)
+    err = rel_err(mu, ref64)
+    print(f"XTT storage={['f32', 'bf16', 'f16'][storage]}: max|d|/max|ref| vs FP64 = {err:.3e}")
+    assert err <= bound
+
+
+@pytest.mark.parametrize("xtt", [True, False])
+def test_graph_epochs_match_direct(oracle, xtt):
+    """XR_OPT_GRAPHS: epochs replayed from CUDA graphs (one per subset order)
+    give the same reconstruction as directly launched epochs."""
+    torch = pytest.importorskip("torch")
+    xr = load_xr()
+    s, ctx = make(16, 24, 12, C=3, K=13 if xtt else 1, seed=70)
+    if xtt:
+        truth = fiber_phantom(s.N, 3, 71, s.basis)
+        v0 = np.full((s.K, s.N, s.N, s.N), 0.01, np.float32)
+    else:
+        truth = ellipsoid_phantom(s.N, 4, 71)
+        v0 = np.ones((s.C, s.N, s.N, s.N), np.float32)
+    b = oracle.forward_all(s, truth, 0, xtt)
+    outs = []
+    for graphs in (0, 1):
+        ctx.set_option(xr.Option.GRAPHS, graphs)
+        db = torch.from_numpy(b).cuda()
+        dv = torch.from_numpy(v0).cuda()
+        torch.cuda.synchronize()
+        ctx.dev_session_begin(db.data_ptr(), dv.data_ptr(), xtt, 4, 3)
+        for _ in range(4):
+            ctx.dev_session_epoch()
+        ctx.dev_session_end(0, 0)
+        outs.append(dv.cpu().numpy())
+    assert rel_err(outs[1], outs[0]) <= TOL

@@ -79,6 +79,13 @@ class Option(enum.IntEnum):
     FDK_AXIS_BLOCKS = 2
     VIEWS_PER_CTA = 3
     STORAGE = 4
+    GRAPHS = 5
+
+
+class Storage(enum.IntEnum):
+    F32 = 0
+    BF16 = 1
+    F16 = 2
 
 
 class _Scan(ctypes.Structure):

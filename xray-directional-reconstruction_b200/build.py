@@ -23,7 +23,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["xr_kernels.cu", "xr_orient.cu", "xr_fdk.cu", "xr_static.cu"]
+CU_SOURCES = ["xr_kernels.cu", "xr_column.cu", "xr_orient.cu", "xr_fdk.cu", "xr_static.cu"]
 CXX_SOURCES = ["xr_host.cpp"]
 
 
@@ -44,7 +44,7 @@ def _stale(obj, deps):
 
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(os.path.dirname(HERE), "include", "xr.h"))
     objs = []
     for src in CU_SOURCES:

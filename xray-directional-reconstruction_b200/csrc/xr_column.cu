@@ -1,0 +1,664 @@
+/*
+ * Column-structured projector kernels for rotation axes whose grating
+ * direction G = elemR_c e_z is a grid axis g (G = +-e_g).
+ *
+ * For such an axis every view's detector v axis is +-e_g and its source and
+ * detector u axis have a zero g component, so along a voxel column parallel
+ * to g the reference's rayCasting (ir.cu:1881-1897) produces the SAME u,
+ * coeff and source-to-voxel (a, b) components — bit for bit, the dropped
+ * terms being exact zeros — and v differs only through o_g:
+ *     v = ((+-(coeff * o_g)) * mag) / det + Nd/2.
+ * A thread owns a segment of 4 voxels along g: the ray set-up is paid once per
+ * column and view, each voxel then costs ~8 operations for its v.  The
+ * sample-rotation axes of the three-axis XTT scans (elemR = I and the two
+ * 90-degree tilts) are of this kind; other axes take the general kernels in
+ * xr_kernels.cu.
+ *
+ * Division by the detector pitch: a / det = q + r * rdet with q = a * rdet,
+ * r = fma(-q, det, a) and rdet = RN(1/det) — one Markstein correction step
+ * (P. Markstein, "Computation of elementary functions on the IBM RISC
+ * System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  Every context
+ * checks it bit for bit against IEEE division over all the magnitudes a
+ * projector meets before using it (k_check_div); otherwise __fdiv_rn is used.
+ */
+#include <cuda_runtime.h>
+
+#include "xr_internal.h"
+#include "xr_storage.cuh"
+#include "xr_tile.cuh"
+
+namespace xr {
+namespace {
+
+constexpr int kTileCap = 48 * 48;
+constexpr int kFwdThreads = 256;               /* forward: 16 (g) x 8 x 8 brick, 4 voxels/thread */
+constexpr int kBackThreads = 128;              /* back: 8 x 8 x 8 brick, 4 voxels/thread          */
+constexpr int kFrameChunk = 128;
+
+__device__ __forceinline__ float vox_base(int i, int N, float vs) {
+    const float a = __fsub_rn(__fsub_rn(__fmul_rn(2.0f, (float)i), (float)N), 1.0f);
+    return __fmul_rn(__fmul_rn(a, 0.5f), vs);
+}
+
+/* a / det, correctly rounded. */
+__device__ __forceinline__ float div_det(float a, const GeomConst &g) {
+    if (!g.exact_rdet) return __fdiv_rn(a, g.det);
+    const float q = __fmul_rn(a, g.rdet);
+    const float r = __fmaf_rn(-q, g.det, a);
+    return __fmaf_rn(r, g.rdet, q);
+}
+
+template <int G>
+struct Ax {
+    static constexpr int A = (G == 0) ? 1 : 0;   /* the two other axes, ascending */
+    static constexpr int B = (G == 2) ? 1 : 2;
+};
+
+/* Per-column part of rayCasting for column axis G: u, coeff and the (a, b)
+ * components of the source-to-voxel vector.  The reference's three-term dot
+ * products lose their g terms (exact zeros). */
+template <int G>
+__device__ __forceinline__ void col_ray(const ViewFrame &f, const GeomConst &g, float ba, float bb, float &u,
+                                        float &coeff, float &da, float &db) {
+    constexpr int A = Ax<G>::A, B = Ax<G>::B;
+    const float oa = __fsub_rn(__fsub_rn(ba, f.off[A]), f.t[A]);
+    const float ob = __fsub_rn(__fsub_rn(bb, f.off[B]), f.t[B]);
+    da = __fsub_rn(oa, f.src[A]);
+    db = __fsub_rn(ob, f.src[B]);
+    const float sd = __fadd_rn(__fmul_rn(f.src[A], da), __fmul_rn(f.src[B], db));
+    coeff = __fdiv_rn(-f.ss, sd);
+    const float pa = __fadd_rn(f.src[A], __fmul_rn(coeff, da));
+    const float pb = __fadd_rn(f.src[B], __fmul_rn(coeff, db));
+    const float pu = __fadd_rn(__fmul_rn(pa, f.eu[A]), __fmul_rn(pb, f.eu[B]));
+    u = __fadd_rn(div_det(__fmul_rn(pu, g.mag), g), g.half);
+}
+
+/* Per-voxel v; dg receives o_g (= the g component of source-to-voxel). */
+template <int G>
+__device__ __forceinline__ float col_v(const ViewFrame &f, const GeomConst &g, float bg, float coeff, float magsig,
+                                       float &dg) {
+    dg = __fsub_rn(__fsub_rn(bg, f.off[G]), f.t[G]);
+    return __fadd_rn(div_det(__fmul_rn(__fmul_rn(coeff, dg), magsig), g), g.half);
+}
+
+/* One axis of the bilinear taps: window test and weights, as ir.cu:1501-1509
+ * (the reference's combined u-and-v test splits exactly into the two). */
+__device__ __forceinline__ bool tap1(const GeomConst &g, float u, int &i, float &f, float &gm) {
+    if (!(0.55f < u && u < g.lim)) return false;
+    const float ut = __fsub_rn(u, 0.5f);
+    const float fi = floorf(ut);
+    i = (int)fi;
+    f = __fsub_rn(ut, fi);
+    gm = __fsub_rn(1.0f, f);
+    return true;
+}
+
+template <int G>
+__device__ __forceinline__ void xyz_of(int ia, int ib, int ig, int &x, int &y, int &z) {
+    constexpr int A = Ax<G>::A, B = Ax<G>::B;
+    int c[3];
+    c[A] = ia;
+    c[B] = ib;
+    c[G] = ig;
+    x = c[0];
+    y = c[1];
+    z = c[2];
+}
+
+/* ------------------------------------------------------------------------ */
+/* Forward splat, column form.  Brick: 16 along g, 8 along a, 8 along b.     */
+/* Warp = 4 segments x 4 (a) x 2 (b) columns; 8 warps tile 8 x 8 columns.    */
+/* ------------------------------------------------------------------------ */
+struct FwdColArgs {
+    GeomConst g;
+    const ViewFrame *frames;
+    const int *view_list;
+    int n_views, vpc;
+    const int *conds;         /* n_cond axis indices, all with column axis G */
+    const float *magsig;      /* per axis: sign(ev[g]) * mag                 */
+    const void *vol;          /* storage type T                              */
+    float *out;
+    const BasisConst *basis;
+    int nbg, nba;             /* bricks along g and a                        */
+};
+
+template <int MODE, int G, typename T>
+__global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
+    const T *vol = reinterpret_cast<const T *>(a.vol);
+    constexpr int A = Ax<G>::A, B = Ax<G>::B;
+    /* Two detector tiles (double-buffered over views) in two-word fixed
+     * point, xr_tile.cuh: native 32-bit shared atomics, per-CTA sums exact
+     * to 2^-41 of the brick's largest contribution. */
+    extern __shared__ int smem[];
+    __shared__ float s_red[kFwdThreads / 32];
+    int4 *bbox = reinterpret_cast<int4 *>(smem + 4 * kTileCap);
+    ViewFrame *fr = reinterpret_cast<ViewFrame *>(bbox + a.vpc);
+
+    const GeomConst &g = a.g;
+    const int N = g.N, Nd = g.Nd;
+    const int cond = a.conds[blockIdx.y];
+    const float magsig = a.magsig[cond];
+    const int j0 = blockIdx.z * a.vpc;
+    const int nv = min(a.vpc, a.n_views - j0);
+    if (nv <= 0) return;
+
+    const int brick = blockIdx.x;
+    const int g0 = (brick % a.nbg) * 16, a0 = ((brick / a.nbg) % a.nba) * 8, b0 = (brick / (a.nbg * a.nba)) * 8;
+    const int g1 = min(g0 + 16, N) - 1, a1 = min(a0 + 8, N) - 1, b1 = min(b0 + 8, N) - 1;
+
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 4 * kTileCap; i += kFwdThreads) smem[i] = 0;
+    for (int i = tid; i < nv * 5; i += kFwdThreads) {
+        const int jj = i / 5, q = i % 5;
+        reinterpret_cast<float4 *>(&fr[jj])[q] =
+            reinterpret_cast<const float4 *>(&a.frames[(size_t)cond * g.V + a.view_list[j0 + jj]])[q];
+    }
+    __syncthreads();
+    /* footprint bounding box per view from the 8 brick corners */
+    for (int i = tid; i < nv; i += kFwdThreads) {
+        const ViewFrame &f = fr[i];
+        float umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
+        bool ok = true;
+        for (int c = 0; c < 8; c++) {
+            const float ba = vox_base((c & 1) ? a1 : a0, N, g.vs);
+            const float bb = vox_base((c & 2) ? b1 : b0, N, g.vs);
+            const float bg = vox_base((c & 4) ? g1 : g0, N, g.vs);
+            float u, coeff, da, db, dg;
+            col_ray<G>(f, g, ba, bb, u, coeff, da, db);
+            const float v = col_v<G>(f, g, bg, coeff, magsig, dg);
+            if (!(fabsf(u) < 1e7f && fabsf(v) < 1e7f)) ok = false;
+            umin = fminf(umin, u); umax = fmaxf(umax, u);
+            vmin = fminf(vmin, v); vmax = fmaxf(vmax, v);
+        }
+        int iu0 = (int)floorf(umin - 0.5f) - 1, iu1 = (int)floorf(umax - 0.5f) + 2;
+        int iv0 = (int)floorf(vmin - 0.5f) - 1, iv1 = (int)floorf(vmax - 0.5f) + 2;
+        iu0 = max(iu0, 0); iv0 = max(iv0, 0);
+        iu1 = min(iu1, Nd - 1); iv1 = min(iv1, Nd - 1);
+        int W = iu1 - iu0 + 1, H = iv1 - iv0 + 1;
+        if (!ok) { W = 1 << 20; H = 1; }
+        if (iu1 < iu0 || iv1 < iv0) { W = 0; H = 0; }
+        bbox[i] = make_int4(iu0, iv0, W, H);
+    }
+
+    const int lane = tid & 31, w = tid >> 5;
+    const int seg = lane & 3;
+    const int ia = a0 + (w & 1) * 4 + ((lane >> 2) & 3);
+    const int ib = b0 + (w >> 1) * 2 + (lane >> 4);
+    const int igb = g0 + seg * 4;
+    const bool col_ok = ia < N && ib < N;
+    const float ba = vox_base(ia, N, g.vs), bb = vox_base(ib, N, g.vs);
+    float bg[4];
+    bool okv[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        bg[q] = vox_base(igb + q, N, g.vs);
+        okv[q] = col_ok && (igb + q <= g1);
+    }
+
+    /* per-voxel value: plain ratio*mu; XTT a0 and M of this axis (xyz order) */
+    float val[4], m[4][6];
+    const size_t NN = (size_t)N * N, N3 = NN * N;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        val[q] = 0.f;
+#pragma unroll
+        for (int e = 0; e < 6; e++) m[q][e] = 0.f;
+        if (!okv[q]) continue;
+        int x, y, z;
+        xyz_of<G>(ia, ib, igb + q, x, y, z);
+        const size_t idx = (size_t)x + (size_t)N * y + NN * z;
+        if (MODE == 0) {
+            val[q] = ldgf<T>(vol + idx);
+        } else if (MODE == 2) {
+            val[q] = 1.0f;
+        } else {
+            const BasisConst *Bc = a.basis;
+            const float sc = __fmul_rn(g.vs, g.ratio);
+            float s0m = 0.f, mm[6] = {0, 0, 0, 0, 0, 0};
+            for (int k = 0; k < g.K; k++) {
+                const float gk = Bc->g[cond * g.K + k] * sc;
+                if (gk == 0.f) continue;
+                const float mu = ldgf<T>(vol + idx + (size_t)k * N3) * gk;
+                const float s0 = Bc->S[3 * k], s1 = Bc->S[3 * k + 1], s2 = Bc->S[3 * k + 2];
+                s0m = fmaf(Bc->S2[k], mu, s0m);
+                mm[0] = fmaf(mu * s0, s0, mm[0]);
+                mm[1] = fmaf(mu * s1, s1, mm[1]);
+                mm[2] = fmaf(mu * s2, s2, mm[2]);
+                mm[3] = fmaf(2.f * mu * s0, s1, mm[3]);
+                mm[4] = fmaf(2.f * mu * s0, s2, mm[4]);
+                mm[5] = fmaf(2.f * mu * s1, s2, mm[5]);
+            }
+            val[q] = s0m;
+#pragma unroll
+            for (int e = 0; e < 6; e++) m[q][e] = mm[e];
+        }
+    }
+    /* bound on |contribution| over the CTA's voxels (weights c <= 1) */
+    float bound = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (!okv[q]) continue;
+        float bq = (MODE == 0) ? fabsf(val[q]) * g.ratio : (MODE == 2 ? 1.0f : fabsf(val[q]));
+        if (MODE == 1)
+#pragma unroll
+            for (int e = 0; e < 6; e++) bq += fabsf(m[q][e]);
+        bound = fmaxf(bound, bq * 1.001f);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bound = fmaxf(bound, __shfl_xor_sync(0xffffffffu, bound, o));
+    if ((tid & 31) == 0) s_red[tid >> 5] = bound;
+    __syncthreads();
+    float S = 0.f;
+#pragma unroll
+    for (int i = 0; i < kFwdThreads / 32; i++) S = fmaxf(S, s_red[i]);
+    if (!(S > 0.f) || !(S < 3e38f)) return;      /* nothing to splat (or non-finite input) */
+    const int sh = fix_shift(S);
+    const float fscale = ldexpf(1.0f, sh);
+    const double finv = ldexp(1.0, -sh);
+
+    const size_t NdNd = (size_t)Nd * Nd;
+    float *outc = a.out + (size_t)cond * g.V * NdNd;
+    for (int jj = 0; jj < nv; jj++) {
+        const ViewFrame f = fr[jj];          /* registers: no reload after the shared atomics */
+        const int4 bb4 = bbox[jj];
+        int *T = smem + (jj & 1) * 2 * kTileCap;   /* hi words, lo words after */
+        float *P = outc + (size_t)f.view * NdNd;
+        const bool use_tile = (bb4.z > 0) && (bb4.z * bb4.w <= kTileCap);
+        float u, coeff, da, db;
+        int iu;
+        float fu, gu;
+        if (bb4.z > 0 && col_ok) {
+            col_ray<G>(f, g, ba, bb, u, coeff, da, db);
+            if (tap1(g, u, iu, fu, gu)) {
+                const float dab2 = fmaf(da, da, db * db);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    if (!okv[q]) continue;
+                    float dg;
+                    const float v = col_v<G>(f, g, bg[q], coeff, magsig, dg);
+                    int iv;
+                    float fv, gv;
+                    if (!tap1(g, v, iv, fv, gv)) continue;
+                    const float c1 = __fmul_rn(gu, fv), c2 = __fmul_rn(fu, fv);
+                    const float c3 = __fmul_rn(fu, gv), c4 = __fmul_rn(gu, gv);
+                    float w1, w2, w3, w4;
+                    if (MODE == 0) {
+                        const float pv = val[q];
+                        w1 = __fmul_rn(__fmul_rn(c1, g.ratio), pv);
+                        w2 = __fmul_rn(__fmul_rn(c2, g.ratio), pv);
+                        w3 = __fmul_rn(__fmul_rn(c3, g.ratio), pv);
+                        w4 = __fmul_rn(__fmul_rn(c4, g.ratio), pv);
+                    } else if (MODE == 2) {
+                        w1 = c1; w2 = c2; w3 = c3; w4 = c4;
+                    } else {
+                        float d[3];
+                        d[A] = da; d[B] = db; d[G] = dg;
+                        const float dd = fmaf(dg, dg, dab2);
+                        const float q2 = m[q][0] * d[0] * d[0] + m[q][1] * d[1] * d[1] + m[q][2] * d[2] * d[2] +
+                                         m[q][3] * d[0] * d[1] + m[q][4] * d[0] * d[2] + m[q][5] * d[1] * d[2];
+                        const float pv = val[q] - __fdividef(q2, dd);
+                        w1 = __fmul_rn(c1, pv); w2 = __fmul_rn(c2, pv);
+                        w3 = __fmul_rn(c3, pv); w4 = __fmul_rn(c4, pv);
+                    }
+                    const int lu = iu - bb4.x, lv = iv - bb4.y;
+                    if (use_tile && lu >= 0 && lu + 1 < bb4.z && lv >= 0 && lv + 1 < bb4.w) {
+                        int *t0 = T + lu + bb4.z * lv;
+                        fix_add(t0 + bb4.z, kTileCap, w1 * fscale);
+                        fix_add(t0 + bb4.z + 1, kTileCap, w2 * fscale);
+                        fix_add(t0 + 1, kTileCap, w3 * fscale);
+                        fix_add(t0, kTileCap, w4 * fscale);
+                    } else {
+                        float *p0 = P + iu + (size_t)Nd * iv;
+                        atomicAdd(p0 + Nd, w1);
+                        atomicAdd(p0 + Nd + 1, w2);
+                        atomicAdd(p0 + 1, w3);
+                        atomicAdd(p0, w4);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (use_tile) {   /* one warp per tile row: coalesced flush, tile cleared behind */
+            for (int r = tid >> 5; r < bb4.w; r += kFwdThreads / 32) {
+                for (int c = tid & 31; c < bb4.z; c += 32) {
+                    float t;
+                    if (fix_take(T + c + bb4.z * r, kTileCap, finv, t)) {
+                        atomicAdd(P + (bb4.x + c) + (size_t)Nd * (bb4.y + r), t);
+                    }
+                }
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Back-projection, column form, fused with the update.                      */
+/* Brick 8 x 8 x 8 voxels, 128 threads.  For each axis the threads map to     */
+/* 64 columns x 2 segments of 4 voxels along that axis's g.                  */
+/*   PLAIN: one axis (IR), tmp/factor in registers, voxelProduct/voxelPlus.   */
+/*   XTT:   every axis; per axis the moments sum(r), sum(r d d^T / d.d) of    */
+/*          4 voxels fold into shared tmp_k; factor_k is the per-subset       */
+/*          sensitivity precomputed by SENS.                                  */
+/*   SENS:  moments sum(1), sum(d d^T / d.d) folded into factor_k, written    */
+/*          to global (geometry only; once per subset).                       */
+/* ------------------------------------------------------------------------ */
+enum { B_PLAIN = 0, B_XTT = 1, B_SENS = 2 };
+
+struct BackColArgs {
+    GeomConst g;
+    const ViewFrame *frames;
+    const int *view_list;
+    int n_views, n_cond;
+    const int *conds;         /* n_cond axes (PLAIN: 1)                      */
+    const int *axis_g;        /* per axis: column axis 0/1/2                 */
+    const float *magsig;      /* per axis: sign * mag                        */
+    const float *proj;        /* ratio images, C blocks                      */
+    void *vol;                /* PLAIN: the axis's N^3; XTT: K*N^3 (type T)  */
+    const float *fac_in;      /* XTT: K*N^3 sensitivity of this subset       */
+    float *fac_out;           /* SENS: K*N^3                                 */
+    const BasisConst *basis;
+    int art;
+    float alpha;
+};
+
+/* One view of one axis for a thread's column segment of 4 voxels: the ray
+ * set-up once, then per voxel v, the taps and the 4-tap gather from the
+ * (L2-resident) ratio image. */
+template <int MODE, int G>
+__device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f, float magsig, float ba, float bb,
+                                          const float bg[4], int nq, const float *Pv, float acc[4][7]) {
+    constexpr int A = Ax<G>::A, B = Ax<G>::B;
+    const int Nd = g.Nd;
+    float u, coeff, da, db;
+    col_ray<G>(f, g, ba, bb, u, coeff, da, db);
+    int iu;
+    float fu, gu;
+    if (!tap1(g, u, iu, fu, gu)) return;
+    const float dab2 = fmaf(da, da, db * db);
+    const float *Pc = Pv + iu;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (q >= nq) continue;
+        float dg;
+        const float v = col_v<G>(f, g, bg[q], coeff, magsig, dg);
+        int iv;
+        float fv, gv;
+        if (!tap1(g, v, iv, fv, gv)) continue;
+        float nb = 0.f;
+        if (MODE != B_SENS) {
+            const float c1 = __fmul_rn(gu, fv), c2 = __fmul_rn(fu, fv);
+            const float c3 = __fmul_rn(fu, gv), c4 = __fmul_rn(gu, gv);
+            const float *pp = Pc + (size_t)Nd * iv;
+            const float p4 = __ldg(pp), p3 = __ldg(pp + 1), p1 = __ldg(pp + Nd), p2 = __ldg(pp + Nd + 1);
+            nb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(c1, p1), __fmul_rn(c2, p2)), __fmul_rn(c3, p3)),
+                           __fmul_rn(c4, p4));
+        }
+        if (MODE == B_PLAIN) {
+            acc[q][0] = __fadd_rn(acc[q][0], nb);     /* tmp    (ir.cu:1750) */
+            acc[q][1] = __fadd_rn(acc[q][1], 1.0f);   /* factor (ir.cu:1749) */
+        } else {
+            float d[3];
+            d[A] = da; d[B] = db; d[G] = dg;
+            const float inv = __frcp_rn(fmaf(dg, dg, dab2));
+            float wgt;
+            if (MODE == B_XTT) {
+                acc[q][6] += nb;
+                wgt = nb * inv;
+            } else {
+                acc[q][6] += 1.0f;
+                wgt = inv;
+            }
+            acc[q][0] = fmaf(wgt, d[0] * d[0], acc[q][0]);
+            acc[q][1] = fmaf(wgt, d[1] * d[1], acc[q][1]);
+            acc[q][2] = fmaf(wgt, d[2] * d[2], acc[q][2]);
+            acc[q][3] = fmaf(wgt, d[0] * d[1], acc[q][3]);
+            acc[q][4] = fmaf(wgt, d[0] * d[2], acc[q][4]);
+            acc[q][5] = fmaf(wgt, d[1] * d[2], acc[q][5]);
+        }
+    }
+}
+
+/* One axis of the back kernel: threads map to 64 columns x 2 segments along
+ * this axis's column axis G; moments accumulate over all listed views; then
+ * PLAIN updates the voxels in place, XTT/SENS fold into the shared per-voxel
+ * channel accumulators. */
+template <int MODE, int G, typename T>
+__device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, float *sacc, int cond, int bx0,
+                                          int by0, int bz0) {
+    constexpr int A = Ax<G>::A, B = Ax<G>::B;
+    const GeomConst &g = a.g;
+    const int N = g.N, K = g.K, Nd = g.Nd;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int ca = lane & 7, cb = ((lane >> 3) & 3) + (w & 1) * 4, sg = w >> 1;
+    const int o[3] = {bx0, by0, bz0};
+    const int ia = o[A] + ca, ib = o[B] + cb, igb = o[G] + sg * 4;
+    const bool col_ok = ia < N && ib < N;
+    const int nq = col_ok ? max(0, min(4, N - igb)) : 0;
+    const float magsig = a.magsig[cond];
+    const float *P = a.proj + (size_t)cond * g.V * (size_t)Nd * Nd;
+    const size_t NN = (size_t)N * N, NdNd = (size_t)Nd * Nd;
+    const float ba = vox_base(ia, N, g.vs), bb = vox_base(ib, N, g.vs);
+    float bg[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) bg[q] = vox_base(igb + q, N, g.vs);
+    float acc[4][7];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int e = 0; e < 7; e++) acc[q][e] = 0.f;
+    for (int c0 = 0; c0 < a.n_views; c0 += kFrameChunk) {
+        const int nc = min(kFrameChunk, a.n_views - c0);
+        __syncthreads();
+        for (int i = tid; i < nc * 5; i += kBackThreads) {
+            const int jj = i / 5, q = i % 5;
+            reinterpret_cast<float4 *>(&fr[jj])[q] =
+                reinterpret_cast<const float4 *>(&a.frames[(size_t)cond * g.V + a.view_list[c0 + jj]])[q];
+        }
+        __syncthreads();
+        if (nq > 0)
+            for (int jj = 0; jj < nc; jj++)
+                back_view<MODE, G>(g, fr[jj], magsig, ba, bb, bg, nq, P + (size_t)fr[jj].view * NdNd, acc);
+    }
+    if (!col_ok) return;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (q >= nq) continue;
+        if (MODE == B_PLAIN) {
+            /* voxelProduct (ir.cu:1637-1654) / voxelPlus (ir.cu:1682-1693) */
+            int x, y, z;
+            xyz_of<G>(ia, ib, igb + q, x, y, z);
+            T *vp = reinterpret_cast<T *>(a.vol) + (size_t)x + (size_t)N * y + NN * z;
+            const float tmp = acc[q][0], fac = acc[q][1], mu = ldf<T>(vp);
+            if (a.art) stf<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmp)));
+            else stf<T>(vp, (fac == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmp), fac));
+        } else {
+            int lx, ly, lz;
+            xyz_of<G>(ca, cb, sg * 4 + q, lx, ly, lz);
+            const int lv = lx + 8 * ly + 64 * lz;
+            const BasisConst *Bc = a.basis;
+            for (int k = 0; k < K; k++) {
+                const float gk = Bc->g[cond * K + k];
+                if (gk == 0.f) continue;
+                const float s0 = Bc->S[3 * k], s1 = Bc->S[3 * k + 1], s2 = Bc->S[3 * k + 2];
+                const float sAs = s0 * s0 * acc[q][0] + s1 * s1 * acc[q][1] + s2 * s2 * acc[q][2] +
+                                  2.f * (s0 * s1 * acc[q][3] + s0 * s2 * acc[q][4] + s1 * s2 * acc[q][5]);
+                sacc[k * 512 + lv] += gk * fmaf(Bc->S2[k], acc[q][6], -sAs);
+            }
+        }
+    }
+}
+
+template <int MODE, typename T>
+__global__ void __launch_bounds__(kBackThreads, 4) k_back_col(BackColArgs a) {
+    __shared__ ViewFrame fr[kFrameChunk];
+    extern __shared__ float sacc[];   /* XTT / SENS: K x 512 per-voxel accumulators */
+    const GeomConst &g = a.g;
+    const int N = g.N;
+    const int nb8 = (N + 7) / 8;
+    const int b = blockIdx.x;
+    const int bx0 = (b % nb8) * 8, by0 = ((b / nb8) % nb8) * 8, bz0 = (b / (nb8 * nb8)) * 8;
+    const int tid = threadIdx.x;
+    const int K = g.K;
+    const size_t NN = (size_t)N * N, N3 = NN * N;
+    if (MODE != B_PLAIN) {
+        for (int i = tid; i < K * 512; i += kBackThreads) sacc[i] = 0.0f;
+    }
+    for (int ci = 0; ci < a.n_cond; ci++) {
+        const int cond = a.conds[ci];
+        const int G = a.axis_g[cond];   /* uniform over the CTA */
+        if (G == 0) axis_pass<MODE, 0, T>(a, fr, sacc, cond, bx0, by0, bz0);
+        else if (G == 1) axis_pass<MODE, 1, T>(a, fr, sacc, cond, bx0, by0, bz0);
+        else axis_pass<MODE, 2, T>(a, fr, sacc, cond, bx0, by0, bz0);
+        __syncthreads();
+    }
+    if (MODE == B_PLAIN) return;
+    /* home layout: brick-linear voxel order */
+    for (int lv = tid; lv < 512; lv += kBackThreads) {
+        const int x = bx0 + (lv & 7), y = by0 + ((lv >> 3) & 7), z = bz0 + (lv >> 6);
+        if (x >= N || y >= N || z >= N) continue;
+        const size_t idx = (size_t)x + (size_t)N * y + NN * z;
+        for (int k = 0; k < K; k++) {
+            const float t = sacc[k * 512 + lv];
+            if (MODE == B_SENS) {
+                a.fac_out[idx + (size_t)k * N3] = t;
+            } else {
+                T *vp = reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3;
+                const float mu = ldf<T>(vp);
+                if (a.art) {
+                    stf<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, t)));
+                } else {
+                    const float f = a.fac_in[idx + (size_t)k * N3];
+                    stf<T>(vp, (f == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, t), f));
+                }
+            }
+        }
+    }
+}
+
+/* Bit-for-bit check of div_det against IEEE division over every float
+ * a in [2^-24, 2^24) * det (both signs give the same result by symmetry). */
+__global__ void k_check_div(float det, float rdet, unsigned lo_bits, unsigned count, unsigned *mismatch) {
+    unsigned bad = 0;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float a = __uint_as_float(lo_bits + i);
+        const float q = __fmul_rn(a, rdet);
+        const float r = __fmaf_rn(-q, det, a);
+        const float m = __fmaf_rn(r, rdet, q);
+        if (__float_as_uint(m) != __float_as_uint(__fdiv_rn(a, det))) bad++;
+    }
+    if (bad) atomicAdd(mismatch, bad);
+}
+
+}  // namespace
+
+cudaError_t check_exact_rdet(float det, float rdet, unsigned *d_flag, unsigned *h_result, cudaStream_t s) {
+    const float lo = det * 5.9604645e-08f, hi = det * 16777216.0f;   /* det * 2^-24, det * 2^24 */
+    const unsigned lo_bits = __builtin_bit_cast(unsigned, lo), hi_bits = __builtin_bit_cast(unsigned, hi);
+    cudaMemsetAsync(d_flag, 0, sizeof(unsigned), s);
+    k_check_div<<<148 * 8, 256, 0, s>>>(det, rdet, lo_bits, hi_bits - lo_bits, d_flag);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(h_result, d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);
+}
+
+cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
+                               const int *view_list, int n_views, const int *d_conds, int n_cond, int G,
+                               const float *d_magsig, const void *vol, float *out, int mode, int views_per_cta,
+                               int storage, cudaStream_t s) {
+    if (n_views <= 0 || n_cond <= 0) return cudaSuccess;
+    FwdColArgs a;
+    a.g = g;
+    a.frames = frames;
+    a.view_list = view_list;
+    a.n_views = n_views;
+    a.conds = d_conds;
+    a.magsig = d_magsig;
+    a.vol = vol;
+    a.out = out;
+    a.basis = d_basis;
+    a.nbg = (g.N + 15) / 16;
+    a.nba = (g.N + 7) / 8;
+    const int nbb = (g.N + 7) / 8;
+    const long bricks = (long)a.nbg * a.nba * nbb;
+    int vpc = views_per_cta;
+    if (vpc <= 0) {
+        const long ctas = bricks * n_cond;
+        const long chunks = ctas >= 2048 ? 1 : (2048 + ctas - 1) / ctas;
+        vpc = (int)((n_views + chunks - 1) / chunks);
+    }
+    vpc = vpc < 1 ? 1 : (vpc > 64 ? 64 : vpc);
+    vpc = vpc > n_views ? n_views : vpc;
+    a.vpc = vpc;
+    const dim3 grid((unsigned)bricks, (unsigned)n_cond, (unsigned)((n_views + vpc - 1) / vpc));
+    const size_t smem = 4 * kTileCap * sizeof(int) + vpc * (sizeof(int4) + sizeof(ViewFrame));
+#define XR_FWD_COL(M, GG, TT)                                                                                     \
+    do {                                                                                                          \
+        cudaError_t e = cudaFuncSetAttribute(k_fwd_col<M, GG, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                                             (int)smem);                                                          \
+        if (e != cudaSuccess) return e;                                                                           \
+        k_fwd_col<M, GG, TT><<<grid, kFwdThreads, smem, s>>>(a);                                                  \
+    } while (0)
+#define XR_FWD_COL_G(M, TT)                                                                                       \
+    do {                                                                                                          \
+        if (G == 0) XR_FWD_COL(M, 0, TT); else if (G == 1) XR_FWD_COL(M, 1, TT); else XR_FWD_COL(M, 2, TT);      \
+    } while (0)
+    if (mode == 2) {
+        XR_FWD_COL_G(2, float);
+    } else if (storage == kBF16) {
+        if (mode == 0) XR_FWD_COL_G(0, __nv_bfloat16); else XR_FWD_COL_G(1, __nv_bfloat16);
+    } else if (storage == kF16) {
+        if (mode == 0) XR_FWD_COL_G(0, __half); else XR_FWD_COL_G(1, __half);
+    } else {
+        if (mode == 0) XR_FWD_COL_G(0, float); else XR_FWD_COL_G(1, float);
+    }
+#undef XR_FWD_COL_G
+#undef XR_FWD_COL
+    return cudaGetLastError();
+}
+
+cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
+                            const int *view_list, int n_views, const int *d_conds, int n_cond, const int *d_axis_g,
+                            const float *d_magsig, const float *proj, void *vol, const float *fac_in, float *fac_out,
+                            int mode, int art, float alpha, int storage, cudaStream_t s) {
+    BackColArgs a;
+    a.g = g;
+    a.frames = frames;
+    a.view_list = view_list;
+    a.n_views = n_views;
+    a.n_cond = n_cond;
+    a.conds = d_conds;
+    a.axis_g = d_axis_g;
+    a.magsig = d_magsig;
+    a.proj = proj;
+    a.vol = vol;
+    a.fac_in = fac_in;
+    a.fac_out = fac_out;
+    a.basis = d_basis;
+    a.art = art;
+    a.alpha = alpha;
+    const int nb8 = (g.N + 7) / 8;
+    const unsigned blocks = (unsigned)((long)nb8 * nb8 * nb8);
+    const size_t smem = (mode == B_PLAIN) ? 0 : (size_t)g.K * 512 * sizeof(float);
+#define XR_BACK_COL(M, TT)                                                                                        \
+    do {                                                                                                          \
+        cudaError_t e = cudaFuncSetAttribute(k_back_col<M, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                                             (int)smem);                                                          \
+        if (e != cudaSuccess) return e;                                                                           \
+        k_back_col<M, TT><<<blocks, kBackThreads, smem, s>>>(a);                                                  \
+    } while (0)
+    if (mode == B_SENS) {
+        XR_BACK_COL(B_SENS, float);
+    } else if (storage == kBF16) {
+        if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, __nv_bfloat16); else XR_BACK_COL(B_XTT, __nv_bfloat16);
+    } else if (storage == kF16) {
+        if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, __half); else XR_BACK_COL(B_XTT, __half);
+    } else {
+        if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, float); else XR_BACK_COL(B_XTT, float);
+    }
+#undef XR_BACK_COL
+    return cudaGetLastError();
+}
+
+}  // namespace xr

@@ -23,6 +23,10 @@
 #include "xr_json.h"
 
 namespace xr {
+inline size_t storage_bytes(int storage) { return storage == 0 ? 4 : 2; }
+}
+
+namespace xr {
 
 constexpr int kMaxBasisXTT = 16; /* XTT back-projection keeps 2 accumulators per channel in registers */
 
@@ -172,6 +176,8 @@ static void fill_consts(xr_ctx *c) {
     g.ratio = (g.vs * g.vs) / (c->det * (c->sod / c->sdd) * c->det * (c->sod / c->sdd)); /* ir.cu:1513 */
     g.sod = c->sod;
     g.sdd = c->sdd;
+    g.rdet = 1.0f / c->det;
+    g.exact_rdet = 0;                                /* set by ensure_device after the check */
     BasisConst &b = c->bc;
     std::memset(&b, 0, sizeof(b));
     for (int k = 0; k < c->K; k++) {
@@ -223,11 +229,100 @@ static xr_status ensure_device(xr_ctx *c) {
         if (st) return st;
     }
     if ((st = ensure(c, c->loss, kLossSlots * sizeof(double), "loss"))) return st;
+    /* a/det as a corrected product only where it equals IEEE division bit for bit */
+    unsigned *h_bad = reinterpret_cast<unsigned *>(c->h_loss);
+    st = cuda_check(c, check_exact_rdet(c->det, c->gc.rdet, (unsigned *)c->loss.p, h_bad, c->stream),
+                    "division check");
+    if (st) return st;
+    c->gc.exact_rdet = (*h_bad == 0) ? 1 : 0;
     c->dev_ready = true;
     return XR_OK;
 }
 
 static const BasisConst *dbasis(xr_ctx *c) { return (const BasisConst *)c->basis_dev.p; }
+
+/* Device layout of the column information (xr_ctx::colinfo). */
+struct ColInfo {
+    int axis_g[kMaxCond];        /* column axis of each axis, -1: general    */
+    float magsig[kMaxCond];      /* sign(ev[g]) * sdd/sod                    */
+    int all[kMaxCond];           /* 0, 1, ..., C-1                           */
+    int group[3][kMaxCond];      /* axes whose column axis is 0, 1, 2        */
+};
+
+/* An axis is column-aligned when, for every view, the detector v axis is
+ * exactly +-e_g and the source and u axis have exactly zero g component:
+ * then u is the same along every voxel column parallel to g. */
+static int aligned_axis(const std::vector<ViewFrame> &h, int cond, int V, float *sign) {
+    const ViewFrame &f0 = h[(size_t)cond * V];
+    int g = -1;
+    for (int i = 0; i < 3; i++)
+        if (f0.ev[i] == 1.0f || f0.ev[i] == -1.0f) g = i;
+    if (g < 0) return -1;
+    *sign = f0.ev[g];
+    for (int v = 0; v < V; v++) {
+        const ViewFrame &f = h[(size_t)cond * V + v];
+        for (int i = 0; i < 3; i++) {
+            if (i == g) {
+                if (f.ev[i] != *sign) return -1;
+            } else if (f.ev[i] != 0.0f) {
+                return -1;
+            }
+        }
+        if (f.src[g] != 0.0f || f.eu[g] != 0.0f) return -1;
+    }
+    return g;
+}
+
+static const ColInfo *dcol(xr_ctx *c) { return (const ColInfo *)c->colinfo.p; }
+
+/* Forward splat of the listed views of the listed axes: column kernels for
+ * column-aligned axes (grouped by column axis), the general kernel else.
+ * vol is the channel base (plain: the axis's own volume when one axis). */
+static cudaError_t forward_dispatch(xr_ctx *c, const int *vl, int n_views, const std::vector<int> &conds,
+                                    const void *vol, float *out, int mode, int storage) {
+    const ViewFrame *fr = (const ViewFrame *)c->frames.p;
+    const ColInfo *ci = dcol(c);
+    std::vector<int> grp[3];
+    for (int cond : conds) {
+        const int g = c->axis_g[cond];
+        if (g < 0) {
+            cudaError_t e = launch_forward(c->gc, dbasis(c), fr, vl, n_views, cond, 1, vol, out, mode,
+                                           c->views_per_cta, storage, c->stream);
+            if (e != cudaSuccess) return e;
+        } else {
+            grp[g].push_back(cond);
+        }
+    }
+    for (int g = 0; g < 3; g++) {
+        if (grp[g].empty()) continue;
+        /* the device group list holds every axis of column axis g in order;
+         * a single axis uses its entry of the identity list instead */
+        const int *dl = (grp[g].size() == 1) ? &ci->all[grp[g][0]] : ci->group[g];
+        if (grp[g].size() != 1) {
+            int n_in_group = 0;
+            for (int cond = 0; cond < c->C; cond++) n_in_group += (c->axis_g[cond] == g);
+            if ((int)grp[g].size() != n_in_group) {   /* a strict subset: one launch per axis */
+                for (int cond : grp[g]) {
+                    cudaError_t e = launch_forward_col(c->gc, dbasis(c), fr, vl, n_views, &ci->all[cond], 1, g,
+                                                       ci->magsig, vol, out, mode, c->views_per_cta, storage,
+                                                       c->stream);
+                    if (e != cudaSuccess) return e;
+                }
+                continue;
+            }
+        }
+        cudaError_t e = launch_forward_col(c->gc, dbasis(c), fr, vl, n_views, dl, (int)grp[g].size(), g, ci->magsig,
+                                           vol, out, mode, c->views_per_cta, storage, c->stream);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+static std::vector<int> all_conds(const xr_ctx *c) {
+    std::vector<int> v(c->C);
+    for (int i = 0; i < c->C; i++) v[i] = i;
+    return v;
+}
 
 /* Frame table for the rotation direction and the normaliser L/(sum c + 1e-5)
  * for every axis and view (geometry only; computed once per context). */
@@ -238,6 +333,25 @@ static xr_status ensure_frames(xr_ctx *c, int rotation) {
         std::vector<ViewFrame> h(nf);
         for (int cond = 0; cond < c->C; cond++)
             for (int v = 0; v < c->V; v++) h[(size_t)cond * c->V + v] = make_frame(c, cond, rotation * v, false);
+        ColInfo ci;
+        std::memset(&ci, 0, sizeof(ci));
+        c->axis_g.assign(c->C, -1);
+        c->all_aligned = true;
+        int ng[3] = {0, 0, 0};
+        for (int cond = 0; cond < c->C; cond++) {
+            float sg = 1.0f;
+            const int g = aligned_axis(h, cond, c->V, &sg);
+            c->axis_g[cond] = g;
+            ci.axis_g[cond] = g;
+            ci.magsig[cond] = sg * c->gc.mag;
+            ci.all[cond] = cond;
+            if (g < 0) c->all_aligned = false;
+            else ci.group[g][ng[g]++] = cond;
+        }
+        if ((st = ensure(c, c->colinfo, sizeof(ColInfo), "column info"))) return st;
+        st = cuda_check(c, cudaMemcpyAsync(c->colinfo.p, &ci, sizeof(ColInfo), cudaMemcpyHostToDevice, c->stream),
+                        "upload column info");
+        if (st) return st;
         if ((st = ensure(c, c->frames, nf * sizeof(ViewFrame), "frames"))) return st;
         st = cuda_check(c, cudaMemcpyAsync(c->frames.p, h.data(), nf * sizeof(ViewFrame), cudaMemcpyHostToDevice,
                                            c->stream), "upload frames");
@@ -246,6 +360,7 @@ static xr_status ensure_frames(xr_ctx *c, int rotation) {
         if (st) return st;
         c->frames_rotation = rotation;
         c->norm_valid = false;
+        c->col_rotation = rotation;
     }
     if (!c->norm_valid) {
         const size_t npx = nf * (size_t)c->Nd * c->Nd;
@@ -258,9 +373,8 @@ static xr_status ensure_frames(xr_ctx *c, int rotation) {
         {
             Timed t(c, XR_T_SETUP);
             cudaMemsetAsync(c->norm.p, 0, npx * sizeof(float), c->stream);
-            st = cuda_check(c, launch_forward(c->gc, dbasis(c), (const ViewFrame *)c->frames.p, (const int *)lst.p,
-                                              c->V, 0, c->C, nullptr, (float *)c->norm.p, 2, c->views_per_cta,
-                                              c->stream), "weight splat");
+            st = cuda_check(c, forward_dispatch(c, (const int *)lst.p, c->V, all_conds(c), nullptr,
+                                                (float *)c->norm.p, 2, 0), "weight splat");
         }
         if (!st) {
             Timed t(c, XR_T_SETUP);
@@ -310,6 +424,101 @@ static bool floats(const JVal *v, std::vector<float> &out) {
         out.push_back((float)e.n);
     }
     return true;
+}
+
+/* Enqueue one epoch's device work on the context stream for the given
+ * subset orders (XTT: one row; IR: one row per axis). */
+static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
+    Session &s = c->sess;
+    xr_status st;
+    cudaStream_t str = c->stream;
+    const size_t NdNd = (size_t)c->Nd * c->Nd;
+    const size_t blk = (size_t)c->V * NdNd;
+    const size_t N3 = (size_t)c->N * c->N * c->N;
+    const float alpha = s.lambda / (float)s.subset_size;   /* reconstruct.cu:124 / :906 */
+    const ViewFrame *fr = (const ViewFrame *)c->frames.p;
+    float *proj = (float *)c->proj.p;
+    const float *norm = (const float *)c->norm.p;
+    double *dl = (double *)c->loss.p;
+    cudaMemsetAsync(dl, 0, kMaxCond * sizeof(double), str);
+    if (s.xtt) {
+        /* XTT::reconstruct epoch, reconstruct.cu:857-917: the ratio images of
+         * every axis are cleared once per epoch. */
+        cudaMemsetAsync(proj, 0, (size_t)c->C * blk * sizeof(float), str);
+        for (int b = 0; b < s.batch; b++) {
+            const int *vl = (const int *)c->subsets.p + (size_t)orders[b] * s.subset_size;
+            {
+                Timed t(c, XR_T_FORWARD);
+                if ((st = cuda_check(c, forward_dispatch(c, vl, s.subset_size, all_conds(c), s.d_vol, proj, 1,
+                                                         s.storage), "XTT forward")))
+                    return st;
+            }
+            {
+                Timed t(c, XR_T_RATIO);
+                if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, norm, s.d_sino, s.art,
+                                                     dl, s.storage, str), "ratio")))
+                    return st;
+            }
+            {
+                Timed t(c, XR_T_BACK);
+                cudaError_t e;
+                if (c->all_aligned) {
+                    const ColInfo *ci = dcol(c);
+                    const float *sens =
+                        s.art ? nullptr : (const float *)c->sens.p + (size_t)orders[b] * c->K * N3;
+                    e = launch_back_col(c->gc, dbasis(c), fr, vl, s.subset_size, ci->all, c->C, ci->axis_g,
+                                        ci->magsig, proj, s.d_vol, sens, nullptr, 1, s.art, alpha, s.storage, str);
+                } else {
+                    e = launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, 0, c->C, proj, s.d_vol, 1, s.art,
+                                           alpha, s.storage, str);
+                }
+                if ((st = cuda_check(c, e, "XTT back"))) return st;
+            }
+        }
+    } else {
+        /* IR::reconstruct epoch (reconstruct.cu:80-132) of every axis. */
+        for (int cond = 0; cond < c->C; cond++) {
+            const int *order = &orders[(size_t)cond * s.batch];
+            float *pc = proj + (size_t)cond * blk;
+            void *vc = (char *)s.d_vol + (size_t)cond * N3 * storage_bytes(s.storage);
+            const void *bc = (const char *)s.d_sino + (size_t)cond * blk * storage_bytes(s.storage);
+            cudaMemsetAsync(pc, 0, blk * sizeof(float), str);
+            for (int b = 0; b < s.batch; b++) {
+                const int *vl = (const int *)c->subsets.p + (size_t)order[b] * s.subset_size;
+                {
+                    Timed t(c, XR_T_FORWARD);
+                    if ((st = cuda_check(c, forward_dispatch(c, vl, s.subset_size, std::vector<int>{cond}, vc, proj, 0,
+                                                             s.storage), "forward")))
+                        return st;
+                }
+                {
+                    Timed t(c, XR_T_RATIO);
+                    if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, 1, pc, norm + (size_t)cond * blk,
+                                                         bc, s.art, dl + cond, s.storage, str), "ratio")))
+                        return st;
+                }
+                {
+                    Timed t(c, XR_T_BACK);
+                    cudaError_t e;
+                    if (c->axis_g[cond] >= 0) {
+                        const ColInfo *ci = dcol(c);
+                        e = launch_back_col(c->gc, dbasis(c), fr, vl, s.subset_size, &ci->all[cond], 1, ci->axis_g,
+                                            ci->magsig, proj, vc, nullptr, nullptr, 0, s.art, alpha, s.storage, str);
+                    } else {
+                        e = launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, cond, 1, proj, vc, 0, s.art,
+                                               alpha, s.storage, str);
+                    }
+                    if ((st = cuda_check(c, e, "back"))) return st;
+                }
+            }
+        }
+    }
+    return XR_OK;
+}
+
+static void drop_graphs(xr_ctx *c) {
+    for (auto &kv : c->sess.graphs) cudaGraphExecDestroy(kv.second);
+    c->sess.graphs.clear();
 }
 
 }  // namespace xr
@@ -448,6 +657,7 @@ void xr_destroy(xr_ctx *c) {
     if (c->dev_ready) {
         cudaSetDevice(c->device);
         cudaStreamSynchronize(c->stream);
+        drop_graphs(c);
         timing_collect(c);
         for (auto &pr : c->timing.pool) {
             cudaEventDestroy(pr.first);
@@ -462,7 +672,10 @@ void xr_destroy(xr_ctx *c) {
     release(c->scratch_vol);
     release(c->scratch_sino);
     release(c->scratch_md);
+    release(c->stage);
     release(c->basis_dev);
+    release(c->colinfo);
+    release(c->sens);
     release(c->fdk_frames);
     release(c->fdk_filt);
     release(c->fdk_weight);
@@ -515,8 +728,10 @@ xr_status xr_set_option(xr_ctx *c, int key, int value) {
             if (value < 0 || value > 64) return fail(c, XR_ERR_ARG, "views per CTA must be in [0, 64]");
             c->views_per_cta = value;
             return XR_OK;
+        case XR_OPT_GRAPHS: c->use_graphs = value != 0; return XR_OK;
         case XR_OPT_STORAGE:
-            if (value != 0) return fail(c, XR_ERR_ARG, "only FP32 storage (0) is available");
+            if (value < 0 || value > 2) return fail(c, XR_ERR_ARG, "storage must be 0 (FP32), 1 (BF16) or 2 (FP16)");
+            if (c->sess.active) return fail(c, XR_ERR_STATE, "storage cannot change during a session");
             c->storage = value;
             return XR_OK;
         default: return fail(c, XR_ERR_ARG, "unknown option " + std::to_string(key));
@@ -546,7 +761,7 @@ xr_status xr_reset_timings(xr_ctx *c) {
 
 /* ------------------------------------------------------------- sessions */
 
-xr_status xr_dev_session_begin(xr_ctx *c, const float *d_sino, float *d_vol, int xtt, int epochs, int batch,
+xr_status xr_dev_session_begin(xr_ctx *c, const void *d_sino, void *d_vol, int xtt, int epochs, int batch,
                                xr_rotate dir, xr_method method, float lambda) {
     if (!c || !d_sino || !d_vol) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
     if (batch < 1 || batch > c->V) return fail(c, XR_ERR_ARG, "batch must be in [1, num_proj]");
@@ -560,6 +775,7 @@ xr_status xr_dev_session_begin(xr_ctx *c, const float *d_sino, float *d_vol, int
     const int rotation = dir == XR_ROTATE_CW ? 1 : -1;
     if ((st = ensure_frames(c, rotation))) return st;
     Session &s = c->sess;
+    drop_graphs(c);
     s = Session();
     s.xtt = xtt != 0;
     s.epochs = epochs;
@@ -570,6 +786,7 @@ xr_status xr_dev_session_begin(xr_ctx *c, const float *d_sino, float *d_vol, int
     s.lambda = lambda;
     s.d_sino = d_sino;
     s.d_vol = d_vol;
+    s.storage = c->storage;
     std::vector<int> lists((size_t)batch * s.subset_size);
     for (int sub = 0; sub < batch; sub++)
         for (int j = 0; j < s.subset_size; j++)   /* n = (sub + batch*j) % nProj, reconstruct.cu:89 */
@@ -593,6 +810,22 @@ xr_status xr_dev_session_begin(xr_ctx *c, const float *d_sino, float *d_vol, int
             std::copy(o.begin(), o.end(), s.ir_orders.begin() + r * batch);
         }
     }
+    if (s.xtt && c->all_aligned && !s.art) {
+        /* factor_k of every subset (geometry only): sum over the subset's views
+         * of (|B x S_k| |S_k . G|)^2 (ir.cu:1847), once per session. */
+        const size_t N3 = (size_t)c->N * c->N * c->N;
+        if ((st = ensure(c, c->sens, (size_t)batch * c->K * N3 * sizeof(float), "sensitivity"))) return st;
+        const ColInfo *ci = dcol(c);
+        for (int sub = 0; sub < batch; sub++) {
+            Timed t(c, XR_T_SETUP);
+            st = cuda_check(c, launch_back_col(c->gc, dbasis(c), (const ViewFrame *)c->frames.p,
+                                               (const int *)c->subsets.p + (size_t)sub * s.subset_size, s.subset_size,
+                                               ci->all, c->C, ci->axis_g, ci->magsig, nullptr, nullptr, nullptr,
+                                               (float *)c->sens.p + (size_t)sub * c->K * N3, 2, 0, 0.f, 0, c->stream),
+                            "sensitivity");
+            if (st) return st;
+        }
+    }
     st = cuda_check(c, cudaStreamSynchronize(c->stream), "session begin");
     if (st) return st;
     s.active = true;
@@ -607,76 +840,45 @@ xr_status xr_dev_session_epoch(xr_ctx *c, double *loss) {
         return fail(c, XR_ERR_STATE, "IR session: all planned epochs already run");
     xr_status st;
     cudaStream_t str = c->stream;
-    const size_t NdNd = (size_t)c->Nd * c->Nd;
-    const size_t blk = (size_t)c->V * NdNd;
-    const size_t N3 = (size_t)c->N * c->N * c->N;
-    const float alpha = s.lambda / (float)s.subset_size;   /* reconstruct.cu:124 / :906 */
-    const ViewFrame *fr = (const ViewFrame *)c->frames.p;
-    float *proj = (float *)c->proj.p;
-    const float *norm = (const float *)c->norm.p;
-    double *dl = (double *)c->loss.p;
-    cudaMemsetAsync(dl, 0, kMaxCond * sizeof(double), str);
+    std::vector<int> orders;
     if (s.xtt) {
-        /* XTT::reconstruct epoch, reconstruct.cu:857-917: a fresh default
-         * engine shuffles the persistent order; the ratio images of every
-         * axis are cleared once per epoch. */
+        /* a fresh default engine shuffles the persistent order (reconstruct.cu:858-859) */
         std::mt19937_64 eng;
         std::shuffle(s.order.begin(), s.order.end(), eng);
-        cudaMemsetAsync(proj, 0, (size_t)c->C * blk * sizeof(float), str);
-        for (int b = 0; b < s.batch; b++) {
-            const int *vl = (const int *)c->subsets.p + (size_t)s.order[b] * s.subset_size;
-            {
-                Timed t(c, XR_T_FORWARD);
-                if ((st = cuda_check(c, launch_forward(c->gc, dbasis(c), fr, vl, s.subset_size, 0, c->C, s.d_vol,
-                                                       proj, 1, c->views_per_cta, str), "XTT forward")))
-                    return st;
-            }
-            {
-                Timed t(c, XR_T_RATIO);
-                if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, norm, s.d_sino, s.art,
-                                                     dl, str), "ratio")))
-                    return st;
-            }
-            {
-                Timed t(c, XR_T_BACK);
-                if ((st = cuda_check(c, launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, 0, c->C, proj,
-                                                           s.d_vol, 1, s.art, alpha, str), "XTT back")))
-                    return st;
-            }
-        }
+        orders = s.order;
     } else {
-        /* IR::reconstruct epoch (reconstruct.cu:80-132) of every axis. */
         for (int cond = 0; cond < c->C; cond++) {
-            const int *order = &s.ir_orders[((size_t)cond * s.epochs + s.epoch_done) * s.batch];
-            float *pc = proj + (size_t)cond * blk;
-            float *vc = s.d_vol + (size_t)cond * N3;
-            cudaMemsetAsync(pc, 0, blk * sizeof(float), str);
-            for (int b = 0; b < s.batch; b++) {
-                const int *vl = (const int *)c->subsets.p + (size_t)order[b] * s.subset_size;
-                {
-                    Timed t(c, XR_T_FORWARD);
-                    if ((st = cuda_check(c, launch_forward(c->gc, dbasis(c), fr, vl, s.subset_size, cond, 1, vc,
-                                                           proj, 0, c->views_per_cta, str), "forward")))
-                        return st;
-                }
-                {
-                    Timed t(c, XR_T_RATIO);
-                    if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, 1, pc, norm + (size_t)cond * blk,
-                                                         s.d_sino + (size_t)cond * blk, s.art, dl + cond,
-                                                         str), "ratio")))
-                        return st;
-                }
-                {
-                    Timed t(c, XR_T_BACK);
-                    if ((st = cuda_check(c, launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, cond, 1,
-                                                               proj, vc, 0, s.art, alpha, str), "back")))
-                        return st;
-                }
-            }
+            const int *o = &s.ir_orders[((size_t)cond * s.epochs + s.epoch_done) * s.batch];
+            orders.insert(orders.end(), o, o + s.batch);
         }
+    }
+    if (c->use_graphs && !c->timing.on) {
+        /* one CUDA graph per distinct subset order, captured on first use */
+        auto it = s.graphs.find(orders);
+        if (it == s.graphs.end()) {
+            if ((st = cuda_check(c, cudaStreamBeginCapture(str, cudaStreamCaptureModeRelaxed), "begin capture")))
+                return st;
+            const xr_status ist = issue_epoch(c, orders);
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(str, &graph);
+            if (ist) {
+                if (graph) cudaGraphDestroy(graph);
+                return ist;
+            }
+            if ((st = cuda_check(c, ce, "end capture"))) return st;
+            cudaGraphExec_t exec = nullptr;
+            const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if ((st = cuda_check(c, ie, "graph instantiate"))) return st;
+            it = s.graphs.emplace(orders, exec).first;
+        }
+        if ((st = cuda_check(c, cudaGraphLaunch(it->second, str), "graph launch"))) return st;
+    } else {
+        if ((st = issue_epoch(c, orders))) return st;
     }
     s.epoch_done++;
     if (loss) {
+        double *dl = (double *)c->loss.p;
         st = cuda_check(c, cudaMemcpyAsync(c->h_loss, dl, kMaxCond * sizeof(double), cudaMemcpyDeviceToHost, str),
                         "loss copy");
         if (st) return st;
@@ -699,15 +901,16 @@ xr_status xr_dev_session_end(xr_ctx *c, float *d_md, float *d_ev) {
         const long nvox = (long)c->N * c->N * c->N;
         {
             Timed t(c, XR_T_ORIENT);
-            st = cuda_check(c, launch_sqrt_abs(nvox * c->K, s.d_vol, c->stream), "sqrt");   /* reconstruct.cu:919-922 */
+            st = cuda_check(c, launch_sqrt_abs(nvox * c->K, s.d_vol, s.storage, c->stream), "sqrt");   /* reconstruct.cu:919-922 */
         }
         if (!st && d_md) {
             Timed t(c, XR_T_ORIENT);
-            st = cuda_check(c, launch_orientation(nvox, c->K, dbasis(c), s.d_vol, d_md, d_ev, c->stream),
+            st = cuda_check(c, launch_orientation(nvox, c->K, dbasis(c), s.d_vol, d_md, d_ev, s.storage, c->stream),
                             "orientation");
         }
     }
     if (!st) st = cuda_check(c, cudaStreamSynchronize(c->stream), "session end");
+    drop_graphs(c);
     s.active = false;
     return st;
 }
@@ -720,7 +923,8 @@ xr_status xr_dev_session_proj(xr_ctx *c, const float **d_proj) {
 
 /* ---------------------------------------------------- device-buffer calls */
 
-static xr_status forward_into(xr_ctx *c, const float *d_vol, float *d_out, int rotation, int mode, bool normalise) {
+static xr_status forward_into(xr_ctx *c, const void *d_vol, float *d_out, int rotation, int mode, bool normalise,
+                              int storage) {
     xr_status st;
     if ((st = ensure_frames(c, rotation))) return st;
     const size_t npx = (size_t)c->C * c->V * c->Nd * c->Nd;
@@ -732,8 +936,7 @@ static xr_status forward_into(xr_ctx *c, const float *d_vol, float *d_out, int r
     cudaMemsetAsync(d_out, 0, npx * sizeof(float), c->stream);
     {
         Timed t(c, XR_T_FORWARD);
-        st = cuda_check(c, launch_forward(c->gc, dbasis(c), (const ViewFrame *)c->frames.p, (const int *)lst.p,
-                                          c->V, 0, c->C, d_vol, d_out, mode, c->views_per_cta, c->stream),
+        st = cuda_check(c, forward_dispatch(c, (const int *)lst.p, c->V, all_conds(c), d_vol, d_out, mode, storage),
                         "forward");
     }
     if (!st && normalise) {
@@ -745,15 +948,15 @@ static xr_status forward_into(xr_ctx *c, const float *d_vol, float *d_out, int r
     return st;
 }
 
-xr_status xr_dev_forward(xr_ctx *c, const float *d_vol, float *d_sino, xr_rotate dir, int xtt) {
+xr_status xr_dev_forward(xr_ctx *c, const void *d_vol, float *d_sino, xr_rotate dir, int xtt) {
     if (!c || !d_vol || !d_sino) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
     xr_status st;
     if (xtt && (st = check_xtt_k(c))) return st;
     if ((st = ensure_device(c))) return st;
-    return forward_into(c, d_vol, d_sino, dir == XR_ROTATE_CCW ? -1 : 1, xtt ? 1 : 0, true);
+    return forward_into(c, d_vol, d_sino, dir == XR_ROTATE_CCW ? -1 : 1, xtt ? 1 : 0, true, c->storage);
 }
 
-xr_status xr_dev_residual(xr_ctx *c, const float *d_vol, const float *d_sino, xr_rotate dir, int xtt,
+xr_status xr_dev_residual(xr_ctx *c, const void *d_vol, const void *d_sino, xr_rotate dir, int xtt,
                           double *rel_l2, double *l1) {
     if (!c || !d_vol || !d_sino) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
     xr_status st;
@@ -762,12 +965,13 @@ xr_status xr_dev_residual(xr_ctx *c, const float *d_vol, const float *d_sino, xr
     const size_t npx = (size_t)c->C * c->V * c->Nd * c->Nd;
     if ((st = ensure(c, c->scratch_sino, npx * sizeof(float), "residual scratch"))) return st;
     float *p = (float *)c->scratch_sino.p;
-    if ((st = forward_into(c, d_vol, p, dir == XR_ROTATE_CCW ? -1 : 1, xtt ? 1 : 0, true))) return st;
+    if ((st = forward_into(c, d_vol, p, dir == XR_ROTATE_CCW ? -1 : 1, xtt ? 1 : 0, true, c->storage))) return st;
     double *dl = (double *)c->loss.p + 40;
     cudaMemsetAsync(dl, 0, 3 * sizeof(double), c->stream);
     {
         Timed t(c, XR_T_OTHER);
-        if ((st = cuda_check(c, launch_residual((long)npx, p, d_sino, dl, c->stream), "residual"))) return st;
+        if ((st = cuda_check(c, launch_residual((long)npx, p, d_sino, dl, c->storage, c->stream), "residual")))
+            return st;
     }
     if ((st = cuda_check(c, cudaMemcpyAsync(c->h_loss, dl, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
                          "residual copy")))
@@ -778,14 +982,14 @@ xr_status xr_dev_residual(xr_ctx *c, const float *d_vol, const float *d_sino, xr
     return XR_OK;
 }
 
-xr_status xr_dev_orientation(xr_ctx *c, const float *d_mu, float *d_md, float *d_ev) {
+xr_status xr_dev_orientation(xr_ctx *c, const void *d_mu, float *d_md, float *d_ev) {
     if (!c || !d_mu || !d_md) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
     xr_status st;
     if ((st = ensure_device(c))) return st;
     {
         Timed t(c, XR_T_ORIENT);
         st = cuda_check(c, launch_orientation((long)c->N * c->N * c->N, c->K, dbasis(c), d_mu, d_md, d_ev,
-                                              c->stream), "orientation");
+                                              c->storage, c->stream), "orientation");
     }
     if (!st) st = cuda_check(c, cudaStreamSynchronize(c->stream), "orientation");
     return st;
@@ -818,16 +1022,38 @@ static xr_status download_planes(xr_ctx *c, const float *d, float *const *dst, i
     return cuda_check(c, cudaStreamSynchronize(c->stream), what);
 }
 
+/* Host float planes into `b` in the storage type (through the FP32 staging
+ * buffer when the storage is 16-bit), and back. */
+static xr_status upload_planes_s(xr_ctx *c, DevBuf &b, const float *const *src, int planes, size_t plane_elems,
+                                 int storage, const char *what) {
+    if (storage == 0) return upload_planes(c, b, src, planes, plane_elems, what);
+    xr_status st;
+    const size_t n = (size_t)planes * plane_elems;
+    if ((st = upload_planes(c, c->stage, src, planes, plane_elems, what))) return st;
+    if ((st = ensure(c, b, n * storage_bytes(storage), what))) return st;
+    return cuda_check(c, launch_convert((long)n, c->stage.p, 0, b.p, storage, c->stream), what);
+}
+
+static xr_status download_planes_s(xr_ctx *c, const void *d, float *const *dst, int planes, size_t plane_elems,
+                                   int storage, const char *what) {
+    if (storage == 0) return download_planes(c, (const float *)d, dst, planes, plane_elems, what);
+    xr_status st;
+    const size_t n = (size_t)planes * plane_elems;
+    if ((st = ensure(c, c->stage, n * sizeof(float), what))) return st;
+    if ((st = cuda_check(c, launch_convert((long)n, d, storage, c->stage.p, 0, c->stream), what))) return st;
+    return download_planes(c, (const float *)c->stage.p, dst, planes, plane_elems, what);
+}
+
 xr_status xr_forward(xr_ctx *c, const float *const *voxel, float *const *sino, xr_rotate dir, int xtt) {
     if (!c || !voxel || !sino) return c ? fail(c, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
     xr_status st;
     if (xtt && (st = check_xtt_k(c))) return st;
     if ((st = ensure_device(c))) return st;
     const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
-    if ((st = upload_planes(c, c->scratch_vol, voxel, xtt ? c->K : 1, N3, "volume"))) return st;
+    if ((st = upload_planes_s(c, c->scratch_vol, voxel, xtt ? c->K : 1, N3, c->storage, "volume"))) return st;
     if ((st = ensure(c, c->scratch_sino, c->C * blk * sizeof(float), "sinogram"))) return st;
-    if ((st = forward_into(c, (const float *)c->scratch_vol.p, (float *)c->scratch_sino.p,
-                           dir == XR_ROTATE_CCW ? -1 : 1, xtt ? 1 : 0, true)))
+    if ((st = forward_into(c, c->scratch_vol.p, (float *)c->scratch_sino.p, dir == XR_ROTATE_CCW ? -1 : 1,
+                           xtt ? 1 : 0, true, c->storage)))
         return st;
     return download_planes(c, (const float *)c->scratch_sino.p, sino, c->C, blk, "sinogram");
 }
@@ -842,8 +1068,8 @@ xr_status xr_forward_proj_only(xr_ctx *c, const float *const *voxel, float *cons
     const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
     if ((st = upload_planes(c, c->scratch_vol, voxel, 1, N3, "volume"))) return st;
     if ((st = ensure(c, c->scratch_sino, c->C * blk * sizeof(float), "sinogram"))) return st;
-    if ((st = forward_into(c, (const float *)c->scratch_vol.p, (float *)c->scratch_sino.p,
-                           dir == XR_ROTATE_CCW ? -1 : 1, 0, false)))
+    if ((st = forward_into(c, c->scratch_vol.p, (float *)c->scratch_sino.p, dir == XR_ROTATE_CCW ? -1 : 1, 0,
+                           false, 0)))
         return st;
     return download_planes(c, (const float *)c->scratch_sino.p, sino, c->C, blk, "sinogram");
 }
@@ -855,10 +1081,9 @@ xr_status xr_ir_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel, 
     xr_status st;
     if ((st = ensure_device(c))) return st;
     const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
-    if ((st = upload_planes(c, c->scratch_sino, sino, c->C, blk, "sinogram"))) return st;
-    if ((st = upload_planes(c, c->scratch_vol, voxel, c->C, N3, "volume"))) return st;
-    if ((st = xr_dev_session_begin(c, (const float *)c->scratch_sino.p, (float *)c->scratch_vol.p, 0, epoch, batch,
-                                   dir, method, lambda)))
+    if ((st = upload_planes_s(c, c->scratch_sino, sino, c->C, blk, c->storage, "sinogram"))) return st;
+    if ((st = upload_planes_s(c, c->scratch_vol, voxel, c->C, N3, c->storage, "volume"))) return st;
+    if ((st = xr_dev_session_begin(c, c->scratch_sino.p, c->scratch_vol.p, 0, epoch, batch, dir, method, lambda)))
         return st;
     std::vector<double> l(c->C);
     for (int ep = 0; ep < epoch; ep++) {
@@ -867,7 +1092,7 @@ xr_status xr_ir_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel, 
             for (int cond = 0; cond < c->C; cond++) losses[(size_t)cond * epoch + ep] = (float)l[cond];
     }
     if ((st = xr_dev_session_end(c, nullptr, nullptr))) return st;
-    return download_planes(c, (const float *)c->scratch_vol.p, voxel, c->C, N3, "volume");
+    return download_planes_s(c, c->scratch_vol.p, voxel, c->C, N3, c->storage, "volume");
 }
 
 xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel, float *const *md,
@@ -879,10 +1104,9 @@ xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
     if ((st = check_xtt_k(c))) return st;
     if ((st = ensure_device(c))) return st;
     const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
-    if ((st = upload_planes(c, c->scratch_sino, sino, c->C, blk, "sinogram"))) return st;
-    if ((st = upload_planes(c, c->scratch_vol, voxel, c->K, N3, "volume"))) return st;
-    if ((st = xr_dev_session_begin(c, (const float *)c->scratch_sino.p, (float *)c->scratch_vol.p, 1, epoch, batch,
-                                   dir, method, lambda)))
+    if ((st = upload_planes_s(c, c->scratch_sino, sino, c->C, blk, c->storage, "sinogram"))) return st;
+    if ((st = upload_planes_s(c, c->scratch_vol, voxel, c->K, N3, c->storage, "volume"))) return st;
+    if ((st = xr_dev_session_begin(c, c->scratch_sino.p, c->scratch_vol.p, 1, epoch, batch, dir, method, lambda)))
         return st;
     for (int ep = 0; ep < epoch; ep++) {
         double l = 0;
@@ -896,7 +1120,7 @@ xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
         d_ev = evalue ? d_md + 3 * N3 : nullptr;
     }
     if ((st = xr_dev_session_end(c, d_md, d_ev))) return st;
-    if ((st = download_planes(c, (const float *)c->scratch_vol.p, voxel, c->K, N3, "volume"))) return st;
+    if ((st = download_planes_s(c, c->scratch_vol.p, voxel, c->K, N3, c->storage, "volume"))) return st;
     if ((st = download_planes(c, (const float *)c->proj.p, sino, c->C, blk, "ratio images"))) return st;
     if (md) {
         if ((st = download_planes(c, d_md, md, 3, N3, "md"))) return st;
@@ -910,11 +1134,11 @@ xr_status xr_orientation(xr_ctx *c, const float *const *mu, float *const *md, fl
     xr_status st;
     if ((st = ensure_device(c))) return st;
     const size_t N3 = (size_t)c->N * c->N * c->N;
-    if ((st = upload_planes(c, c->scratch_vol, mu, c->K, N3, "mu"))) return st;
+    if ((st = upload_planes_s(c, c->scratch_vol, mu, c->K, N3, c->storage, "mu"))) return st;
     if ((st = ensure(c, c->scratch_md, 6 * N3 * sizeof(float), "orientation"))) return st;
     float *d_md = (float *)c->scratch_md.p;
     float *d_ev = evalue ? d_md + 3 * N3 : nullptr;
-    if ((st = xr_dev_orientation(c, (const float *)c->scratch_vol.p, d_md, d_ev))) return st;
+    if ((st = xr_dev_orientation(c, c->scratch_vol.p, d_md, d_ev))) return st;
     if ((st = download_planes(c, d_md, md, 3, N3, "md"))) return st;
     if (evalue) return download_planes(c, d_ev, evalue, 3, N3, "evalue");
     return XR_OK;
@@ -958,10 +1182,10 @@ xr_status xr_residual(xr_ctx *c, const float *const *voxel, const float *const *
     if (xtt && (st = check_xtt_k(c))) return st;
     if ((st = ensure_device(c))) return st;
     const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
-    if ((st = upload_planes(c, c->scratch_vol, voxel, xtt ? c->K : 1, N3, "volume"))) return st;
+    if ((st = upload_planes_s(c, c->scratch_vol, voxel, xtt ? c->K : 1, N3, c->storage, "volume"))) return st;
     DevBuf b;
-    if ((st = upload_planes(c, b, sino, c->C, blk, "sinogram"))) return st;
-    st = xr_dev_residual(c, (const float *)c->scratch_vol.p, (const float *)b.p, dir, xtt, rel_l2, l1);
+    if ((st = upload_planes_s(c, b, sino, c->C, blk, c->storage, "sinogram"))) return st;
+    st = xr_dev_residual(c, c->scratch_vol.p, b.p, dir, xtt, rel_l2, l1);
     release(b);
     return st;
 }

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -47,6 +48,9 @@ struct GeomConst {
     float lim;     /* (float)Nd - 0.55f: detector window             */
     float ratio;   /* vs^2 / (det*(sod/sdd)*det*(sod/sdd)) (ir.cu:1513) */
     float sod, sdd;
+    float rdet;    /* RN(1/det)                                      */
+    int exact_rdet;/* 1: a/det as a Markstein-corrected product, checked
+                      bit for bit against IEEE division on this device */
 };
 
 /* XTT basis constants: S_k, |S_k|^2 and g_kc = |S_k . G_c|^2 where
@@ -79,10 +83,12 @@ struct Session {
     int rotation = 1;
     bool art = false;
     float lambda = 0.f;
-    const float *d_sino = nullptr;
-    float *d_vol = nullptr;
+    const void *d_sino = nullptr;     /* storage type */
+    void *d_vol = nullptr;            /* storage type */
+    int storage = 0;
     std::vector<int> order;            /* persistent subset order (XTT)     */
     std::vector<int> ir_orders;        /* C*epochs rows (IR)                */
+    std::map<std::vector<int>, cudaGraphExec_t> graphs;  /* per subset order */
 };
 
 }  // namespace xr
@@ -102,6 +108,7 @@ struct xr_ctx {
     int fdk_axis_blocks = 0;
     int views_per_cta = 0;
     int storage = 0;
+    bool use_graphs = false;
 
     xr::GeomConst gc{};
     xr::BasisConst bc{};
@@ -115,13 +122,20 @@ struct xr_ctx {
     xr::DevBuf proj;                   /* C*V*Nd*Nd: forward / ratio images         */
     xr::DevBuf subsets;                /* batch*subset_size view indices            */
     xr::DevBuf loss;                   /* doubles: loss accumulators                */
-    xr::DevBuf scratch_vol, scratch_sino, scratch_md;
+    xr::DevBuf scratch_vol, scratch_sino, scratch_md, stage;
     xr::DevBuf basis_dev;              /* BasisConst                                */
     xr::DevBuf fdk_frames;             /* C*V ViewFrame with the FDK source         */
     int fdk_rotation = 0;
     xr::DevBuf fdk_filt, fdk_weight, fdk_sf;
     bool dev_ready = false;
     double *h_loss = nullptr;          /* pinned, kLossSlots doubles                */
+
+    /* column-aligned axes (grating direction = +-grid axis for every view) */
+    int col_rotation = 0;              /* rotation the column info was built for   */
+    std::vector<int> axis_g;           /* per axis: column axis 0/1/2, -1 general   */
+    bool all_aligned = false;
+    xr::DevBuf colinfo;                /* int axis_g[C], float magsig[C], int conds[C] */
+    xr::DevBuf sens;                   /* XTT: batch x K x N^3 per-subset sensitivity  */
 
     xr::Session sess;
 };
@@ -141,28 +155,43 @@ void timing_end(xr_ctx *c, int cls, cudaEvent_t ev);
  * weights only (value 1, the reference's devProjFactor).  out: C blocks of
  * V*Nd*Nd, accumulated with float atomics. */
 cudaError_t launch_forward(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
-                           const int *view_list, int n_views, int cond0, int n_cond, const float *vol,
-                           float *out, int mode, int views_per_cta, cudaStream_t s);
+                           const int *view_list, int n_views, int cond0, int n_cond, const void *vol,
+                           float *out, int mode, int views_per_cta, int storage, cudaStream_t s);
 /* Chord-length normaliser: norm = L / (norm + 1e-5) in place, every view. */
 cudaError_t launch_chord(const GeomConst &g, const ViewFrame *frames, float *norm, int n_cond, cudaStream_t s);
 /* Normalise + ratio (MLEM) or subtract (ART) on listed views of every axis,
  * FP64 loss sum added to *loss. */
 cudaError_t launch_ratio(const GeomConst &g, const int *view_list, int n_views, int n_cond, float *proj,
-                         const float *norm, const float *sino, int art, double *loss, cudaStream_t s);
+                         const float *norm, const void *sino, int art, double *loss, int storage, cudaStream_t s);
 /* Normalise only (proj *= norm) on every view: the forward operator A. */
 cudaError_t launch_normalize(const GeomConst &g, int n_cond, float *proj, const float *norm, cudaStream_t s);
 /* Back-projection of the listed views fused with the MLEM / ART update. */
 cudaError_t launch_back_update(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, int cond0, int n_cond, const float *proj,
-                               float *vol, int xtt, int art, float alpha, cudaStream_t s);
+                               void *vol, int xtt, int art, float alpha, int storage, cudaStream_t s);
 /* FP64 sums: out[0] += sum (p-b)^2, out[1] += sum b^2, out[2] += sum |p-b|. */
-cudaError_t launch_residual(long n, const float *p, const float *b, double *out, cudaStream_t s);
+cudaError_t launch_residual(long n, const float *p, const void *b, double *out, int storage, cudaStream_t s);
 /* mu = sqrt|mu| over n values. */
-cudaError_t launch_sqrt_abs(long n, float *mu, cudaStream_t s);
+cudaError_t launch_sqrt_abs(long n, void *mu, int storage, cudaStream_t s);
+/* n values from one storage type to another (0 FP32, 1 BF16, 2 FP16). */
+cudaError_t launch_convert(long n, const void *src, int src_storage, void *dst, int dst_storage, cudaStream_t s);
+
+/* ---- xr_column.cu: kernels for axes whose grating direction is a grid axis ---- */
+cudaError_t check_exact_rdet(float det, float rdet, unsigned *d_flag, unsigned *h_result, cudaStream_t s);
+cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
+                               const int *view_list, int n_views, const int *d_conds, int n_cond, int G,
+                               const float *d_magsig, const void *vol, float *out, int mode, int views_per_cta,
+                               int storage, cudaStream_t s);
+/* mode 0: plain (one axis, update in place); 1: XTT (fac_in = sensitivity);
+ * 2: sensitivity of the listed views into fac_out. */
+cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
+                            const int *view_list, int n_views, const int *d_conds, int n_cond, const int *d_axis_g,
+                            const float *d_magsig, const float *proj, void *vol, const float *fac_in, float *fac_out,
+                            int mode, int art, float alpha, int storage, cudaStream_t s);
 
 /* ---- xr_orient.cu ---- */
-cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, const float *mu, float *md,
-                               float *ev, cudaStream_t s);
+cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, const void *mu, float *md,
+                               float *ev, int storage, cudaStream_t s);
 cudaError_t launch_angle_from_md(long nvox, const float *md, float *angle, cudaStream_t s);
 cudaError_t launch_direction_normalization(long nvox, float *md, cudaStream_t s);
 

@@ -34,13 +34,15 @@
 #include <cuda_runtime.h>
 
 #include "xr_internal.h"
+#include "xr_storage.cuh"
+#include "xr_tile.cuh"
 
 namespace xr {
 namespace {
 
 constexpr int kFwdThreads = 256;
 constexpr int kBX = 16, kBY = 8, kBZ = 8;     /* forward brick                 */
-constexpr int kTileCap = 48 * 48;             /* floats per shared tile        */
+constexpr int kTileCap = 48 * 48;             /* pixels per shared tile        */
 constexpr int kBackThreads = 256;             /* 8 x 4 x 8 brick per CTA       */
 constexpr int kFrameChunk = 128;              /* frames staged in smem at once */
 
@@ -52,6 +54,15 @@ __device__ __forceinline__ float vox_base(int i, int N, float vs) {
 
 __device__ __forceinline__ float dot_rn(float a0, float a1, float a2, float b0, float b1, float b2) {
     return __fadd_rn(__fadd_rn(__fmul_rn(a0, b0), __fmul_rn(a1, b1)), __fmul_rn(a2, b2));
+}
+
+/* a / det, correctly rounded: a Markstein-corrected product when the context
+ * verified it on this device (xr_column.cu), else IEEE division. */
+__device__ __forceinline__ float div_det(float a, const GeomConst &g) {
+    if (!g.exact_rdet) return __fdiv_rn(a, g.det);
+    const float q = __fmul_rn(a, g.rdet);
+    const float r = __fmaf_rn(-q, g.det, a);
+    return __fmaf_rn(r, g.rdet, q);
 }
 
 /* Per-voxel half of rayCasting (ir.cu:1881-1897): returns u, v and the
@@ -68,8 +79,8 @@ __device__ __forceinline__ void ray_uv(const ViewFrame &f, const GeomConst &g, f
     const float p0 = __fadd_rn(f.src[0], __fmul_rn(coeff, d0));
     const float p1 = __fadd_rn(f.src[1], __fmul_rn(coeff, d1));
     const float p2 = __fadd_rn(f.src[2], __fmul_rn(coeff, d2));
-    u = __fadd_rn(__fdiv_rn(__fmul_rn(dot_rn(p0, p1, p2, f.eu[0], f.eu[1], f.eu[2]), g.mag), g.det), g.half);
-    v = __fadd_rn(__fdiv_rn(__fmul_rn(dot_rn(p0, p1, p2, f.ev[0], f.ev[1], f.ev[2]), g.mag), g.det), g.half);
+    u = __fadd_rn(div_det(__fmul_rn(dot_rn(p0, p1, p2, f.eu[0], f.eu[1], f.eu[2]), g.mag), g), g.half);
+    v = __fadd_rn(div_det(__fmul_rn(dot_rn(p0, p1, p2, f.ev[0], f.ev[1], f.ev[2]), g.mag), g), g.half);
 }
 
 /* Detector window and bilinear taps (ir.cu:1501-1509).  Weights in the
@@ -100,16 +111,19 @@ struct FwdArgs {
     const ViewFrame *frames;  /* [C][V]                      */
     const int *view_list;     /* n_views view indices        */
     int n_views, vpc, cond0;
-    const float *vol;         /* mode 0: N^3; mode 1: K*N^3  */
+    const void *vol;          /* mode 0: N^3; mode 1: K*N^3 (type T) */
     float *out;               /* C blocks of V*Nd*Nd         */
     const BasisConst *basis;  /* device                      */
     int nbx, nby;             /* bricks along x, y           */
 };
 
-template <int MODE>
+template <int MODE, typename T>
 __global__ void __launch_bounds__(kFwdThreads, 2) k_forward(FwdArgs a) {
-    extern __shared__ float smem[];
-    int4 *bbox = reinterpret_cast<int4 *>(smem + 2 * kTileCap);  /* vpc entries */
+    const T *vol = reinterpret_cast<const T *>(a.vol);
+    /* Detector tiles in two-word fixed point (xr_tile.cuh). */
+    extern __shared__ int smem[];
+    __shared__ float s_red[kFwdThreads / 32];
+    int4 *bbox = reinterpret_cast<int4 *>(smem + 4 * kTileCap);  /* vpc entries */
     ViewFrame *fr = reinterpret_cast<ViewFrame *>(bbox + a.vpc);
 
     const GeomConst &g = a.g;
@@ -125,7 +139,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_forward(FwdArgs a) {
     const int x1 = min(x0 + kBX, N) - 1, y1 = min(y0 + kBY, N) - 1, z1 = min(z0 + kBZ, N) - 1;
 
     const int tid = threadIdx.x;
-    for (int i = tid; i < 2 * kTileCap; i += kFwdThreads) smem[i] = 0.0f;
+    for (int i = tid; i < 4 * kTileCap; i += kFwdThreads) smem[i] = 0;
     for (int i = tid; i < nv * 5; i += kFwdThreads) {
         const int jj = i / 5, q = i % 5;
         const float4 *s4 = reinterpret_cast<const float4 *>(&a.frames[(size_t)cond * g.V + a.view_list[j0 + jj]]);
@@ -189,7 +203,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_forward(FwdArgs a) {
         if (!okv[q]) continue;
         const size_t idx = (size_t)x + (size_t)N * (yb + 2 * q) + NN * z;
         if (MODE == 0) {
-            val[q] = a.vol[idx];
+            val[q] = ldgf<T>(vol + idx);
         } else if (MODE == 2) {
             val[q] = 1.0f;
         } else {
@@ -199,7 +213,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_forward(FwdArgs a) {
             for (int k = 0; k < g.K; k++) {
                 const float gk = B->g[cond * g.K + k] * sc;
                 if (gk == 0.f) continue;
-                const float mu = __ldg(&a.vol[idx + (size_t)k * N3]) * gk;
+                const float mu = ldgf<T>(vol + idx + (size_t)k * N3) * gk;
                 const float s0 = B->S[3 * k], s1 = B->S[3 * k + 1], s2 = B->S[3 * k + 2];
                 a0 = fmaf(B->S2[k], mu, a0);
                 mm[0] = fmaf(mu * s0, s0, mm[0]);
@@ -214,14 +228,34 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_forward(FwdArgs a) {
             for (int e = 0; e < 6; e++) m[q][e] = mm[e];
         }
     }
+    float bound = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (!okv[q]) continue;
+        float bq = (MODE == 0) ? fabsf(val[q]) * g.ratio : (MODE == 2 ? 1.0f : fabsf(val[q]));
+        if (MODE == 1)
+#pragma unroll
+            for (int e = 0; e < 6; e++) bq += fabsf(m[q][e]);
+        bound = fmaxf(bound, bq * 1.001f);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bound = fmaxf(bound, __shfl_xor_sync(0xffffffffu, bound, o));
+    if ((tid & 31) == 0) s_red[tid >> 5] = bound;
     __syncthreads();
+    float S = 0.f;
+#pragma unroll
+    for (int i = 0; i < kFwdThreads / 32; i++) S = fmaxf(S, s_red[i]);
+    if (!(S > 0.f) || !(S < 3e38f)) return;
+    const int sh = fix_shift(S);
+    const float fscale = ldexpf(1.0f, sh);
+    const double finv = ldexp(1.0, -sh);
 
     const size_t NdNd = (size_t)Nd * Nd;
     float *outc = a.out + (size_t)cond * g.V * NdNd;
     for (int jj = 0; jj < nv; jj++) {
-        const ViewFrame &f = fr[jj];
+        const ViewFrame f = fr[jj];
         const int4 bb = bbox[jj];
-        float *T = smem + (jj & 1) * kTileCap;
+        int *T = smem + (jj & 1) * 2 * kTileCap;   /* hi words, lo words after */
         float *P = outc + (size_t)f.view * NdNd;
         const bool use_tile = (bb.z > 0) && (bb.z * bb.w <= kTileCap);
         if (bb.z > 0) {
@@ -258,11 +292,11 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_forward(FwdArgs a) {
                 }
                 const int lu = iu - bb.x, lv = iv - bb.y;
                 if (use_tile && lu >= 0 && lu + 1 < bb.z && lv >= 0 && lv + 1 < bb.w) {
-                    float *t0 = T + lu + bb.z * lv;
-                    atomicAdd(t0 + bb.z, w1);
-                    atomicAdd(t0 + bb.z + 1, w2);
-                    atomicAdd(t0 + 1, w3);
-                    atomicAdd(t0, w4);
+                    int *t0 = T + lu + bb.z * lv;
+                    fix_add(t0 + bb.z, kTileCap, w1 * fscale);
+                    fix_add(t0 + bb.z + 1, kTileCap, w2 * fscale);
+                    fix_add(t0 + 1, kTileCap, w3 * fscale);
+                    fix_add(t0, kTileCap, w4 * fscale);
                 } else {
                     float *p0 = P + iu + (size_t)Nd * iv;
                     atomicAdd(p0 + Nd, w1);
@@ -274,13 +308,12 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_forward(FwdArgs a) {
         }
         __syncthreads();
         if (use_tile) {
-            const int n = bb.z * bb.w;
-            for (int i = tid; i < n; i += kFwdThreads) {
-                const float t = T[i];
-                if (t != 0.0f) {
-                    T[i] = 0.0f;
-                    const int r = i / bb.z, c = i - r * bb.z;
-                    atomicAdd(P + (bb.x + c) + (size_t)Nd * (bb.y + r), t);
+            for (int r = tid >> 5; r < bb.w; r += kFwdThreads / 32) {
+                for (int c = tid & 31; c < bb.z; c += 32) {
+                    float t;
+                    if (fix_take(T + c + bb.z * r, kTileCap, finv, t)) {
+                        atomicAdd(P + (bb.x + c) + (size_t)Nd * (bb.y + r), t);
+                    }
                 }
             }
         }
@@ -368,8 +401,9 @@ __device__ __forceinline__ double block_sum(double x) {
     return s;
 }
 
+template <typename T>
 __global__ void k_ratio(GeomConst g, const int *view_list, int n_views, float *proj, const float *norm,
-                        const float *sino, int art, double *loss) {
+                        const T *sino, int art, double *loss) {
     const size_t NdNd = (size_t)g.Nd * g.Nd;
     const int cond = blockIdx.y / n_views, j = blockIdx.y % n_views;
     const size_t base = ((size_t)cond * g.V + view_list[j]) * NdNd;
@@ -377,7 +411,7 @@ __global__ void k_ratio(GeomConst g, const int *view_list, int n_views, float *p
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < NdNd; i += (size_t)gridDim.x * blockDim.x) {
         const size_t idx = base + i;
         float p = __fmul_rn(proj[idx], norm[idx]);
-        const float b = sino[idx];
+        const float b = ldgf<T>(sino + idx);
         acc += (double)fabsf(__fsub_rn(b, p));
         if (art) {
             p = __fsub_rn(b, p);
@@ -410,13 +444,13 @@ struct BackArgs {
     const int *view_list;
     int n_views, cond0, n_cond;
     const float *proj;
-    float *vol;
+    void *vol;                /* type T */
     const BasisConst *basis;
     int art;
     float alpha;
 };
 
-template <bool XTT>
+template <bool XTT, typename T>
 __global__ void __launch_bounds__(kBackThreads) k_back_update(BackArgs a) {
     __shared__ ViewFrame fr[kFrameChunk];
     const GeomConst &g = a.g;
@@ -500,27 +534,31 @@ __global__ void __launch_bounds__(kBackThreads) k_back_update(BackArgs a) {
     const size_t NN = (size_t)N * N, N3 = NN * N;
     const size_t idx = (size_t)x + (size_t)N * y + NN * z;
     if (!XTT) {
-        float *vp = a.vol + idx;
-        if (a.art) *vp = __fadd_rn(*vp, __fmul_rn(a.alpha, tmp));
-        else *vp = (fac == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(*vp, tmp), fac);
+        T *vp = reinterpret_cast<T *>(a.vol) + idx;
+        const float mu = ldf<T>(vp);
+        if (a.art) stf<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmp)));
+        else stf<T>(vp, (fac == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmp), fac));
     } else {
 #pragma unroll
         for (int k = 0; k < 16; k++) {
             if (k >= g.K) break;
-            float *vp = a.vol + idx + (size_t)k * N3;
-            if (a.art) *vp = __fadd_rn(*vp, __fmul_rn(a.alpha, tmpk[k]));
-            else *vp = (fack[k] == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(*vp, tmpk[k]), fack[k]);
+            T *vp = reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3;
+            const float mu = ldf<T>(vp);
+            if (a.art) stf<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmpk[k])));
+            else stf<T>(vp, (fack[k] == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmpk[k]), fack[k]));
         }
     }
 }
 
 /* ------------------------------------------------------------------------ */
-__global__ void k_residual(size_t n, const float *p, const float *b, double *out) {
+template <typename T>
+__global__ void k_residual(size_t n, const float *p, const T *b, double *out) {
     double s2 = 0, b2 = 0, s1 = 0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const double d = (double)p[i] - (double)b[i];
+        const double bi = (double)ldgf<T>(b + i);
+        const double d = (double)p[i] - bi;
         s2 += d * d;
-        b2 += (double)b[i] * (double)b[i];
+        b2 += bi * bi;
         s1 += fabs(d);
     }
     s2 = block_sum(s2);
@@ -534,11 +572,19 @@ __global__ void k_residual(size_t n, const float *p, const float *b, double *out
 }
 
 /* voxelSqrt, ir.cu:1707-1717. */
-__global__ void k_sqrt_abs(size_t n, float *mu) {
+template <typename T>
+__global__ void k_sqrt_abs(size_t n, T *mu) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const float m = mu[i];
-        mu[i] = (m < 0.0f) ? __fsqrt_rn(-m) : __fsqrt_rn(m);
+        const float m = ldf<T>(mu + i);
+        stf<T>(mu + i, (m < 0.0f) ? __fsqrt_rn(-m) : __fsqrt_rn(m));
     }
+}
+
+/* storage conversions (round to nearest even) */
+template <typename S, typename D>
+__global__ void k_convert(size_t n, const S *src, D *dst) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        stf<D>(dst + i, ldgf<S>(src + i));
 }
 
 int grid_for(size_t n, int threads) {
@@ -551,8 +597,8 @@ int grid_for(size_t n, int threads) {
 }  // namespace
 
 cudaError_t launch_forward(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
-                           const int *view_list, int n_views, int cond0, int n_cond, const float *vol, float *out,
-                           int mode, int views_per_cta, cudaStream_t s) {
+                           const int *view_list, int n_views, int cond0, int n_cond, const void *vol, float *out,
+                           int mode, int views_per_cta, int storage, cudaStream_t s) {
     if (n_views <= 0 || n_cond <= 0) return cudaSuccess;
     FwdArgs a;
     a.g = g;
@@ -577,22 +623,18 @@ cudaError_t launch_forward(const GeomConst &g, const BasisConst *d_basis, const 
     vpc = vpc > n_views ? n_views : vpc;
     a.vpc = vpc;
     const dim3 grid((unsigned)bricks, (unsigned)n_cond, (unsigned)((n_views + vpc - 1) / vpc));
-    const size_t smem = 2 * kTileCap * sizeof(float) + vpc * (sizeof(int4) + sizeof(ViewFrame));
+    const size_t smem = 4 * kTileCap * sizeof(int) + vpc * (sizeof(int4) + sizeof(ViewFrame));
     cudaError_t e = cudaSuccess;
-    switch (mode) {
-        case 0:
-            e = cudaFuncSetAttribute(k_forward<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess) k_forward<0><<<grid, kFwdThreads, smem, s>>>(a);
-            break;
-        case 1:
-            e = cudaFuncSetAttribute(k_forward<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess) k_forward<1><<<grid, kFwdThreads, smem, s>>>(a);
-            break;
-        default:
-            e = cudaFuncSetAttribute(k_forward<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess) k_forward<2><<<grid, kFwdThreads, smem, s>>>(a);
-            break;
-    }
+#define XR_FWD(M, TT)                                                                                             \
+    do {                                                                                                          \
+        e = cudaFuncSetAttribute(k_forward<M, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
+        if (e == cudaSuccess) k_forward<M, TT><<<grid, kFwdThreads, smem, s>>>(a);                                \
+    } while (0)
+    if (mode == 2) XR_FWD(2, float);
+    else if (storage == kBF16) { if (mode == 0) XR_FWD(0, __nv_bfloat16); else XR_FWD(1, __nv_bfloat16); }
+    else if (storage == kF16) { if (mode == 0) XR_FWD(0, __half); else XR_FWD(1, __half); }
+    else { if (mode == 0) XR_FWD(0, float); else XR_FWD(1, float); }
+#undef XR_FWD
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -605,13 +647,18 @@ cudaError_t launch_chord(const GeomConst &g, const ViewFrame *frames, float *nor
 }
 
 cudaError_t launch_ratio(const GeomConst &g, const int *view_list, int n_views, int n_cond, float *proj,
-                         const float *norm, const float *sino, int art, double *loss, cudaStream_t s) {
+                         const float *norm, const void *sino, int art, double *loss, int storage, cudaStream_t s) {
     if (n_views <= 0) return cudaSuccess;
     const size_t NdNd = (size_t)g.Nd * g.Nd;
     int bx = (int)((NdNd + 255) / 256);
     if (bx > 64) bx = 64;
     const dim3 grid(bx, (unsigned)(n_views * n_cond));
-    k_ratio<<<grid, 256, 0, s>>>(g, view_list, n_views, proj, norm, sino, art, loss);
+    if (storage == kBF16)
+        k_ratio<<<grid, 256, 0, s>>>(g, view_list, n_views, proj, norm, (const __nv_bfloat16 *)sino, art, loss);
+    else if (storage == kF16)
+        k_ratio<<<grid, 256, 0, s>>>(g, view_list, n_views, proj, norm, (const __half *)sino, art, loss);
+    else
+        k_ratio<<<grid, 256, 0, s>>>(g, view_list, n_views, proj, norm, (const float *)sino, art, loss);
     return cudaGetLastError();
 }
 
@@ -623,7 +670,7 @@ cudaError_t launch_normalize(const GeomConst &g, int n_cond, float *proj, const 
 
 cudaError_t launch_back_update(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, int cond0, int n_cond, const float *proj,
-                               float *vol, int xtt, int art, float alpha, cudaStream_t s) {
+                               void *vol, int xtt, int art, float alpha, int storage, cudaStream_t s) {
     BackArgs a;
     a.g = g;
     a.frames = frames;
@@ -637,20 +684,45 @@ cudaError_t launch_back_update(const GeomConst &g, const BasisConst *d_basis, co
     a.art = art;
     a.alpha = alpha;
     const long nb = (long)((g.N + 7) / 8) * ((g.N + 3) / 4) * ((g.N + 7) / 8);
-    if (xtt)
-        k_back_update<true><<<(unsigned)nb, kBackThreads, 0, s>>>(a);
+#define XR_BACK(X, TT) k_back_update<X, TT><<<(unsigned)nb, kBackThreads, 0, s>>>(a)
+    if (storage == kBF16) { if (xtt) XR_BACK(true, __nv_bfloat16); else XR_BACK(false, __nv_bfloat16); }
+    else if (storage == kF16) { if (xtt) XR_BACK(true, __half); else XR_BACK(false, __half); }
+    else { if (xtt) XR_BACK(true, float); else XR_BACK(false, float); }
+#undef XR_BACK
+    return cudaGetLastError();
+}
+
+cudaError_t launch_residual(long n, const float *p, const void *b, double *out, int storage, cudaStream_t s) {
+    const int gr = grid_for((size_t)n, 256);
+    if (storage == kBF16) k_residual<<<gr, 256, 0, s>>>((size_t)n, p, (const __nv_bfloat16 *)b, out);
+    else if (storage == kF16) k_residual<<<gr, 256, 0, s>>>((size_t)n, p, (const __half *)b, out);
+    else k_residual<<<gr, 256, 0, s>>>((size_t)n, p, (const float *)b, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sqrt_abs(long n, void *mu, int storage, cudaStream_t s) {
+    const int gr = grid_for((size_t)n, 256);
+    if (storage == kBF16) k_sqrt_abs<<<gr, 256, 0, s>>>((size_t)n, (__nv_bfloat16 *)mu);
+    else if (storage == kF16) k_sqrt_abs<<<gr, 256, 0, s>>>((size_t)n, (__half *)mu);
+    else k_sqrt_abs<<<gr, 256, 0, s>>>((size_t)n, (float *)mu);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert(long n, const void *src, int src_storage, void *dst, int dst_storage, cudaStream_t s) {
+    const int gr = grid_for((size_t)n, 256);
+    const size_t m = (size_t)n;
+    if (src_storage == kF32 && dst_storage == kBF16)
+        k_convert<<<gr, 256, 0, s>>>(m, (const float *)src, (__nv_bfloat16 *)dst);
+    else if (src_storage == kF32 && dst_storage == kF16)
+        k_convert<<<gr, 256, 0, s>>>(m, (const float *)src, (__half *)dst);
+    else if (src_storage == kBF16 && dst_storage == kF32)
+        k_convert<<<gr, 256, 0, s>>>(m, (const __nv_bfloat16 *)src, (float *)dst);
+    else if (src_storage == kF16 && dst_storage == kF32)
+        k_convert<<<gr, 256, 0, s>>>(m, (const __half *)src, (float *)dst);
+    else if (src_storage == dst_storage)
+        return cudaMemcpyAsync(dst, src, m * storage_bytes(src_storage), cudaMemcpyDeviceToDevice, s);
     else
-        k_back_update<false><<<(unsigned)nb, kBackThreads, 0, s>>>(a);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_residual(long n, const float *p, const float *b, double *out, cudaStream_t s) {
-    k_residual<<<grid_for((size_t)n, 256), 256, 0, s>>>((size_t)n, p, b, out);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_sqrt_abs(long n, float *mu, cudaStream_t s) {
-    k_sqrt_abs<<<grid_for((size_t)n, 256), 256, 0, s>>>((size_t)n, mu);
+        return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "xr_internal.h"
+#include "xr_storage.cuh"
 
 namespace xr {
 namespace {
@@ -57,11 +58,12 @@ __device__ void jacobi3(double A[9], double w[3], double V[9]) {
     w[2] = A[8];
 }
 
-__global__ void k_orientation(long nvox, int K, const BasisConst *B, const float *mu, float *md, float *ev) {
+template <typename TS>
+__global__ void k_orientation(long nvox, int K, const BasisConst *B, const TS *mu, float *md, float *ev) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nvox; i += (long)gridDim.x * blockDim.x) {
         double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, mean = 0.0;
         for (int k = 0; k < K; k++) {
-            const double m = (double)__ldg(&mu[(long)k * nvox + i]);
+            const double m = (double)ldgf<TS>(mu + (long)k * nvox + i);
             const double s0 = m * B->S[3 * k], s1 = m * B->S[3 * k + 1], s2 = m * B->S[3 * k + 2];
             mean += m;
             T[0] += s0 * s0; T[1] += s0 * s1; T[2] += s0 * s2;
@@ -133,9 +135,12 @@ int grid_for(long n, int threads) {
 
 }  // namespace
 
-cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, const float *mu, float *md, float *ev,
-                               cudaStream_t s) {
-    k_orientation<<<grid_for(nvox, 128), 128, 0, s>>>(nvox, K, d_basis, mu, md, ev);
+cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, const void *mu, float *md, float *ev,
+                               int storage, cudaStream_t s) {
+    const int gr = grid_for(nvox, 128);
+    if (storage == kBF16) k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const __nv_bfloat16 *)mu, md, ev);
+    else if (storage == kF16) k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const __half *)mu, md, ev);
+    else k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const float *)mu, md, ev);
     return cudaGetLastError();
 }
 

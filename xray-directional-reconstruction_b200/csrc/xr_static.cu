@@ -115,6 +115,6 @@ extern "C" xr_status xr_dev_forward_proj_only_static(xr_ctx *c, const float *d_v
     st = cuda_check(c, cudaMemsetAsync(d_sino, 0, npx * sizeof(float), s), "clear output");
     if (st) return st;
     return cuda_check(c, launch_forward(c->gc, nullptr, dev->frames, dev->views, c->V, 0, c->C, d_vol, d_sino, 0,
-                                        c->views_per_cta, s),
+                                        c->views_per_cta, 0, s),
                       "static forward splat");
 }

@@ -1,0 +1,50 @@
+/*
+ * Two-word fixed-point detector tiles for the forward splats.
+ *
+ * A 32-bit integer atomicAdd on shared memory is a native instruction, a
+ * float (or 64-bit) one runs as a compare-and-swap loop.  Each contribution
+ * x, scaled by the CTA's power of two (xs = x * 2^sh, |xs| < 2^20), is split
+ * into an integer part h = rint(xs) and a remainder r = xs - h (exact, Sterbenz)
+ * kept to 2^-21 in a second word: two native atomics per tap, a per-CTA sum
+ * exact to 2^-41 of the CTA's largest contribution, i.e. below the FP32 rounding
+ * of every pixel the reference itself accumulates.  With at most 1024
+ * contributions per pixel (one tap per voxel of a brick) both words stay below
+ * 2^30.  A pixel's relative precision matters: the normalised projection
+ * divides by the weight image, so footprint-edge pixels with small sums are
+ * amplified to the scale of the largest ones.
+ */
+#ifndef XR_TILE_CUH
+#define XR_TILE_CUH
+
+namespace xr {
+
+constexpr float kFixLoScale = 2097152.0f;           /* 2^21 */
+constexpr double kFixLoInv = 1.0 / 2097152.0;
+
+/* tile word layout per buffer: [hi: cap ints][lo: cap ints] */
+__device__ __forceinline__ void fix_add(int *hi, int cap, float xs) {
+    const float h = rintf(xs);
+    atomicAdd(hi, (int)h);
+    atomicAdd(hi + cap, __float2int_rn(__fsub_rn(xs, h) * kFixLoScale));
+}
+
+/* Reads and clears one pixel's two words; returns the sum unscaled by 2^-sh. */
+__device__ __forceinline__ bool fix_take(int *hi, int cap, double finv, float &out) {
+    const int h = *hi, l = hi[cap];
+    if ((h | l) == 0) return false;
+    *hi = 0;
+    hi[cap] = 0;
+    out = (float)(((double)h + (double)l * kFixLoInv) * finv);
+    return true;
+}
+
+/* Power-of-two scale for a CTA whose contributions are bounded by S > 0. */
+__device__ __forceinline__ int fix_shift(float S) {
+    int ex;
+    frexpf(S, &ex);          /* S < 2^ex */
+    return max(-126, min(126, 20 - ex));
+}
+
+}  // namespace xr
+
+#endif
