@@ -238,50 +238,79 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def load_replicas():
+    spec = importlib.util.spec_from_file_location("xr_replicas", os.path.join(PKG, "replicas.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_warmstart():
+    if "xrd.warmstart" in sys.modules:
+        return sys.modules["xrd.warmstart"]
+    load_pkg()
+    spec = importlib.util.spec_from_file_location("xrd.warmstart", os.path.join(PKG, "warmstart.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["xrd.warmstart"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def run_ttr(args, local):
-    """Time to a relative data residual: OS-EM epochs (device-timed with CUDA
-    events) from the reference's MLEM start mu = 0.01 (main.cu:38-43), with
-    ||A mu - b|| / ||b|| checked every few epochs outside the timed work."""
+    """Time to a relative data residual ||A mu - b|| / ||b|| <= --target (FP64
+    norms) on the XTT 256^3 x 13 workload, arms on the same data b = A mu_true
+    (device fiber phantom, seed held out from the training seeds):
+      plain_f32:    FP32 OS-EM (5 subsets) from mu = 0.01 (main.cu:38-43);
+      learned_bf16: BF16 volumes (FP32 data): 5 OS-EM epochs from mu = 0.01,
+                    the warm-start network in place, then OS-EM to the target;
+      plain_bf16:   BF16 volumes without the network (isolates the storage).
+    Device time (CUDA events): session set-up, epochs and inference.  The
+    residual is checked every --check-every epochs, outside the timed work."""
     import torch
+    ws = load_warmstart()
     xr = load_pkg()
     torch.cuda.set_device(local)
-    ctx = xr.Context.create(W["sdd"], W["sod"], W["det"], W["N"], W["Nd"], W["V"], three_axes(), None, None,
-                            basis13(), device=local)
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    ctx.set_stream(stream.cuda_stream)
-    N, Nd, V, C, K = W["N"], W["Nd"], W["V"], W["C"], W["K"]
-    mu_true = fiber_phantom(N, W["n_fibers"], W["seed"], basis13())
-    d_true = torch.from_numpy(mu_true).cuda()
-    d_b = torch.empty((C, V, Nd, Nd), dtype=torch.float32, device="cuda")
-    ctx.dev_forward(d_true.data_ptr(), d_b.data_ptr(), True)
-    d_vol = torch.full((K, N, N, N), 0.01, dtype=torch.float32, device="cuda")
+    scan = ws.Scan(W["N"], W["V"], device=local, n_fibers=W["n_fibers"])
+    mu_true = scan.phantom(W["seed"])
+    b = scan.project(mu_true)
     torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    ctx.dev_session_begin(d_b.data_ptr(), d_vol.data_ptr(), True, args.max_epochs, W["batch"])
-    e1.record(stream)
-    torch.cuda.synchronize()
-    total_ms = e0.elapsed_time(e1)
-    hist = []
-    reached = None
-    for ep in range(1, args.max_epochs + 1):
-        e0.record(stream)
-        ctx.dev_session_epoch()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        total_ms += e0.elapsed_time(e1)
-        if ep % args.check_every == 0 or ep == args.max_epochs:
-            r, _ = ctx.dev_residual(d_vol.data_ptr(), d_b.data_ptr(), True)
-            hist.append((ep, r, total_ms))
-            if r <= args.target:
-                reached = (ep, r, total_ms)
-                break
-    line = {"mode": "time_to_residual", "workload": WORKLOAD, "target": args.target, "storage": "f32",
-            "start": "mu = 0.01", "reached": reached is not None,
-            "epochs": reached[0] if reached else None, "seconds": (reached[2] / 1e3) if reached else None,
-            "history": [{"epoch": e, "rel_l2": r, "ms": t} for e, r, t in hist]}
+    K, N = scan.K, scan.N
+    arms = {}
+
+    def run_arm(name, storage, learned):
+        dt = {0: torch.float32, 1: torch.bfloat16}[storage]
+        vol = torch.full((K, N, N, N), 0.01, dtype=dt, device="cuda")
+        ms0, e0, r0 = 0.0, 0, None
+        if learned:
+            if not os.path.exists(ws.WEIGHTS):
+                arms[name] = {"unavailable": "no trained weights at " + os.path.relpath(ws.WEIGHTS, ROOT)}
+                return
+            net = xr.Net(K, 32, 4)
+            net.load(ws.WEIGHTS)
+            net.set_stream(scan.stream.cuda_stream)
+            ms0 = ws.warm_start(scan, net, b, vol, args.early, W["batch"], storage, 0)
+            e0 = args.early
+            r0 = scan.residual(vol, b, storage, 0)
+            net.close()
+        e, ms, trace = scan.osem(b, vol, 0, W["batch"], storage, 0, residual_every=args.check_every,
+                                 target=args.target, max_epochs=args.max_epochs, final_sqrt=False)
+        reached = bool(trace) and trace[-1][2] <= args.target
+        err = float(torch.linalg.vector_norm(vol.float() - mu_true) / torch.linalg.vector_norm(mu_true))
+        arms[name] = {"storage": {0: "f32", 1: "bf16"}[storage], "sinogram": "f32", "learned": learned,
+                      "reached": reached, "epochs": e0 + e, "seconds": (ms0 + ms) / 1e3 if reached else None,
+                      "seconds_run": (ms0 + ms) / 1e3, "residual_final": trace[-1][2] if trace else r0,
+                      "residual_after_warm_start": r0, "volume_rel_error_final": err,
+                      "history": [{"epoch": e0 + ep, "ms": ms0 + t, "rel_l2": r} for ep, t, r in trace]}
+        del vol
+
+    for name in args.arms.split(","):
+        run_arm(name, 0 if name.endswith("f32") else 1, name.startswith("learned"))
+    line = {"mode": "time_to_residual", "metric": "XTT 256^3x13 time-to-%g residual (learned+BF16 vs plain FP32)"
+            % args.target, "unit": "s", "higher_is_better": False, "workload": WORKLOAD, "target": args.target,
+            "check_every": args.check_every, "max_epochs": args.max_epochs, "arms": arms}
+    p, l = arms.get("plain_f32", {}), arms.get("learned_bf16", {})
+    line["speedup_learned_bf16_vs_plain_f32"] = (p["seconds"] / l["seconds"]) if p.get("seconds") and \
+        l.get("seconds") else None
     print(json.dumps(line), flush=True)
 
 
@@ -297,8 +326,10 @@ def main():
     ap.add_argument("--ttr", action="store_true",
                     help="time-to-residual: OS-EM from mu = 0.01 until ||A mu - b|| / ||b|| <= --target")
     ap.add_argument("--target", type=float, default=1e-3)
-    ap.add_argument("--max-epochs", type=int, default=300)
-    ap.add_argument("--check-every", type=int, default=2)
+    ap.add_argument("--max-epochs", type=int, default=1000)
+    ap.add_argument("--check-every", type=int, default=10)
+    ap.add_argument("--early", type=int, default=5, help="--ttr: OS-EM epochs before the warm-start network")
+    ap.add_argument("--arms", default="plain_f32,learned_bf16,plain_bf16", help="--ttr arms")
     args = ap.parse_args()
     if args.size == "profile":
         W.update(W_PROFILE)
@@ -307,26 +338,22 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rp = load_replicas()
+    rank, world, local = rp.rank_env()
 
     if args.impl == "reference":
         run_reference(args, rank)
         return
 
     import torch
-    import torch.distributed as dist
-    from datetime import timedelta
 
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-
     if args.ttr:
-        run_ttr(args, local)
+        if rank == 0:          # one GPU: the time-to-residual comparison runs on rank 0 only
+            run_ttr(args, local)
         return
+    if world > 1:
+        rp.init("nccl")
 
     xr = load_pkg()
     s_basis = basis13()
@@ -339,7 +366,7 @@ def main():
     ctx.set_stream(stream.cuda_stream)
 
     N, Nd, V, C, K = W["N"], W["Nd"], W["V"], W["C"], W["K"]
-    mu_true = fiber_phantom(N, W["n_fibers"], W["seed"] + rank, s_basis)
+    mu_true = fiber_phantom(N, W["n_fibers"], rp.specimen_seed(W["seed"], rank), s_basis)   # one specimen per replica
     d_true = torch.from_numpy(mu_true).cuda()
     d_b = torch.empty((C, V, Nd, Nd), dtype=torch.float32, device="cuda")
     ctx.dev_forward(d_true.data_ptr(), d_b.data_ptr(), True)           # b = A mu_true
@@ -355,7 +382,7 @@ def main():
 
     sampler = ClockSampler(local)
     if world > 1:
-        dist.barrier()
+        rp.barrier()
     torch.cuda.synchronize()
     sampler.start()
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -467,13 +494,12 @@ def main():
         e2e_ms = float(np.mean(times))
 
     if world > 1:
-        t = torch.tensor([t_ms, e2e_ms or 0.0], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms, e2e_ms = float(t[0].item()), (float(t[1].item()) if e2e_ms else None)
-        value = world * per_gpu_bytes / (t_ms / 1e3) / 1e9
-        if dist.get_rank() != 0:
-            dist.barrier()
-            dist.destroy_process_group()
+        t_max, e_max = rp.max_over_ranks([t_ms, e2e_ms or 0.0], device="cuda")
+        t_ms, e2e_ms = t_max, (e_max if e2e_ms else None)
+        value = rp.whole_job_rate(per_gpu_bytes, world, t_ms) / 1e9
+        if rank != 0:
+            ctx.close()
+            rp.finish()
             return
     if e2e_ms:
         h2d = C * V * Nd * Nd * 4 + K * N ** 3 * 4
@@ -503,8 +529,7 @@ def main():
     print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+        rp.finish()
 
 
 if __name__ == "__main__":

@@ -98,9 +98,20 @@ enum {
                                   residual norms).  Device-buffer calls then take
                                   volumes / sinograms of that type; host-buffer
                                   calls keep float arrays and convert on the GPU */
-    XR_OPT_GRAPHS = 5          /* 1: each session epoch runs as a CUDA graph, one
+    XR_OPT_GRAPHS = 5,         /* 1: each session epoch runs as a CUDA graph, one
                                   captured per distinct subset order and replayed
                                   (ignored while XR_OPT_TIMING is on)            */
+    XR_OPT_SINO_STORAGE = 6,   /* storage of measured sinograms alone: -1 (default)
+                                  the XR_OPT_STORAGE type, else 0 / 1 / 2 as there
+                                  (e.g. BF16 volumes with FP16 or FP32 data)      */
+    XR_OPT_ROUNDING = 7,       /* 16-bit volume updates: 1 (default) stochastic
+                                  rounding, 0 round to nearest even.  Nearest
+                                  rounding drops every update below half a unit
+                                  in the last place, so late OS-EM epochs stall */
+    XR_OPT_XTT_SQRT = 8        /* 1 (default): an XTT session ends with the
+                                  reference's voxelSqrt (reconstruct.cu:919-922);
+                                  0: it leaves the iterate itself, so a later
+                                  session can continue it                         */
 };
 
 /* ---- context ----------------------------------------------------------- */
@@ -185,9 +196,10 @@ xr_status xr_residual(xr_ctx *ctx, const float *const *voxel, const float *const
                       int xtt, double *rel_l2, double *l1);
 
 /* ---- device-buffer entry points (no host copies) ------------------------ */
-/* Volumes (d_vol, d_mu) and measured sinograms (d_sino of the residual and
- * of sessions) hold elements of the storage type (XR_OPT_STORAGE); forward
- * projections, orientations and eigenvalues are FP32. */
+/* Volumes (d_vol, d_mu) hold elements of the storage type (XR_OPT_STORAGE),
+ * measured sinograms (d_sino of the residual and of sessions) of the
+ * sinogram storage type (XR_OPT_SINO_STORAGE); forward projections,
+ * orientations and eigenvalues are FP32. */
 
 xr_status xr_dev_forward(xr_ctx *ctx, const void *d_vol, float *d_sino, xr_rotate dir, int xtt);
 xr_status xr_dev_residual(xr_ctx *ctx, const void *d_vol, const void *d_sino, xr_rotate dir, int xtt,
@@ -211,6 +223,33 @@ xr_status xr_dev_session_epoch(xr_ctx *ctx, double *loss);
 xr_status xr_dev_session_end(xr_ctx *ctx, float *d_md, float *d_evalue);
 /* The session's current ratio images (C*V*Nd^2 floats, device pointer). */
 xr_status xr_dev_session_proj(xr_ctx *ctx, const float **d_proj);
+
+/* ---- several specimens at once (no reference counterpart) -------------- */
+/* A batch runs the OS-EM sessions of several independent specimens (each its
+ * own context: geometry, size, storage options) together: one epoch of every
+ * specimen is enqueued on the specimens' streams, forked from and joined to
+ * the batch's stream, so their kernels overlap on the GPU; with
+ * XR_OPT_GRAPHS set on the first context the whole multi-specimen epoch is
+ * captured once per distinct combination of subset orders and replayed as
+ * one CUDA graph.  The reference reconstructs one specimen per run
+ * (reconstruct.cu:799-954); each specimen's result equals its own session's. */
+typedef struct xr_batch xr_batch;
+
+/* Contexts on one device; the batch holds (does not own) them. */
+xr_status xr_batch_create(xr_ctx *const *ctxs, int n, xr_batch **out);
+void xr_batch_destroy(xr_batch *batch);
+const char *xr_batch_last_error(const xr_batch *batch);
+/* xr_dev_session_begin on every specimen (same epochs / subsets / method). */
+xr_status xr_batch_session_begin(xr_batch *batch, const void *const *d_sinos, void *const *d_vols, int xtt, int epochs,
+                                 int subsets, xr_rotate dir, xr_method method, float lambda);
+/* One epoch of every specimen; losses[i] (may be NULL) = specimen i's epoch loss
+ * (XTT: its single loss; IR: its axis 0 loss). */
+xr_status xr_batch_epoch(xr_batch *batch, double *losses);
+xr_status xr_batch_session_end(xr_batch *batch);
+/* Autotuner: for each specimen, times its XTT forward splat over one subset
+ * for each candidate views-per-CTA chunk and keeps the fastest
+ * (XR_OPT_VIEWS_PER_CTA of that context); chosen[i] receives it (may be NULL). */
+xr_status xr_batch_autotune(xr_batch *batch, int *chosen);
 
 /* The raw forward splat of xr_forward_proj_only on device buffers, for
  * callers that cannot allocate device memory: code whose device memory is

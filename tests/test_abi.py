@@ -1,5 +1,5 @@
 """C-ABI boundary checks that need no GPU: libxr.so loads, exports every
-function include/xr.h declares, parses settings files of the reference's
+function include/xr.h and include/xr_learn.h declare, parses settings files of the reference's
 schema like init_params (params.cu:42-104), validates scans, and reports
 XR_ERR_NODEV (instead of crashing) when no device is present."""
 from __future__ import annotations
@@ -14,12 +14,12 @@ import pytest
 
 from conftest import ROOT, gpu_available, load_xr
 
-HEADER = os.path.join(ROOT, "include", "xr.h")
+HEADERS = [os.path.join(ROOT, "include", "xr.h"), os.path.join(ROOT, "include", "xr_learn.h")]
 REF_SETTINGS = "/root/reference/utility/settings.json"
 
 
 def declared_functions():
-    text = open(HEADER).read()
+    text = "".join(open(h).read() for h in HEADERS)
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(xr_[a-z_0-9]+)\s*\(", text)))
 

@@ -398,3 +398,49 @@ def test_graph_epochs_match_direct(oracle, xtt):
         ctx.dev_session_end(0, 0)
         outs.append(dv.cpu().numpy())
     assert rel_err(outs[1], outs[0]) <= TOL
+
+
+def test_bf16_stochastic_rounding_is_unbiased(oracle):
+    """BF16 volumes with FP32 data and XTT ART steps far below half a BF16
+    unit (relative 2^-9): nearest rounding drops the updates (the iteration
+    stalls: almost no voxel changes), stochastic rounding (the default,
+    XR_OPT_ROUNDING = 1) applies them in expectation: regressed on the FP32
+    updates, its updates have slope 1, directly launched or replayed from a
+    CUDA graph.  (The draw hashes the FP32 value, whose last bits vary with
+    the order of the forward's float atomics, so runs agree statistically,
+    not bit for bit.)"""
+    torch = pytest.importorskip("torch")
+    xr = load_xr()
+    s, ctx = make(24, 36, 12, C=3, K=13, seed=80, shifts=False)
+    truth = fiber_phantom(s.N, 5, 81, s.basis)
+    db = torch.from_numpy(oracle.forward_all(s, truth, 0, True)).cuda()
+    mu0 = np.random.default_rng(82).uniform(0.25, 0.75, (s.K, s.N, s.N, s.N)).astype(np.float32)
+    mu0 = torch.from_numpy(mu0).to(torch.bfloat16).float().numpy()          # exactly representable
+
+    def run(storage, rounding, graphs, lam):
+        ctx.set_option(xr.Option.STORAGE, storage)
+        ctx.set_option(xr.Option.SINO_STORAGE, 0)
+        ctx.set_option(xr.Option.ROUNDING, rounding)
+        ctx.set_option(xr.Option.GRAPHS, graphs)
+        ctx.set_option(xr.Option.XTT_SQRT, 0)  # keep the iterate (no final voxelSqrt)
+        dv = torch.from_numpy(mu0).cuda().to(torch.float32 if storage == 0 else torch.bfloat16)
+        torch.cuda.synchronize()
+        ctx.dev_session_begin(db.data_ptr(), dv.data_ptr(), True, 1, 2, method=xr.Method.ART, lam=lam)
+        ctx.dev_session_epoch()
+        ctx.dev_session_end(0, 0)
+        return dv.float().cpu().numpy().astype(np.float64) - mu0
+
+    probe = run(0, 1, 0, 1e-2)
+    lam = 1e-2 * 2e-4 / np.median(np.abs(probe) / mu0)                   # median step 2e-4 of the value
+    d32 = run(0, 1, 0, lam)
+    d_near = run(1, 0, 0, lam)
+    d_sr = run(1, 1, 0, lam)
+    d_sr_g = run(1, 1, 1, lam)
+    ctx.set_option(xr.Option.GRAPHS, 0)
+    slope = lambda d: float((d * d32).sum() / (d32 * d32).sum())
+    changed = lambda d: float((np.abs(d) > 1e-6 * mu0).mean())
+    print(f"lambda {lam:.3e}: slope nearest {slope(d_near):.3f} (changed {changed(d_near):.3f}), "
+          f"stochastic {slope(d_sr):.3f} (changed {changed(d_sr):.3f})")
+    assert abs(slope(d_sr) - 1.0) <= 0.15
+    assert abs(slope(d_sr_g) - 1.0) <= 0.15
+    assert abs(slope(d_near)) <= 0.3

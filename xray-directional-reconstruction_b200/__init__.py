@@ -80,6 +80,9 @@ class Option(enum.IntEnum):
     VIEWS_PER_CTA = 3
     STORAGE = 4
     GRAPHS = 5
+    SINO_STORAGE = 6
+    ROUNDING = 7
+    XTT_SQRT = 8
 
 
 class Storage(enum.IntEnum):
@@ -140,6 +143,40 @@ _SIGS = {
     "xr_dev_session_proj": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "xr_dev_forward_proj_only_static": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                          ctypes.c_void_p], ctypes.c_int),
+    "xr_batch_create": ([ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+                        ctypes.c_int),
+    "xr_batch_destroy": ([ctypes.c_void_p], None),
+    "xr_batch_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
+    "xr_batch_session_begin": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                ctypes.c_float], ctypes.c_int),
+    "xr_batch_epoch": ([ctypes.c_void_p, _D], ctypes.c_int),
+    "xr_batch_session_end": ([ctypes.c_void_p], ctypes.c_int),
+    "xr_batch_autotune": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    # include/xr_learn.h
+    "xr_net_create": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
+                       ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "xr_net_destroy": ([ctypes.c_void_p], None),
+    "xr_net_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
+    "xr_net_set_stream": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "xr_net_num_params": ([ctypes.c_void_p], ctypes.c_size_t),
+    "xr_net_get_params": ([ctypes.c_void_p, _F, ctypes.c_size_t], ctypes.c_int),
+    "xr_net_set_params": ([ctypes.c_void_p, _F, ctypes.c_size_t], ctypes.c_int),
+    "xr_net_save": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
+    "xr_net_load": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
+    "xr_net_infer": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                      ctypes.c_int, ctypes.c_float, ctypes.c_float], ctypes.c_int),
+    "xr_net_loss_grad": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_int, ctypes.c_float, _D, _F], ctypes.c_int),
+    "xr_net_adam_step": ([ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float],
+                         ctypes.c_int),
+    "xr_conv3d_fprop": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                         ctypes.c_int], ctypes.c_int),
+    "xr_dev_fiber_phantom": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, _F, ctypes.c_void_p],
+                             ctypes.c_int),
+    "xr_conv3d_wgrad": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                         ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
 }
 
 _lib = None
@@ -549,3 +586,155 @@ def directionNormalization(md: Sequence[Volume]) -> None:
 
 def version() -> str:
     return lib().xr_version().decode()
+
+
+class Batch:
+    """Several specimens' OS-EM sessions run together (xr_batch_*): one epoch
+    of every specimen per call, their kernels overlapping on the GPU, the
+    whole multi-specimen epoch replayed as one CUDA graph when the first
+    context has Option.GRAPHS set.  Holds references to the contexts."""
+
+    def __init__(self, contexts: Sequence["Context"]):
+        self.contexts = list(contexts)
+        arr = (ctypes.c_void_p * len(self.contexts))(*[c._h for c in self.contexts])
+        h = ctypes.c_void_p()
+        st = lib().xr_batch_create(arr, len(self.contexts), ctypes.byref(h))
+        if st:
+            raise XRError(st, "xr_batch_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().xr_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st:
+            msg = lib().xr_batch_last_error(self._h)
+            raise XRError(st, msg.decode() if msg else "")
+
+    def session_begin(self, d_sinos, d_vols, xtt: bool, epochs: int, subsets: int, rotate: int = 0,
+                      method: int = 1, lam: float = 1e-2):
+        n = len(self.contexts)
+        s = (ctypes.c_void_p * n)(*[int(p) for p in d_sinos])
+        v = (ctypes.c_void_p * n)(*[int(p) for p in d_vols])
+        self._check(lib().xr_batch_session_begin(self._h, s, v, int(xtt), int(epochs), int(subsets), int(rotate),
+                                                 int(method), float(lam)))
+
+    def epoch(self) -> np.ndarray:
+        loss = np.zeros(len(self.contexts), np.float64)
+        self._check(lib().xr_batch_epoch(self._h, loss.ctypes.data_as(_D)))
+        return loss
+
+    def session_end(self):
+        self._check(lib().xr_batch_session_end(self._h))
+
+    def autotune(self) -> list:
+        out = (ctypes.c_int * len(self.contexts))()
+        self._check(lib().xr_batch_autotune(self._h, out))
+        return list(out)
+
+
+# ---------------------------------------------------------------------------
+# Learned warm start (include/xr_learn.h; no counterpart in the reference)
+# ---------------------------------------------------------------------------
+
+class Net:
+    """The warm-start network: depth 3x3x3 convolutions of `width` channels
+    on K-channel volumes, y = x + net(s*x)/s, trained and run on the tensor
+    cores by libxr.  Device buffers are passed as raw pointers (e.g.
+    torch.Tensor.data_ptr())."""
+
+    def __init__(self, channels: int = 13, width: int = 32, depth: int = 4, seed: int = 0, device: int = 0):
+        h = ctypes.c_void_p()
+        st = lib().xr_net_create(int(device), int(channels), int(width), int(depth), int(seed), ctypes.byref(h))
+        if st:
+            raise XRError(st, "xr_net_create")
+        self._h = h
+        self.channels, self.width, self.depth = channels, width, depth
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().xr_net_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st:
+            msg = lib().xr_net_last_error(self._h)
+            raise XRError(st, msg.decode() if msg else "")
+
+    def set_stream(self, stream_handle: int):
+        self._check(lib().xr_net_set_stream(self._h, ctypes.c_void_p(stream_handle)))
+
+    @property
+    def num_params(self) -> int:
+        return int(lib().xr_net_num_params(self._h))
+
+    def get_params(self) -> np.ndarray:
+        p = np.empty(self.num_params, np.float32)
+        self._check(lib().xr_net_get_params(self._h, p.ctypes.data_as(_F), p.size))
+        return p
+
+    def set_params(self, p) -> None:
+        p = _f32(p).ravel()
+        self._check(lib().xr_net_set_params(self._h, p.ctypes.data_as(_F), p.size))
+
+    def save(self, path: str) -> None:
+        self._check(lib().xr_net_save(self._h, path.encode()))
+
+    def load(self, path: str) -> None:
+        self._check(lib().xr_net_load(self._h, path.encode()))
+
+    def infer(self, d_in: int, d_out: int, shape, storage: int = 0, in_scale: float = 1.0,
+              floor_value: float = 0.0) -> None:
+        """d_out = max(net(d_in), floor_value); shape = (nz, ny, nx) of each
+        of the K planes; storage 0 FP32, 1 BF16, 2 FP16."""
+        nz, ny, nx = shape
+        self._check(lib().xr_net_infer(self._h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out), int(storage), nx, ny,
+                                       nz, float(in_scale), float(floor_value)))
+
+    def loss_grad(self, d_in: int, d_target: int, shape, in_scale: float = 1.0, want_grad: bool = False):
+        """(loss, gradient or None) of the FP32 device volumes; the gradient
+        stays on the device for adam_step."""
+        nz, ny, nx = shape
+        loss = ctypes.c_double()
+        g = np.empty(self.num_params, np.float32) if want_grad else None
+        self._check(lib().xr_net_loss_grad(self._h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_target), nx, ny, nz,
+                                           float(in_scale), ctypes.byref(loss),
+                                           g.ctypes.data_as(_F) if g is not None else None))
+        return loss.value, g
+
+    def adam_step(self, lr: float, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8) -> None:
+        self._check(lib().xr_net_adam_step(self._h, float(lr), float(beta1), float(beta2), float(eps)))
+
+
+def conv3d_fprop(x: int, cin: int, w: int, bias: int, mask: int, y: int, cout: int, shape, epilogue: int,
+                 stream: int = 0) -> None:
+    """Layer-level tensor-core convolution (device pointers, BF16 channels-last)."""
+    nz, ny, nx = shape
+    st = lib().xr_conv3d_fprop(ctypes.c_void_p(stream), ctypes.c_void_p(x), cin, ctypes.c_void_p(w),
+                               ctypes.c_void_p(bias or None), ctypes.c_void_p(mask or None), ctypes.c_void_p(y),
+                               cout, nx, ny, nz, epilogue)
+    if st:
+        raise XRError(st, "xr_conv3d_fprop")
+
+
+def conv3d_wgrad(x: int, cin: int, dy: int, cout: int, dw: int, shape, stream: int = 0) -> None:
+    """Layer-level weight gradient, accumulated into the FP32 dw[27][cout][cin]."""
+    nz, ny, nx = shape
+    st = lib().xr_conv3d_wgrad(ctypes.c_void_p(stream), ctypes.c_void_p(x), cin, ctypes.c_void_p(dy), cout,
+                               ctypes.c_void_p(dw), nx, ny, nz)
+    if st:
+        raise XRError(st, "xr_conv3d_wgrad")

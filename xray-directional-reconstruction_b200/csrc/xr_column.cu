@@ -359,6 +359,7 @@ struct BackColArgs {
     const BasisConst *basis;
     int art;
     float alpha;
+    int sr;                   /* 16-bit volumes: stochastic rounding of updates */
 };
 
 /* One view of one axis for a thread's column segment of 4 voxels: the ray
@@ -469,8 +470,9 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
             xyz_of<G>(ia, ib, igb + q, x, y, z);
             T *vp = reinterpret_cast<T *>(a.vol) + (size_t)x + (size_t)N * y + NN * z;
             const float tmp = acc[q][0], fac = acc[q][1], mu = ldf<T>(vp);
-            if (a.art) stf<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmp)));
-            else stf<T>(vp, (fac == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmp), fac));
+            const uint32_t key = (uint32_t)((size_t)x + (size_t)N * y + NN * z);
+            if (a.art) stu<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmp)), key, a.sr);
+            else stu<T>(vp, (fac == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmp), fac), key, a.sr);
         } else {
             int lx, ly, lz;
             xyz_of<G>(ca, cb, sg * 4 + q, lx, ly, lz);
@@ -524,11 +526,12 @@ __global__ void __launch_bounds__(kBackThreads, 4) k_back_col(BackColArgs a) {
             } else {
                 T *vp = reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3;
                 const float mu = ldf<T>(vp);
+                const uint32_t key = (uint32_t)(idx + (size_t)k * N3);
                 if (a.art) {
-                    stf<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, t)));
+                    stu<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, t)), key, a.sr);
                 } else {
                     const float f = a.fac_in[idx + (size_t)k * N3];
-                    stf<T>(vp, (f == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, t), f));
+                    stu<T>(vp, (f == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, t), f), key, a.sr);
                 }
             }
         }
@@ -623,6 +626,8 @@ cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const
                             const float *d_magsig, const float *proj, void *vol, const float *fac_in, float *fac_out,
                             int mode, int art, float alpha, int storage, cudaStream_t s) {
     BackColArgs a;
+    a.sr = (storage & kStoreStochastic) != 0;
+    storage &= ~kStoreStochastic;
     a.g = g;
     a.frames = frames;
     a.view_list = view_list;

@@ -273,6 +273,9 @@ static int aligned_axis(const std::vector<ViewFrame> &h, int cond, int V, float 
     return g;
 }
 
+/* storage type of measured sinograms */
+static int sino_st(const xr_ctx *c) { return c->sino_storage < 0 ? c->storage : c->sino_storage; }
+
 static const ColInfo *dcol(xr_ctx *c) { return (const ColInfo *)c->colinfo.p; }
 
 /* Forward splat of the listed views of the listed axes: column kernels for
@@ -456,7 +459,7 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
             {
                 Timed t(c, XR_T_RATIO);
                 if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, norm, s.d_sino, s.art,
-                                                     dl, s.storage, str), "ratio")))
+                                                     dl, s.sino_storage, str), "ratio")))
                     return st;
             }
             {
@@ -467,10 +470,11 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                     const float *sens =
                         s.art ? nullptr : (const float *)c->sens.p + (size_t)orders[b] * c->K * N3;
                     e = launch_back_col(c->gc, dbasis(c), fr, vl, s.subset_size, ci->all, c->C, ci->axis_g,
-                                        ci->magsig, proj, s.d_vol, sens, nullptr, 1, s.art, alpha, s.storage, str);
+                                        ci->magsig, proj, s.d_vol, sens, nullptr, 1, s.art, alpha, s.update_storage,
+                                        str);
                 } else {
                     e = launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, 0, c->C, proj, s.d_vol, 1, s.art,
-                                           alpha, s.storage, str);
+                                           alpha, s.update_storage, str);
                 }
                 if ((st = cuda_check(c, e, "XTT back"))) return st;
             }
@@ -481,7 +485,7 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
             const int *order = &orders[(size_t)cond * s.batch];
             float *pc = proj + (size_t)cond * blk;
             void *vc = (char *)s.d_vol + (size_t)cond * N3 * storage_bytes(s.storage);
-            const void *bc = (const char *)s.d_sino + (size_t)cond * blk * storage_bytes(s.storage);
+            const void *bc = (const char *)s.d_sino + (size_t)cond * blk * storage_bytes(s.sino_storage);
             cudaMemsetAsync(pc, 0, blk * sizeof(float), str);
             for (int b = 0; b < s.batch; b++) {
                 const int *vl = (const int *)c->subsets.p + (size_t)order[b] * s.subset_size;
@@ -494,7 +498,7 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                 {
                     Timed t(c, XR_T_RATIO);
                     if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, 1, pc, norm + (size_t)cond * blk,
-                                                         bc, s.art, dl + cond, s.storage, str), "ratio")))
+                                                         bc, s.art, dl + cond, s.sino_storage, str), "ratio")))
                         return st;
                 }
                 {
@@ -503,10 +507,11 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                     if (c->axis_g[cond] >= 0) {
                         const ColInfo *ci = dcol(c);
                         e = launch_back_col(c->gc, dbasis(c), fr, vl, s.subset_size, &ci->all[cond], 1, ci->axis_g,
-                                            ci->magsig, proj, vc, nullptr, nullptr, 0, s.art, alpha, s.storage, str);
+                                            ci->magsig, proj, vc, nullptr, nullptr, 0, s.art, alpha, s.update_storage,
+                                            str);
                     } else {
                         e = launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, cond, 1, proj, vc, 0, s.art,
-                                               alpha, s.storage, str);
+                                               alpha, s.update_storage, str);
                     }
                     if ((st = cuda_check(c, e, "back"))) return st;
                 }
@@ -514,6 +519,44 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
         }
     }
     return XR_OK;
+}
+
+static xr_status epoch_ready(xr_ctx *c) {
+    Session &s = c->sess;
+    if (!s.active) return fail(c, XR_ERR_STATE, "no active session (call xr_dev_session_begin)");
+    if (!s.xtt && s.epoch_done >= s.epochs) return fail(c, XR_ERR_STATE, "IR session: all planned epochs already run");
+    return XR_OK;
+}
+
+/* Subset orders of the session's next epoch (advances the XTT order). */
+static std::vector<int> next_orders(xr_ctx *c) {
+    Session &s = c->sess;
+    std::vector<int> orders;
+    if (s.xtt) {
+        /* a fresh default engine shuffles the persistent order (reconstruct.cu:858-859) */
+        std::mt19937_64 eng;
+        std::shuffle(s.order.begin(), s.order.end(), eng);
+        orders = s.order;
+    } else {
+        for (int cond = 0; cond < c->C; cond++) {
+            const int *o = &s.ir_orders[((size_t)cond * s.epochs + s.epoch_done) * s.batch];
+            orders.insert(orders.end(), o, o + s.batch);
+        }
+    }
+    return orders;
+}
+
+static xr_status loss_copy(xr_ctx *c, cudaStream_t str) {
+    return cuda_check(c, cudaMemcpyAsync(c->h_loss, c->loss.p, kMaxCond * sizeof(double), cudaMemcpyDeviceToHost, str),
+                      "loss copy");
+}
+
+static void loss_read(const xr_ctx *c, double *loss) {
+    if (c->sess.xtt) {
+        loss[0] = c->h_loss[0];
+    } else {
+        for (int cond = 0; cond < c->C; cond++) loss[cond] = c->h_loss[cond];
+    }
 }
 
 static void drop_graphs(xr_ctx *c) {
@@ -729,6 +772,17 @@ xr_status xr_set_option(xr_ctx *c, int key, int value) {
             c->views_per_cta = value;
             return XR_OK;
         case XR_OPT_GRAPHS: c->use_graphs = value != 0; return XR_OK;
+        case XR_OPT_XTT_SQRT: c->xtt_sqrt = value != 0; return XR_OK;
+        case XR_OPT_ROUNDING:
+            if (value < 0 || value > 1) return fail(c, XR_ERR_ARG, "rounding must be 0 (nearest) or 1 (stochastic)");
+            if (c->sess.active) return fail(c, XR_ERR_STATE, "rounding cannot change during a session");
+            c->stochastic = value != 0;
+            return XR_OK;
+        case XR_OPT_SINO_STORAGE:
+            if (value < -1 || value > 2) return fail(c, XR_ERR_ARG, "sinogram storage must be -1, 0, 1 or 2");
+            if (c->sess.active) return fail(c, XR_ERR_STATE, "storage cannot change during a session");
+            c->sino_storage = value;
+            return XR_OK;
         case XR_OPT_STORAGE:
             if (value < 0 || value > 2) return fail(c, XR_ERR_ARG, "storage must be 0 (FP32), 1 (BF16) or 2 (FP16)");
             if (c->sess.active) return fail(c, XR_ERR_STATE, "storage cannot change during a session");
@@ -787,6 +841,8 @@ xr_status xr_dev_session_begin(xr_ctx *c, const void *d_sino, void *d_vol, int x
     s.d_sino = d_sino;
     s.d_vol = d_vol;
     s.storage = c->storage;
+    s.sino_storage = sino_st(c);
+    s.update_storage = s.storage | ((c->stochastic && s.storage != 0) ? kStoreStochastic : 0);
     std::vector<int> lists((size_t)batch * s.subset_size);
     for (int sub = 0; sub < batch; sub++)
         for (int j = 0; j < s.subset_size; j++)   /* n = (sub + batch*j) % nProj, reconstruct.cu:89 */
@@ -835,23 +891,10 @@ xr_status xr_dev_session_begin(xr_ctx *c, const void *d_sino, void *d_vol, int x
 xr_status xr_dev_session_epoch(xr_ctx *c, double *loss) {
     if (!c) return XR_ERR_ARG;
     Session &s = c->sess;
-    if (!s.active) return fail(c, XR_ERR_STATE, "no active session (call xr_dev_session_begin)");
-    if (!s.xtt && s.epoch_done >= s.epochs)
-        return fail(c, XR_ERR_STATE, "IR session: all planned epochs already run");
     xr_status st;
+    if ((st = epoch_ready(c))) return st;
+    const std::vector<int> orders = next_orders(c);
     cudaStream_t str = c->stream;
-    std::vector<int> orders;
-    if (s.xtt) {
-        /* a fresh default engine shuffles the persistent order (reconstruct.cu:858-859) */
-        std::mt19937_64 eng;
-        std::shuffle(s.order.begin(), s.order.end(), eng);
-        orders = s.order;
-    } else {
-        for (int cond = 0; cond < c->C; cond++) {
-            const int *o = &s.ir_orders[((size_t)cond * s.epochs + s.epoch_done) * s.batch];
-            orders.insert(orders.end(), o, o + s.batch);
-        }
-    }
     if (c->use_graphs && !c->timing.on) {
         /* one CUDA graph per distinct subset order, captured on first use */
         auto it = s.graphs.find(orders);
@@ -878,16 +921,9 @@ xr_status xr_dev_session_epoch(xr_ctx *c, double *loss) {
     }
     s.epoch_done++;
     if (loss) {
-        double *dl = (double *)c->loss.p;
-        st = cuda_check(c, cudaMemcpyAsync(c->h_loss, dl, kMaxCond * sizeof(double), cudaMemcpyDeviceToHost, str),
-                        "loss copy");
-        if (st) return st;
+        if ((st = loss_copy(c, str))) return st;
         if ((st = cuda_check(c, cudaStreamSynchronize(str), "epoch"))) return st;
-        if (s.xtt) {
-            loss[0] = c->h_loss[0];
-        } else {
-            for (int cond = 0; cond < c->C; cond++) loss[cond] = c->h_loss[cond];
-        }
+        loss_read(c, loss);
     }
     return cuda_check(c, cudaGetLastError(), "epoch");
 }
@@ -899,7 +935,7 @@ xr_status xr_dev_session_end(xr_ctx *c, float *d_md, float *d_ev) {
     xr_status st = XR_OK;
     if (s.xtt) {
         const long nvox = (long)c->N * c->N * c->N;
-        {
+        if (c->xtt_sqrt) {
             Timed t(c, XR_T_ORIENT);
             st = cuda_check(c, launch_sqrt_abs(nvox * c->K, s.d_vol, s.storage, c->stream), "sqrt");   /* reconstruct.cu:919-922 */
         }
@@ -970,7 +1006,7 @@ xr_status xr_dev_residual(xr_ctx *c, const void *d_vol, const void *d_sino, xr_r
     cudaMemsetAsync(dl, 0, 3 * sizeof(double), c->stream);
     {
         Timed t(c, XR_T_OTHER);
-        if ((st = cuda_check(c, launch_residual((long)npx, p, d_sino, dl, c->storage, c->stream), "residual")))
+        if ((st = cuda_check(c, launch_residual((long)npx, p, d_sino, dl, sino_st(c), c->stream), "residual")))
             return st;
     }
     if ((st = cuda_check(c, cudaMemcpyAsync(c->h_loss, dl, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
@@ -1081,7 +1117,7 @@ xr_status xr_ir_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel, 
     xr_status st;
     if ((st = ensure_device(c))) return st;
     const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
-    if ((st = upload_planes_s(c, c->scratch_sino, sino, c->C, blk, c->storage, "sinogram"))) return st;
+    if ((st = upload_planes_s(c, c->scratch_sino, sino, c->C, blk, sino_st(c), "sinogram"))) return st;
     if ((st = upload_planes_s(c, c->scratch_vol, voxel, c->C, N3, c->storage, "volume"))) return st;
     if ((st = xr_dev_session_begin(c, c->scratch_sino.p, c->scratch_vol.p, 0, epoch, batch, dir, method, lambda)))
         return st;
@@ -1104,7 +1140,7 @@ xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
     if ((st = check_xtt_k(c))) return st;
     if ((st = ensure_device(c))) return st;
     const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
-    if ((st = upload_planes_s(c, c->scratch_sino, sino, c->C, blk, c->storage, "sinogram"))) return st;
+    if ((st = upload_planes_s(c, c->scratch_sino, sino, c->C, blk, sino_st(c), "sinogram"))) return st;
     if ((st = upload_planes_s(c, c->scratch_vol, voxel, c->K, N3, c->storage, "volume"))) return st;
     if ((st = xr_dev_session_begin(c, c->scratch_sino.p, c->scratch_vol.p, 1, epoch, batch, dir, method, lambda)))
         return st;
@@ -1184,7 +1220,7 @@ xr_status xr_residual(xr_ctx *c, const float *const *voxel, const float *const *
     const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
     if ((st = upload_planes_s(c, c->scratch_vol, voxel, xtt ? c->K : 1, N3, c->storage, "volume"))) return st;
     DevBuf b;
-    if ((st = upload_planes_s(c, b, sino, c->C, blk, c->storage, "sinogram"))) return st;
+    if ((st = upload_planes_s(c, b, sino, c->C, blk, sino_st(c), "sinogram"))) return st;
     st = xr_dev_residual(c, c->scratch_vol.p, b.p, dir, xtt, rel_l2, l1);
     release(b);
     return st;
@@ -1235,6 +1271,227 @@ xr_status xr_fdk_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
     if (st) return st;
     if ((st = download_planes(c, (const float *)c->scratch_vol.p, voxel, c->C, N3, "volume"))) return st;
     return download_planes(c, (const float *)x.fdk_sf.p, sino, c->C, blk, "filtered sinogram");
+}
+
+/* ---------------------------------------------------------------- batches */
+
+struct xr_batch {
+    std::vector<xr_ctx *> ctx;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaEvent_t> ev;                          /* fork, then one join per specimen */
+    std::map<std::vector<int>, cudaGraphExec_t> graphs;   /* per combination of subset orders */
+    std::string err;
+};
+
+static xr_status bfail(xr_batch *b, xr_status st, const std::string &m) {
+    b->err = m;
+    return st;
+}
+
+static xr_status bspec(xr_batch *b, int i, xr_status st) {
+    return bfail(b, st, "specimen " + std::to_string(i) + ": " + b->ctx[i]->err);
+}
+
+static void batch_drop_graphs(xr_batch *b) {
+    for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    b->graphs.clear();
+}
+
+xr_status xr_batch_create(xr_ctx *const *ctxs, int n, xr_batch **out) {
+    if (!ctxs || n < 1 || !out) return XR_ERR_ARG;
+    *out = nullptr;
+    for (int i = 0; i < n; i++)
+        if (!ctxs[i] || ctxs[i]->device != ctxs[0]->device) return XR_ERR_ARG;
+    for (int i = 0; i < n; i++) {
+        const xr_status st = ensure_device(ctxs[i]);
+        if (st) return st;
+    }
+    xr_batch *b = new xr_batch();
+    b->ctx.assign(ctxs, ctxs + n);
+    b->device = ctxs[0]->device;
+    cudaSetDevice(b->device);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    for (int i = 0; i <= n && e == cudaSuccess; i++) {
+        cudaEvent_t ev = nullptr;
+        e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) b->ev.push_back(ev);
+    }
+    if (e != cudaSuccess) {
+        xr_batch_destroy(b);
+        return XR_ERR_CUDA;
+    }
+    *out = b;
+    return XR_OK;
+}
+
+void xr_batch_destroy(xr_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_drop_graphs(b);
+    for (cudaEvent_t ev : b->ev) cudaEventDestroy(ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+const char *xr_batch_last_error(const xr_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+xr_status xr_batch_session_begin(xr_batch *b, const void *const *d_sinos, void *const *d_vols, int xtt, int epochs,
+                                 int subsets, xr_rotate dir, xr_method method, float lambda) {
+    if (!b || !d_sinos || !d_vols) return b ? bfail(b, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
+    batch_drop_graphs(b);
+    for (size_t i = 0; i < b->ctx.size(); i++) {
+        const xr_status st = xr_dev_session_begin(b->ctx[i], d_sinos[i], d_vols[i], xtt, epochs, subsets, dir, method,
+                                                  lambda);
+        if (st) return bspec(b, (int)i, st);
+    }
+    return XR_OK;
+}
+
+/* Fork every specimen's stream from the batch stream, enqueue its epoch,
+ * join it back. */
+static xr_status batch_issue(xr_batch *b, const std::vector<std::vector<int>> &orders) {
+    if (cudaEventRecord(b->ev[0], b->stream) != cudaSuccess) return bfail(b, XR_ERR_CUDA, "fork event");
+    for (size_t i = 0; i < b->ctx.size(); i++) {
+        xr_ctx *c = b->ctx[i];
+        if (cudaStreamWaitEvent(c->stream, b->ev[0], 0) != cudaSuccess) return bfail(b, XR_ERR_CUDA, "fork wait");
+        const xr_status st = issue_epoch(c, orders[i]);
+        if (st) return bspec(b, (int)i, st);
+        if (cudaEventRecord(b->ev[i + 1], c->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(b->stream, b->ev[i + 1], 0) != cudaSuccess)
+            return bfail(b, XR_ERR_CUDA, "join");
+    }
+    return XR_OK;
+}
+
+xr_status xr_batch_epoch(xr_batch *b, double *losses) {
+    if (!b) return XR_ERR_ARG;
+    cudaSetDevice(b->device);
+    const size_t n = b->ctx.size();
+    xr_status st;
+    bool timing = false;
+    for (size_t i = 0; i < n; i++) {
+        if ((st = epoch_ready(b->ctx[i]))) return bspec(b, (int)i, st);
+        timing = timing || b->ctx[i]->timing.on;
+    }
+    std::vector<std::vector<int>> orders(n);
+    std::vector<int> key;
+    for (size_t i = 0; i < n; i++) {
+        orders[i] = next_orders(b->ctx[i]);
+        key.insert(key.end(), orders[i].begin(), orders[i].end());
+        key.push_back(-1);
+    }
+    if (b->ctx[0]->use_graphs && !timing) {
+        auto it = b->graphs.find(key);
+        if (it == b->graphs.end()) {
+            if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+                return bfail(b, XR_ERR_CUDA, "begin capture");
+            const xr_status ist = batch_issue(b, orders);
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(b->stream, &graph);
+            if (ist) {
+                if (graph) cudaGraphDestroy(graph);
+                return ist;
+            }
+            if (ce != cudaSuccess) return bfail(b, XR_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ce));
+            cudaGraphExec_t exec = nullptr;
+            const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ie != cudaSuccess) return bfail(b, XR_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ie));
+            it = b->graphs.emplace(key, exec).first;
+        }
+        if (cudaGraphLaunch(it->second, b->stream) != cudaSuccess) return bfail(b, XR_ERR_CUDA, "graph launch");
+    } else {
+        if ((st = batch_issue(b, orders))) return st;
+    }
+    for (size_t i = 0; i < n; i++) b->ctx[i]->sess.epoch_done++;
+    if (losses) {
+        for (size_t i = 0; i < n; i++)
+            if ((st = loss_copy(b->ctx[i], b->stream))) return bspec(b, (int)i, st);
+    }
+    const cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return bfail(b, XR_ERR_CUDA, std::string("epoch: ") + cudaGetErrorString(e));
+    if (losses) {
+        double tmp[kMaxCond];
+        for (size_t i = 0; i < n; i++) {
+            loss_read(b->ctx[i], tmp);
+            losses[i] = tmp[0];
+        }
+    }
+    return XR_OK;
+}
+
+xr_status xr_batch_session_end(xr_batch *b) {
+    if (!b) return XR_ERR_ARG;
+    batch_drop_graphs(b);
+    xr_status first = XR_OK;
+    for (size_t i = 0; i < b->ctx.size(); i++) {
+        const xr_status st = xr_dev_session_end(b->ctx[i], nullptr, nullptr);
+        if (st && !first) first = bspec(b, (int)i, st);
+    }
+    return first;
+}
+
+xr_status xr_batch_autotune(xr_batch *b, int *chosen) {
+    if (!b) return XR_ERR_ARG;
+    cudaSetDevice(b->device);
+    batch_drop_graphs(b);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        return bfail(b, XR_ERR_CUDA, "events");
+    }
+    xr_status st = XR_OK;
+    for (size_t i = 0; i < b->ctx.size() && !st; i++) {
+        xr_ctx *c = b->ctx[i];
+        Session &s = c->sess;
+        if (!s.active || !s.xtt) {
+            st = bfail(b, XR_ERR_STATE, "autotune needs an active XTT session on every specimen");
+            break;
+        }
+        drop_graphs(c);
+        if ((st = ensure(c, c->scratch_sino, (size_t)c->C * c->V * c->Nd * c->Nd * sizeof(float), "autotune"))) {
+            st = bspec(b, (int)i, st);
+            break;
+        }
+        const int ss = s.subset_size;
+        std::vector<int> cand = {0, ss, (ss + 1) / 2, (ss + 3) / 4, 8, 4};
+        std::sort(cand.begin(), cand.end());
+        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+        const int saved = c->views_per_cta;
+        int best = saved;
+        float best_ms = 1e30f;
+        for (int v : cand) {
+            if (v > 64 || (v > ss && v != 0)) continue;
+            c->views_per_cta = v;
+            float total = 0.f;
+            for (int rep = 0; rep < 3 && !st; rep++) {
+                cudaEventRecord(e0, c->stream);
+                st = cuda_check(c, forward_dispatch(c, (const int *)c->subsets.p, ss, all_conds(c), s.d_vol,
+                                                    (float *)c->scratch_sino.p, 1, s.storage),
+                                "autotune forward");
+                cudaEventRecord(e1, c->stream);
+                if (!st) st = cuda_check(c, cudaEventSynchronize(e1), "autotune");
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0) total += ms;   /* first run warms up */
+            }
+            if (st) {
+                st = bspec(b, (int)i, st);
+                break;
+            }
+            if (total < best_ms) {
+                best_ms = total;
+                best = v;
+            }
+        }
+        c->views_per_cta = st ? saved : best;
+        if (chosen) chosen[i] = c->views_per_cta;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return st;
 }
 
 }  // extern "C"

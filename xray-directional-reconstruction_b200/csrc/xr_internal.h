@@ -20,6 +20,9 @@ namespace xr {
 constexpr int kMaxCond = 32;
 constexpr int kMaxBasis = 32;
 constexpr int kLossSlots = 64;   /* [0, 32): per-axis epoch losses; [40, 43): residual sums */
+/* Flag or-ed into the storage argument of the update launchers: 16-bit
+ * volumes are written with stochastic rounding. */
+constexpr int kStoreStochastic = 0x10;
 
 /* Per-(axis, view) constants of the reference's rayCasting (ir.cu:1860-1879),
  * computed once on the host with the reference's float operations.  The
@@ -85,7 +88,9 @@ struct Session {
     float lambda = 0.f;
     const void *d_sino = nullptr;     /* storage type */
     void *d_vol = nullptr;            /* storage type */
-    int storage = 0;
+    int storage = 0;                  /* volume                      */
+    int sino_storage = 0;             /* measured sinogram           */
+    int update_storage = 0;           /* volume, | kStoreStochastic  */
     std::vector<int> order;            /* persistent subset order (XTT)     */
     std::vector<int> ir_orders;        /* C*epochs rows (IR)                */
     std::map<std::vector<int>, cudaGraphExec_t> graphs;  /* per subset order */
@@ -108,6 +113,9 @@ struct xr_ctx {
     int fdk_axis_blocks = 0;
     int views_per_cta = 0;
     int storage = 0;
+    int sino_storage = -1;            /* -1: same as storage */
+    bool stochastic = true;           /* 16-bit updates: stochastic rounding */
+    bool xtt_sqrt = true;             /* XTT session end applies voxelSqrt   */
     bool use_graphs = false;
 
     xr::GeomConst gc{};

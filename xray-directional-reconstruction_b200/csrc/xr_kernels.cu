@@ -448,6 +448,7 @@ struct BackArgs {
     const BasisConst *basis;
     int art;
     float alpha;
+    int sr;                   /* 16-bit volumes: stochastic rounding of updates */
 };
 
 template <bool XTT, typename T>
@@ -536,16 +537,17 @@ __global__ void __launch_bounds__(kBackThreads) k_back_update(BackArgs a) {
     if (!XTT) {
         T *vp = reinterpret_cast<T *>(a.vol) + idx;
         const float mu = ldf<T>(vp);
-        if (a.art) stf<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmp)));
-        else stf<T>(vp, (fac == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmp), fac));
+        if (a.art) stu<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmp)), (uint32_t)idx, a.sr);
+        else stu<T>(vp, (fac == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmp), fac), (uint32_t)idx, a.sr);
     } else {
 #pragma unroll
         for (int k = 0; k < 16; k++) {
             if (k >= g.K) break;
             T *vp = reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3;
             const float mu = ldf<T>(vp);
-            if (a.art) stf<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmpk[k])));
-            else stf<T>(vp, (fack[k] == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmpk[k]), fack[k]));
+            const uint32_t key = (uint32_t)(idx + (size_t)k * N3);
+            if (a.art) stu<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmpk[k])), key, a.sr);
+            else stu<T>(vp, (fack[k] == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmpk[k]), fack[k]), key, a.sr);
         }
     }
 }
@@ -672,6 +674,8 @@ cudaError_t launch_back_update(const GeomConst &g, const BasisConst *d_basis, co
                                const int *view_list, int n_views, int cond0, int n_cond, const float *proj,
                                void *vol, int xtt, int art, float alpha, int storage, cudaStream_t s) {
     BackArgs a;
+    a.sr = (storage & kStoreStochastic) != 0;
+    storage &= ~kStoreStochastic;
     a.g = g;
     a.frames = frames;
     a.view_list = view_list;

@@ -8,6 +8,7 @@
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <stdint.h>
 
 namespace xr {
 
@@ -42,6 +43,45 @@ template <>
 __device__ __forceinline__ void stf<__half>(__half *p, float v) { *p = __float2half_rn(v); }
 
 inline size_t storage_bytes(int storage) { return storage == kF32 ? 4 : 2; }
+
+/* 32-bit integer mixer ("lowbias32", from C. Wellons' public-domain hash
+ * prospector). */
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+/* Store of an iterative update.  16-bit types with sr != 0 round
+ * stochastically: up with probability (v - lo) / (hi - lo) between the two
+ * neighbours lo <= v <= hi, so updates smaller than half a unit in the last
+ * place still move the stored value in expectation (nearest rounding
+ * returns them unchanged and the iteration stalls).  The uniform draw is a
+ * hash of the element index and the FP32 value: deterministic, and fresh
+ * whenever the value changes. */
+template <typename T>
+__device__ __forceinline__ void stu(T *p, float v, uint32_t key, int sr);
+template <>
+__device__ __forceinline__ void stu<float>(float *p, float v, uint32_t, int) { *p = v; }
+template <>
+__device__ __forceinline__ void stu<__nv_bfloat16>(__nv_bfloat16 *p, float v, uint32_t key, int sr) {
+    if (!sr) { *p = __float2bfloat16_rn(v); return; }
+    const __nv_bfloat16 lo = __float2bfloat16_rd(v), hi = __float2bfloat16_ru(v);
+    const float flo = __bfloat162float(lo), fhi = __bfloat162float(hi);
+    const float t = (float)(mix32(__float_as_uint(v) ^ (key * 0x9E3779B9u)) >> 8) * 5.9604645e-08f;   /* [0, 1) */
+    *p = (fhi != flo && t * (fhi - flo) < (v - flo)) ? hi : lo;
+}
+template <>
+__device__ __forceinline__ void stu<__half>(__half *p, float v, uint32_t key, int sr) {
+    if (!sr) { *p = __float2half_rn(v); return; }
+    const __half lo = __float2half_rd(v), hi = __float2half_ru(v);
+    const float flo = __half2float(lo), fhi = __half2float(hi);
+    const float t = (float)(mix32(__float_as_uint(v) ^ (key * 0x9E3779B9u)) >> 8) * 5.9604645e-08f;
+    *p = (fhi != flo && t * (fhi - flo) < (v - flo)) ? hi : lo;
+}
 
 }  // namespace xr
 

@@ -1,0 +1,129 @@
+/*
+ * sm_100a tensor-core primitives in inline PTX: tcgen05.mma (kind::f16, BF16
+ * operands from shared memory, FP32 accumulator in tensor memory), its commit
+ * to an mbarrier, tensor-memory allocation and loads, and bounded mbarrier
+ * waits.
+ *
+ * Shared-memory operand layout: no swizzle ("interleaved").  A core matrix is
+ * 8 rows x 16 bytes stored as 128 contiguous bytes.  K-major operands keep 8
+ * consecutive K elements of one M (or N) row in a 16-byte row of the core
+ * matrix; MN-major operands keep 8 consecutive M (or N) elements of one K.
+ * The descriptor's leading byte offset (LBO) is the distance between core
+ * matrices adjacent along K, the stride byte offset (SBO) the distance between
+ * core matrices adjacent along M / N.
+ */
+#ifndef XR_TC_CUH
+#define XR_TC_CUH
+
+#include <stdint.h>
+
+namespace xr {
+namespace tc {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+/* Shared-memory matrix descriptor: start address, LBO, SBO (bytes, multiples
+ * of 16), descriptor version 1, base offset 0, no swizzle. */
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+/* Instruction descriptor, kind::f16: FP32 accumulator, BF16 A and B, dense,
+ * A/B K-major (0) or MN-major (1), N / 8 at bit 17, M / 16 at bit 24. */
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int a_mn, int b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+/* Generic-proxy shared-memory writes become visible to the tensor core. */
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+/* Waits for the phase of the given parity to complete; gives up after about
+ * `limit` clock cycles (false). */
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
+    if (mbar_test(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_test(bar, parity))
+        if (clock64() - t0 > limit) return false;
+    return true;
+}
+
+/* Tensor memory: whole-warp allocation of ncols columns (power of two >= 32);
+ * the base address is written to shared memory. */
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+/* D[tmem] (+)= A[smem] * B[smem]^T, one CTA, issued by one thread. */
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+/* The mbarrier receives one arrival when every tcgen05.mma issued so far by
+ * this thread has completed. */
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+/* Lane-per-thread loads of 16 / 32 consecutive FP32 columns (32x32b shape):
+ * thread t of the warp receives lane (taddr.lane + t). */
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+    tmem_ld16(taddr, v);
+    tmem_ld16(taddr + 16, v + 16);
+}
+
+}  // namespace tc
+}  // namespace xr
+
+#endif
