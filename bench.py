@@ -106,6 +106,49 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_tensor_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+def conv_roofline(local: int, N: int = 256, reps: int = 3):
+    """Tensor-core roofline of the warm-start network's inference on an
+    N^3 x 13 BF16 volume (in place): algorithmic FLOPs = 2 * nvox * 27 *
+    sum_l cin_l * cout_l (unpadded channels) over the CUDA-event time of one
+    inference (the network's conv launches plus the input packing)."""
+    import struct
+    import torch
+    ws = load_warmstart()
+    if not os.path.exists(ws.WEIGHTS):
+        return None
+    with open(ws.WEIGHTS, "rb") as f:
+        channels, width, depth = struct.unpack("<3i", f.read(20)[8:20])
+    net = ws.load_net(ws.WEIGHTS, local)
+    stream = torch.cuda.current_stream()
+    net.set_stream(stream.cuda_stream)
+    vol = torch.full((channels, N, N, N), 0.5, dtype=torch.bfloat16, device="cuda")
+    net.infer(vol.data_ptr(), vol.data_ptr(), (N, N, N), storage=1, floor_value=-1e30)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        net.infer(vol.data_ptr(), vol.data_ptr(), (N, N, N), storage=1, floor_value=-1e30)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    macs = 27 * sum(ci * co for ci, co in
+                    [((channels if l == 0 else width), (channels if l == depth - 1 else width)) for l in range(depth)])
+    flops = 2.0 * N ** 3 * macs
+    peak, kind = measured_tensor_peak()
+    net.close()
+    return {"bound": "tensor", "kernel": "k_conv_halo (tcgen05, BF16 x BF16 -> FP32)", "achieved": flops / ms / 1e9,
+            "peak": peak, "unit": "TFLOP/s", "frac": flops / ms / 1e9 / peak, "peak_kind": kind,
+            "infer_ms": ms, "flops_per_inference": flops, "workload": f"{N}^3 x {channels}, depth {depth}, width {width}"}
+
+
 def profile_traffic(kernel: str):
     """Per-launch DRAM bytes of `kernel` at this workload from the committed
     ncu summary, if present (profiles/*.md line 'traffic_per_launch <kernel> <bytes>')."""
@@ -285,8 +328,7 @@ def run_ttr(args, local):
             if not os.path.exists(ws.WEIGHTS):
                 arms[name] = {"unavailable": "no trained weights at " + os.path.relpath(ws.WEIGHTS, ROOT)}
                 return
-            net = xr.Net(K, 32, 4)
-            net.load(ws.WEIGHTS)
+            net = ws.load_net(ws.WEIGHTS, local)
             net.set_stream(scan.stream.cuda_stream)
             ms0 = ws.warm_start(scan, net, b, vol, args.early, W["batch"], storage, 0)
             e0 = args.early
@@ -311,7 +353,107 @@ def run_ttr(args, local):
     p, l = arms.get("plain_f32", {}), arms.get("learned_bf16", {})
     line["speedup_learned_bf16_vs_plain_f32"] = (p["seconds"] / l["seconds"]) if p.get("seconds") and \
         l.get("seconds") else None
+    scan.ctx.close()
+    return line
+
+
+def run_c4(args, local):
+    """Uneven batch: 8 XTT specimens with N drawn from {96, 128, 160, 192}
+    (seed 4), 3 axes x U{90..180} views, 256^2 detector, K = 13; BF16
+    volumes and sinograms with stochastic rounding, FP32 arithmetic, FP64
+    residual norms.  One batched epoch (all specimens forked onto their
+    streams, replayed as one CUDA graph, views-per-CTA autotuned) against the
+    same epochs run specimen after specimen; per specimen the BF16 result's
+    error against an FP32 run of the same epochs."""
+    import torch
+    ws = load_warmstart()
+    xr = load_pkg()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    rng = np.random.default_rng(4)
+    sizes = [int(v) for v in rng.choice([96, 128, 160, 192], 8)]
+    views = [int(v) for v in rng.integers(90, 181, 8)]
+    basis = basis13()
+    specs = []
+    for i, (N, V) in enumerate(zip(sizes, views)):
+        ctx = xr.Context.create(1000.0, 500.0, 2.0, N, 256, V, three_axes(), None, None, basis, device=local)
+        ctx.set_stream(stream.cuda_stream)   # batch forks onto each context's own stream below
+        mu = torch.empty((13, N, N, N), dtype=torch.float32, device="cuda")
+        ws.fiber_phantom_dev(mu.data_ptr(), N, 12, 400 + i, basis, stream.cuda_stream)
+        b = torch.empty((3, V, 256, 256), dtype=torch.float32, device="cuda")
+        ctx.dev_forward(mu.data_ptr(), b.data_ptr(), True)
+        specs.append({"N": N, "V": V, "ctx": ctx, "b32": b, "b16": b.to(torch.bfloat16)})
+    torch.cuda.synchronize()
+    E = args.steps
+
+    def fresh(storage):
+        dt = torch.bfloat16 if storage else torch.float32
+        return [torch.full((13, sp["N"], sp["N"], sp["N"]), 0.01, dtype=dt, device="cuda") for sp in specs]
+
+    def set_opts(storage, graphs):
+        for sp in specs:
+            sp["ctx"].set_option(xr.Option.STORAGE, storage)
+            sp["ctx"].set_option(xr.Option.GRAPHS, graphs)
+            sp["ctx"].set_option(xr.Option.XTT_SQRT, 0)
+
+    # FP32 reference results (specimen after specimen)
+    set_opts(0, 0)
+    ref = fresh(0)
+    for sp, v in zip(specs, ref):
+        sp["ctx"].dev_session_begin(sp["b32"].data_ptr(), v.data_ptr(), True, E + 1, 5)
+        for _ in range(E + 1):
+            sp["ctx"].dev_session_epoch()
+        sp["ctx"].dev_session_end(0, 0)
+    # sequential BF16: each specimen's own session and graphs
+    set_opts(1, 1)
+    seq = fresh(1)
+    seq_ms = 0.0
+    for sp, v in zip(specs, seq):
+        c = sp["ctx"]
+        c.dev_session_begin(sp["b16"].data_ptr(), v.data_ptr(), True, E + 1, 5)
+        c.dev_session_epoch()                                  # warm-up (graph capture)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(E):
+            c.dev_session_epoch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        seq_ms += e0.elapsed_time(e1)
+        c.dev_session_end(0, 0)
+    # batched BF16: every specimen's epoch in one graph
+    for sp in specs:
+        sp["ctx"].set_stream(0)                                # each context back on its own stream
+    bat = fresh(1)
+    batch = xr.Batch([sp["ctx"] for sp in specs])
+    batch.session_begin([sp["b16"].data_ptr() for sp in specs], [v.data_ptr() for v in bat], True, E + 1, 5)
+    chosen = batch.autotune()
+    batch.epoch()                                              # warm-up (graph capture)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(E):
+        batch.epoch()
+    bat_ms = (time.perf_counter() - t0) * 1e3                  # each epoch call ends with a synchronize
+    batch.session_end()                                        # XTT_SQRT 0: the iterates stay
+    batch.close()
+    per = []
+    for sp, v, r, vpc in zip(specs, bat, ref, chosen):
+        c = sp["ctx"]
+        c.set_option(xr.Option.SINO_STORAGE, 0)                # residual against the FP32 data
+        res, _ = c.dev_residual(v.data_ptr(), sp["b32"].data_ptr(), True)
+        err = float((v.float() - r).abs().max() / r.abs().max())
+        per.append({"N": sp["N"], "views": sp["V"], "views_per_cta": vpc, "residual_rel_l2": res,
+                    "bf16_vs_fp32_max_rel": err})
+    vox_views = sum(3 * sp["V"] * sp["N"] ** 3 for sp in specs)
+    line = {"mode": "uneven_batch", "specimens": per, "epochs_timed": E, "storage": "bf16 volumes and sinograms, "
+            "stochastic rounding", "sequential_ms_per_epoch": seq_ms / E, "batched_ms_per_epoch": bat_ms / E,
+            "speedup_batched": seq_ms / bat_ms, "gvoxel_views_per_s_batched": 2 * vox_views / (bat_ms / E / 1e3) / 1e9,
+            "note": "batched time by host clock around synchronized epoch calls; sequential by CUDA events"}
     print(json.dumps(line), flush=True)
+    for sp in specs:
+        sp["ctx"].close()
 
 
 def main():
@@ -329,7 +471,9 @@ def main():
     ap.add_argument("--max-epochs", type=int, default=1000)
     ap.add_argument("--check-every", type=int, default=10)
     ap.add_argument("--early", type=int, default=5, help="--ttr: OS-EM epochs before the warm-start network")
-    ap.add_argument("--arms", default="plain_f32,learned_bf16,plain_bf16", help="--ttr arms")
+    ap.add_argument("--arms", default="plain_f32,learned_bf16", help="--ttr arms (also plain_bf16, learned_f32)")
+    ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-residual comparison of the default run")
+    ap.add_argument("--c4", action="store_true", help="uneven batch of 8 specimens (BF16), batched vs sequential")
     args = ap.parse_args()
     if args.size == "profile":
         W.update(W_PROFILE)
@@ -348,9 +492,12 @@ def main():
     import torch
 
     torch.cuda.set_device(local)
-    if args.ttr:
-        if rank == 0:          # one GPU: the time-to-residual comparison runs on rank 0 only
-            run_ttr(args, local)
+    if args.ttr or args.c4:
+        if rank == 0:          # one GPU: these comparisons run on rank 0 only
+            if args.ttr:
+                print(json.dumps(run_ttr(args, local)), flush=True)
+            else:
+                run_c4(args, local)
         return
     if world > 1:
         rp.init("nccl")
@@ -516,6 +663,21 @@ def main():
                "sample": f"{n_views} of {C * V} views (forward+ratio+back, all K), reference ir.cu kernels "
                          "compiled for the host, OpenMP"}
 
+    ttr = None
+    if world == 1 and not args.no_ttr and args.size == "full":
+        ctx.close()
+        del d_true, d_b, d_vol
+        torch.cuda.empty_cache()
+        t = run_ttr(args, local)
+        ttr = {"target_rel_residual": t["target"], "speedup_learned_bf16_vs_plain_f32":
+               t["speedup_learned_bf16_vs_plain_f32"], "note": "device time to the target, residual checked every "
+               f"{t['check_every']} epochs outside the timed work; same data b = A mu_true (held-out phantom)"}
+        for k, a in t["arms"].items():
+            ttr[k] = {x: a.get(x) for x in ("seconds", "epochs", "reached", "residual_final", "storage",
+                                            "unavailable") if x in a}
+    conv = None
+    if world == 1 and args.size == "full":
+        conv = conv_roofline(local)
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -525,7 +687,7 @@ def main():
                        "residual_rel_l2_after": rel},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in tim.items() if v[1]},
-            "variants_ms_per_step": variants}
+            "variants_ms_per_step": variants, "time_to_residual": ttr, "roofline_conv": conv}
     print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -123,7 +123,7 @@ struct FwdColArgs {
 };
 
 template <int MODE, int G, typename T>
-__global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
+__global__ void __launch_bounds__(kFwdThreads, 3) k_fwd_col(FwdColArgs a) {
     const T *vol = reinterpret_cast<const T *>(a.vol);
     constexpr int A = Ax<G>::A, B = Ax<G>::B;
     /* Two detector tiles (double-buffered over views) in two-word fixed
@@ -377,30 +377,42 @@ __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f
     if (!tap1(g, u, iu, fu, gu)) return;
     const float dab2 = fmaf(da, da, db * db);
     const float *Pc = Pv + iu;
+    /* Two phases: first every voxel's taps and its 4 gathers (16 loads in
+     * flight; a voxel off the detector reads row 0 and is dropped), then the
+     * accumulation. */
+    float fv[4], gv[4], dg[4], pr[4][4];
+    bool ok[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        if (q >= nq) continue;
-        float dg;
-        const float v = col_v<G>(f, g, bg[q], coeff, magsig, dg);
-        int iv;
-        float fv, gv;
-        if (!tap1(g, v, iv, fv, gv)) continue;
+        const float v = col_v<G>(f, g, bg[q], coeff, magsig, dg[q]);
+        int iv = 0;
+        ok[q] = (q < nq) && tap1(g, v, iv, fv[q], gv[q]);
+        if (MODE != B_SENS) {
+            const float *pp = Pc + (size_t)Nd * (ok[q] ? iv : 0);
+            pr[q][0] = __ldg(pp);
+            pr[q][1] = __ldg(pp + 1);
+            pr[q][2] = __ldg(pp + Nd);
+            pr[q][3] = __ldg(pp + Nd + 1);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (!ok[q]) continue;
         float nb = 0.f;
         if (MODE != B_SENS) {
-            const float c1 = __fmul_rn(gu, fv), c2 = __fmul_rn(fu, fv);
-            const float c3 = __fmul_rn(fu, gv), c4 = __fmul_rn(gu, gv);
-            const float *pp = Pc + (size_t)Nd * iv;
-            const float p4 = __ldg(pp), p3 = __ldg(pp + 1), p1 = __ldg(pp + Nd), p2 = __ldg(pp + Nd + 1);
-            nb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(c1, p1), __fmul_rn(c2, p2)), __fmul_rn(c3, p3)),
-                           __fmul_rn(c4, p4));
+            const float c1 = __fmul_rn(gu, fv[q]), c2 = __fmul_rn(fu, fv[q]);
+            const float c3 = __fmul_rn(fu, gv[q]), c4 = __fmul_rn(gu, gv[q]);
+            nb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(c1, pr[q][2]), __fmul_rn(c2, pr[q][3])),
+                                     __fmul_rn(c3, pr[q][1])),
+                           __fmul_rn(c4, pr[q][0]));
         }
         if (MODE == B_PLAIN) {
             acc[q][0] = __fadd_rn(acc[q][0], nb);     /* tmp    (ir.cu:1750) */
             acc[q][1] = __fadd_rn(acc[q][1], 1.0f);   /* factor (ir.cu:1749) */
         } else {
             float d[3];
-            d[A] = da; d[B] = db; d[G] = dg;
-            const float inv = __frcp_rn(fmaf(dg, dg, dab2));
+            d[A] = da; d[B] = db; d[G] = dg[q];
+            const float inv = __frcp_rn(fmaf(dg[q], dg[q], dab2));
             float wgt;
             if (MODE == B_XTT) {
                 acc[q][6] += nb;

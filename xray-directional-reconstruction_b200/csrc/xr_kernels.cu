@@ -118,7 +118,7 @@ struct FwdArgs {
 };
 
 template <int MODE, typename T>
-__global__ void __launch_bounds__(kFwdThreads, 2) k_forward(FwdArgs a) {
+__global__ void __launch_bounds__(kFwdThreads, 3) k_forward(FwdArgs a) {
     const T *vol = reinterpret_cast<const T *>(a.vol);
     /* Detector tiles in two-word fixed point (xr_tile.cuh). */
     extern __shared__ int smem[];

@@ -28,7 +28,7 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-WEIGHTS = os.path.join(HERE, "weights", "warmstart_k13_w32_d4.bin")
+WEIGHTS = os.path.join(HERE, "weights", "warmstart_k13.bin")
 
 
 def _pkg():
@@ -40,6 +40,20 @@ def _pkg():
     sys.modules["xrd"] = mod
     spec.loader.exec_module(mod)
     return mod
+
+
+def load_net(path: str = WEIGHTS, device: int = 0):
+    """A network of the shape recorded in a weights file (xr_net_save
+    format: magic, int32 channels, width, depth, FP32 parameters)."""
+    import struct
+    with open(path, "rb") as f:
+        head = f.read(20)
+    if len(head) < 20 or head[:6] != b"XRNET1":
+        raise ValueError(f"not a network file: {path}")
+    channels, width, depth = struct.unpack("<3i", head[8:20])
+    net = _pkg().Net(channels, width, depth, device=device)
+    net.load(path)
+    return net
 
 
 def cubic13() -> np.ndarray:
@@ -244,8 +258,9 @@ def main(argv=None):
     ap.add_argument("--crops", type=int, default=4)
     ap.add_argument("--crop", type=int, default=64)
     ap.add_argument("--early", type=int, default=5)
-    ap.add_argument("--steps", type=int, default=4000)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--depth", type=int, default=6)
+    ap.add_argument("--steps", type=int, default=12000)
+    ap.add_argument("--lr", type=float, default=1.5e-3)
     ap.add_argument("--storage", type=int, default=1, help="volume storage of the early iterates (1 = BF16)")
     ap.add_argument("--log", default="")
     args = ap.parse_args(argv)
@@ -256,7 +271,7 @@ def main(argv=None):
     xin, tgt = make_pool(scan, range(args.seed0, args.seed0 + args.phantoms), args.crops, args.crop, args.early,
                          storage=args.storage)
     t1 = time.time()
-    net = xr.Net(scan.K, 32, 4, seed=0)
+    net = xr.Net(scan.K, 32, args.depth, seed=0)
     net.set_stream(scan.stream.cuda_stream)
     trace = train(net, xin, tgt, args.steps, args.lr)
     torch.cuda.synchronize()
@@ -264,7 +279,8 @@ def main(argv=None):
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     net.save(args.out)
     rec = {"pairs": int(xin.shape[0]), "phantoms": args.phantoms, "seeds": [args.seed0, args.seed0 + args.phantoms - 1],
-           "N": args.N, "crop": args.crop, "early_epochs": args.early, "steps": args.steps, "lr": args.lr,
+           "N": args.N, "crop": args.crop, "early_epochs": args.early, "depth": args.depth, "steps": args.steps,
+           "lr": args.lr,
            "storage": args.storage,
            "pool_s": t1 - t0, "train_s": t2 - t1, "loss_trace": trace}
     print(json.dumps(rec))
