@@ -474,6 +474,8 @@ def main():
     ap.add_argument("--arms", default="plain_f32,learned_bf16", help="--ttr arms (also plain_bf16, learned_f32)")
     ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-residual comparison of the default run")
     ap.add_argument("--c4", action="store_true", help="uneven batch of 8 specimens (BF16), batched vs sequential")
+    ap.add_argument("--conv", type=int, default=0, metavar="N",
+                    help="only the warm-start network's tensor-core roofline on an N^3 x 13 volume")
     args = ap.parse_args()
     if args.size == "profile":
         W.update(W_PROFILE)
@@ -492,6 +494,11 @@ def main():
     import torch
 
     torch.cuda.set_device(local)
+    if args.conv:
+        if rank == 0:
+            torch.cuda.set_stream(torch.cuda.Stream())
+            print(json.dumps(conv_roofline(local, args.conv)), flush=True)
+        return
     if args.ttr or args.c4:
         if rank == 0:          # one GPU: these comparisons run on rank 0 only
             if args.ttr:

@@ -10,15 +10,14 @@
  * channels are 32 or 64 contiguous bytes: exactly the 16-byte rows the tensor
  * core's shared-memory operands are built of.
  *
- *  k_conv_fwd (fprop and dgrad): M = 128 consecutive voxels, N = output
- *    channels, K = 27 taps x input channels.  A CTA keeps all 27 taps of the
- *    weights in shared memory (K-major core matrices) and streams the voxel
- *    tile of one tap at a time through a 4-stage ring: every thread loads its
- *    voxel's neighbour row for the next tap while one thread issues the
- *    current tap's MMAs and commits them to the stage's mbarrier, whose
- *    completion frees the stage.  dgrad is the same operator on the output
- *    gradient with the weights transposed and the taps mirrored; its
- *    epilogue multiplies by the ReLU derivative (forward activation > 0).
+ *  k_conv_halo (fprop and dgrad): M = 128 voxels (an 8 x 16 patch of one
+ *    z-slice), N = output channels, K = 27 taps x input channels.  A CTA keeps
+ *    all 27 taps of the weights in shared memory (K-major core matrices) and
+ *    a ring of halo slices; every tap's operand is a shifted window of the
+ *    halo, addressed by the descriptor alone, so a slice costs one load of
+ *    its halo and 27 x K/16 back-to-back MMAs.  dgrad is the same operator on
+ *    the output gradient with the weights transposed and the taps mirrored;
+ *    its epilogue multiplies by the ReLU derivative (forward activation > 0).
  *  k_conv_wgrad: M = 128 (tap, input channel) rows, N = output channels,
  *    K = voxels in chunks of 64; both operands MN-major, so the 16-byte rows
  *    come straight from the channels-last tensors.  CTAs split the voxels
@@ -47,7 +46,6 @@ namespace xr {
 namespace {
 
 constexpr int kConvThreads = 128;
-constexpr int kStages = 4;
 constexpr long long kWaitCycles = 4000000000LL;   /* ~2 s at 1.9 GHz */
 constexpr int kTmemCols = 32;
 
@@ -97,37 +95,105 @@ __device__ __forceinline__ uint8_t *align1k(uint8_t *p) {
     return p + (((s + 1023u) & ~1023u) - s);
 }
 
+/* Output of one voxel's NP accumulators (row of the M = 128 tile). */
+template <int NP, int EPI>
+__device__ __forceinline__ void conv_epilogue(const ConvArgs &a, long v, long nvox, const float *acc) {
+    if (EPI == EPI_RESID) {
+#pragma unroll
+        for (int n = 0; n < NP; n++) {
+            if (n >= a.nout) break;
+            const size_t i = (size_t)n * nvox + v;
+            float val = acc[n] + (a.bias ? a.bias[n] : 0.f);
+            if (a.storage == kBF16) {
+                val = fmaxf(ldf(reinterpret_cast<const __nv_bfloat16 *>(a.res) + i) + val * a.inv_scale,
+                            a.floor_value);
+                stf(reinterpret_cast<__nv_bfloat16 *>(a.out) + i, val);
+            } else if (a.storage == kF16) {
+                val = fmaxf(ldf(reinterpret_cast<const __half *>(a.res) + i) + val * a.inv_scale, a.floor_value);
+                stf(reinterpret_cast<__half *>(a.out) + i, val);
+            } else {
+                val = fmaxf(ldf(reinterpret_cast<const float *>(a.res) + i) + val * a.inv_scale, a.floor_value);
+                stf(reinterpret_cast<float *>(a.out) + i, val);
+            }
+        }
+    } else {
+        uint4 *yo = reinterpret_cast<uint4 *>(a.y + (size_t)v * NP);
+        const uint4 *mk = reinterpret_cast<const uint4 *>(a.mask + (size_t)v * NP);
+#pragma unroll
+        for (int j = 0; j < NP / 8; j++) {
+            float o[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int n = 8 * j + i;
+                o[i] = acc[n];
+                if (EPI != EPI_MASK && a.bias) o[i] += a.bias[n];
+                if (EPI == EPI_RELU) o[i] = fmaxf(o[i], 0.f);
+            }
+            if (EPI == EPI_MASK) {
+                const uint4 m = mk[j];
+                const uint32_t mw[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    if (!(bf_lo(mw[i]) > 0.f)) o[2 * i] = 0.f;
+                    if (!(bf_hi(mw[i]) > 0.f)) o[2 * i + 1] = 0.f;
+                }
+            }
+            yo[j] = make_uint4(pack2(o[0], o[1]), pack2(o[2], o[3]), pack2(o[4], o[5]), pack2(o[6], o[7]));
+        }
+    }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Spatial-tile convolution (fprop / dgrad).                               */
+/* An output tile is 8 (x) x 16 (y) voxels of one z-slice: M = 128 rows,   */
+/* row r = (x = r % 8, y = r / 8).  The input around it is a halo slice of */
+/* 10 x 18 voxels, stored as KP/8 planes of 16-byte rows (plane j holds    */
+/* channels 8j..8j+7 of every halo voxel, x fastest).  For tap (dz,dy,dx)  */
+/* the A operand is then a window of the halo: 8 consecutive 16-byte rows  */
+/* are the 8 x-voxels of one y-row (a core matrix), y-rows are 160 bytes   */
+/* apart (SBO), planes PLANE bytes apart (LBO) - the descriptor's start    */
+/* address moves by (dy * 10 + dx) * 16 bytes and by one slice for dz.     */
+/* No per-tap loads or barriers: each input slice is loaded once (zero     */
+/* outside the volume) into a 4-slot ring and serves three output slices;  */
+/* the 27 x KP/16 MMAs of a slice are issued back to back into one of two  */
+/* tensor-memory accumulators while the previous slice's epilogue runs.    */
+/* ---------------------------------------------------------------------- */
+constexpr int kHX = 10, kHY = 18, kHV = kHX * kHY;   /* halo slice: 180 voxels */
+constexpr int kRing = 4;
+
 template <int KP, int NP>
-struct FwdSmem {
-    static constexpr int BT = NP * KP * 2;                          /* one tap of weights */
+struct HaloSmem {
+    static constexpr int BT = NP * KP * 2;
     static constexpr int BB = ((27 * BT + 1023) / 1024) * 1024;
-    static constexpr int AB = 128 * KP * 2;                         /* one A stage        */
-    static constexpr int bytes = 1024 + BB + kStages * AB + kStages * 8 + 16;
+    static constexpr int PLANE = kHV * 16;                       /* 2880 bytes */
+    static constexpr int SLOT = (KP / 8) * PLANE;
+    static constexpr int bytes = 1024 + BB + kRing * SLOT + 2 * 8 + 16;
+    static constexpr int LOADS = (kHV * KP / 8 + kConvThreads - 1) / kConvThreads;   /* 16-byte loads per thread */
 };
 
 template <int KP, int NP, int EPI>
-__global__ void __launch_bounds__(kConvThreads) k_conv_fwd(ConvArgs a) {
-    using L = FwdSmem<KP, NP>;
-    constexpr uint32_t SBO = (KP / 8) * 128;                        /* next 8 rows (M or N) */
+__global__ void __launch_bounds__(kConvThreads) k_conv_halo(ConvArgs a, int zchunk) {
+    using L = HaloSmem<KP, NP>;
+    constexpr uint32_t SBO_B = (KP / 8) * 128;
     constexpr uint32_t IDESC = tc::idesc_bf16(128, NP, 0, 0);
     extern __shared__ uint8_t smem_raw[];
     uint8_t *sm = align1k(smem_raw);
-    uint8_t *sB = sm, *sA = sm + L::BB;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sA + kStages * L::AB);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + kStages);
+    uint8_t *sB = sm, *ring = sm + L::BB;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(ring + kRing * L::SLOT);   /* one per accumulator */
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
     __shared__ int s_abort;
 
     const int tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) {
-        for (int s = 0; s < kStages; s++) tc::mbar_init(&bar[s], 1);
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
         tc::fence_mbar_init();
         s_abort = 0;
     }
-    if (warp == 0) tc::tmem_alloc(tslot, kTmemCols);
-    /* weights -> K-major core matrices: (tap, n, 8-channel group j) */
+    if (warp == 0) tc::tmem_alloc(tslot, 2 * kTmemCols);
     for (int c = tid; c < 27 * NP * KP / 8; c += kConvThreads) {
         const int j = c % (KP / 8), n = (c / (KP / 8)) % NP, t = c / (NP * KP / 8);
-        *reinterpret_cast<uint4 *>(sB + t * L::BT + (n >> 3) * SBO + j * 128 + (n & 7) * 16) =
+        *reinterpret_cast<uint4 *>(sB + t * L::BT + (n >> 3) * SBO_B + j * 128 + (n & 7) * 16) =
             __ldg(reinterpret_cast<const uint4 *>(a.w) + c);
     }
     tc::fence_async_smem();
@@ -138,119 +204,124 @@ __global__ void __launch_bounds__(kConvThreads) k_conv_fwd(ConvArgs a) {
 
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const long nvox = (long)nx * ny * nz;
-    const long ntiles = (nvox + 127) / 128;
-    uint32_t use = 0;       /* stage uses (= MMA commits) so far, equal in every thread */
+    const int ntx = (nx + 7) / 8, nty = (ny + 15) / 16, ntz = (nz + zchunk - 1) / zchunk;
+    const long items = (long)ntx * nty * ntz;
+    uint32_t uses0 = 0, uses1 = 0;        /* completions waited for, per accumulator   */
+    uint32_t commits0 = 0, commits1 = 0;  /* commits issued (by thread 0; tracked by all) */
     bool aborted = false;
-    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long v = tile * 128 + tid;
-        const bool vok = v < nvox;
-        int x = 0, y = 0, z = 0;
-        if (vok) {
-            x = (int)(v % nx);
-            const long q = v / nx;
-            y = (int)(q % ny);
-            z = (int)(q / ny);
-        }
-        uint4 r[KP / 8];
-        {
-            long src = 0;
-            const bool ok = vok && tap_src(0, v, x, y, z, nx, ny, nz, src);
-            load_row<KP>(a.x, src, ok, r);
-        }
-        for (int t = 0; t < 27; t++) {
-            const int s = use % kStages;
-            const uint32_t k_use = use / kStages;
-            if (k_use > 0 && !tc::mbar_wait(&bar[s], (k_use - 1) & 1, kWaitCycles)) s_abort = 1;
-            uint8_t *st = sA + s * L::AB;
+
+    /* 16-byte halo loads of input slice zin into registers */
+    auto fetch = [&](int x0, int y0, int zin, uint4 *r) {
 #pragma unroll
-            for (int j = 0; j < KP / 8; j++)
-                *reinterpret_cast<uint4 *>(st + (tid >> 3) * SBO + j * 128 + (tid & 7) * 16) = r[j];
-            if (t + 1 < 27) {
-                long src = 0;
-                const bool ok = vok && tap_src(t + 1, v, x, y, z, nx, ny, nz, src);
-                load_row<KP>(a.x, src, ok, r);
+        for (int u = 0; u < L::LOADS; u++) {
+            const int e = tid + u * kConvThreads;
+            r[u] = make_uint4(0u, 0u, 0u, 0u);
+            if (e < kHV * KP / 8 && zin >= 0 && zin < nz) {
+                const int j = e % (KP / 8), hv = e / (KP / 8);
+                const int gx = x0 - 1 + hv % kHX, gy = y0 - 1 + hv / kHX;
+                if (gx >= 0 && gx < nx && gy >= 0 && gy < ny)
+                    r[u] = __ldg(reinterpret_cast<const uint4 *>(
+                                     a.x + ((size_t)gx + (size_t)nx * (gy + (size_t)ny * zin)) * KP) + j);
             }
-            tc::fence_async_smem();
-            __syncthreads();
-            if (s_abort) { aborted = true; break; }
-            if (tid == 0) {
-                tc::fence_after_sync();
-                const uint32_t a0 = tc::smem_u32(st), b0 = tc::smem_u32(sB + t * L::BT);
+        }
+    };
+    auto stash = [&](uint8_t *slot, const uint4 *r) {
 #pragma unroll
-                for (int kk = 0; kk < KP / 16; kk++)
-                    tc::mma_bf16(tmem, tc::sdesc(a0 + kk * 256, 128, SBO), tc::sdesc(b0 + kk * 256, 128, SBO),
-                                 IDESC, (t | kk) != 0);
-                tc::mma_commit(&bar[s]);
+        for (int u = 0; u < L::LOADS; u++) {
+            const int e = tid + u * kConvThreads;
+            if (e < kHV * KP / 8) {
+                const int j = e % (KP / 8), hv = e / (KP / 8);
+                *reinterpret_cast<uint4 *>(slot + j * L::PLANE + hv * 16) = r[u];
             }
-            use++;
+        }
+    };
+
+    for (long item = blockIdx.x; item < items && !aborted; item += gridDim.x) {
+        const int tx = (int)(item % ntx), ty = (int)((item / ntx) % nty), tz = (int)(item / ((long)ntx * nty));
+        const int x0 = tx * 8, y0 = ty * 16, z0 = tz * zchunk;
+        const int nzs = min(zchunk, nz - z0);      /* output slices of this item */
+        const int ox = x0 + (tid & 7), oy = y0 + (tid >> 3);
+        /* input slice k (z = z0 - 1 + k) lives in ring slot k % 4; prologue: k = 0, 1 */
+        uint4 r[L::LOADS];
+        fetch(x0, y0, z0 - 1, r);
+        stash(ring + 0 * L::SLOT, r);
+        fetch(x0, y0, z0, r);
+        stash(ring + 1 * L::SLOT, r);
+        fetch(x0, y0, z0 + 1, r);                 /* slice k = 2, stored in iteration 0 */
+        for (int i = 0; i <= nzs; i++) {
+            if (i < nzs) {
+                /* slot (i+2) % 4 held slice i-2, whose last reader (output i-1... i-2)
+                 * completed: output i-2's epilogue waited for its MMAs, and output
+                 * i-1 reads slices i-1..i+1 only */
+                stash(ring + ((i + 2) % kRing) * L::SLOT, r);
+                if (i + 1 < nzs) fetch(x0, y0, z0 + i + 2, r);
+                tc::fence_async_smem();
+                tc::fence_before_sync();
+                __syncthreads();
+                if (s_abort) { aborted = true; break; }
+                if (tid == 0) {
+                    tc::fence_after_sync();
+                    const int buf = i & 1;
+                    const uint32_t d = tmem + buf * kTmemCols;
+                    /* descriptors: a base per input slice (dz), the tap's (dy, dx)
+                     * window and the K step added to the start-address field
+                     * (16-byte units; no carry: shared addresses < 256 KB) */
+                    uint64_t aS[3];
+#pragma unroll
+                    for (int dz = 0; dz < 3; dz++)
+                        aS[dz] = tc::sdesc(tc::smem_u32(ring + ((i + dz) % kRing) * L::SLOT), L::PLANE, kHX * 16);
+                    const uint64_t bS = tc::sdesc(tc::smem_u32(sB), 128, SBO_B);
+#pragma unroll
+                    for (int t = 0; t < 27; t++) {
+                        const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+                        const uint64_t at = aS[dz] + (uint64_t)(dy * kHX + dx);
+                        const uint64_t bt = bS + (uint64_t)(t * (L::BT >> 4));
+#pragma unroll
+                        for (int kk = 0; kk < KP / 16; kk++)
+                            tc::mma_bf16(d, at + (uint64_t)(kk * (2 * L::PLANE >> 4)), bt + (uint64_t)(kk * 16), IDESC,
+                                         (t | kk) != 0);
+                    }
+                    tc::mma_commit(&bar[buf]);
+                }
+                if (i & 1) commits1++;
+                else commits0++;
+            }
+            if (i >= 1) {   /* epilogue of output slice i - 1 */
+                const int buf = (i - 1) & 1;
+                const uint32_t k_use = buf ? uses1++ : uses0++;
+                /* a wait that runs out is seen by every thread at the next barrier */
+                if (!tc::mbar_wait(&bar[buf], k_use & 1, kWaitCycles)) {
+                    s_abort = 1;
+                } else {
+                    tc::fence_after_sync();
+                    float acc[NP];
+                    const uint32_t taddr = tmem + buf * kTmemCols + ((uint32_t)(warp * 32) << 16);
+                    if (NP == 16) tc::tmem_ld16(taddr, acc);
+                    else tc::tmem_ld32(taddr, acc);
+                    tc::fence_before_sync();
+                    const int oz = z0 + i - 1;
+                    if (ox < nx && oy < ny)
+                        conv_epilogue<NP, EPI>(a, (long)ox + (long)nx * (oy + (long)ny * oz), nvox, acc);
+                }
+            }
+            if (aborted) break;
         }
         if (aborted) break;
-        {
-            const uint32_t last = use - 1;
-            if (!tc::mbar_wait(&bar[last % kStages], (last / kStages) & 1, kWaitCycles)) s_abort = 1;
-        }
-        __syncthreads();
-        if (s_abort) { aborted = true; break; }
-        tc::fence_after_sync();
-        float acc[NP];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-        if (NP == 16) tc::tmem_ld16(taddr, acc);
-        else tc::tmem_ld32(taddr, acc);
-        tc::fence_before_sync();   /* the next tile's first MMA follows a barrier */
-        if (!vok) continue;
-        if (EPI == EPI_RESID) {
-#pragma unroll
-            for (int n = 0; n < NP; n++) {
-                if (n >= a.nout) break;
-                const size_t i = (size_t)n * nvox + v;
-                float val = acc[n] + (a.bias ? a.bias[n] : 0.f);
-                if (a.storage == kBF16) {
-                    val = fmaxf(ldf(reinterpret_cast<const __nv_bfloat16 *>(a.res) + i) + val * a.inv_scale,
-                                a.floor_value);
-                    stf(reinterpret_cast<__nv_bfloat16 *>(a.out) + i, val);
-                } else if (a.storage == kF16) {
-                    val = fmaxf(ldf(reinterpret_cast<const __half *>(a.res) + i) + val * a.inv_scale, a.floor_value);
-                    stf(reinterpret_cast<__half *>(a.out) + i, val);
-                } else {
-                    val = fmaxf(ldf(reinterpret_cast<const float *>(a.res) + i) + val * a.inv_scale, a.floor_value);
-                    stf(reinterpret_cast<float *>(a.out) + i, val);
-                }
-            }
-        } else {
-            uint4 *yo = reinterpret_cast<uint4 *>(a.y + (size_t)v * NP);
-            const uint4 *mk = reinterpret_cast<const uint4 *>(a.mask + (size_t)v * NP);
-#pragma unroll
-            for (int j = 0; j < NP / 8; j++) {
-                float o[8];
-#pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    const int n = 8 * j + i;
-                    o[i] = acc[n];
-                    if (EPI != EPI_MASK && a.bias) o[i] += a.bias[n];
-                    if (EPI == EPI_RELU) o[i] = fmaxf(o[i], 0.f);
-                }
-                if (EPI == EPI_MASK) {
-                    const uint4 m = mk[j];
-                    const uint32_t mw[4] = {m.x, m.y, m.z, m.w};
-#pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        if (!(bf_lo(mw[i]) > 0.f)) o[2 * i] = 0.f;
-                        if (!(bf_hi(mw[i]) > 0.f)) o[2 * i + 1] = 0.f;
-                    }
-                }
-                yo[j] = make_uint4(pack2(o[0], o[1]), pack2(o[2], o[3]), pack2(o[4], o[5]), pack2(o[6], o[7]));
-            }
-        }
     }
-    if (aborted && use > 0) {   /* MMAs still in flight read shared memory and write tensor memory */
-        const uint32_t last = use - 1;
-        tc::mbar_wait(&bar[last % kStages], (last / kStages) & 1, kWaitCycles);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (s_abort) aborted = true;
+    /* a wait that ran out leaves MMAs possibly in flight: wait (bounded) for
+     * each accumulator's last commit */
+    if (aborted) {
+        if (commits0 > 0) tc::mbar_wait(&bar[0], (commits0 - 1) & 1, kWaitCycles);
+        if (commits1 > 0) tc::mbar_wait(&bar[1], (commits1 - 1) & 1, kWaitCycles);
     }
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, kTmemCols);
+        tc::tmem_dealloc(tmem, 2 * kTmemCols);
     }
     if (aborted && tid == 0) atomicExch(a.err, 1);
 }
@@ -556,18 +627,25 @@ int sm_count() {
 }
 
 template <int KP, int NP, int EPI>
-cudaError_t launch_fwd_t(const ConvArgs &a, cudaStream_t s) {
-    const int bytes = FwdSmem<KP, NP>::bytes;
-    cudaError_t e = cudaFuncSetAttribute(k_conv_fwd<KP, NP, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+cudaError_t launch_halo_t(const ConvArgs &a, cudaStream_t s) {
+    const int bytes = HaloSmem<KP, NP>::bytes;
+    cudaError_t e = cudaFuncSetAttribute(k_conv_halo<KP, NP, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_conv_halo<KP, NP, EPI>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
-    int occ = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv_fwd<KP, NP, EPI>, kConvThreads, bytes);
-    if (e != cudaSuccess) return e;
-    occ = occ < 1 ? 1 : (occ > 4 ? 4 : occ);   /* tensor memory: 4 x 32 columns of 512 */
-    const long nvox = (long)a.nx * a.ny * a.nz;
-    const long ntiles = (nvox + 127) / 128;
-    const long grid = std::min<long>(ntiles, (long)sm_count() * occ);
-    k_conv_fwd<KP, NP, EPI><<<(int)grid, kConvThreads, bytes, s>>>(a);
+    /* CTAs per SM from shared memory (228 KB per SM, 1 KB reserved per CTA),
+     * at most 4 (tensor memory: 4 x 64 of 512 columns) */
+    int occ = 233472 / (bytes + 1024);
+    occ = occ < 1 ? 1 : (occ > 4 ? 4 : occ);
+    const long grid0 = (long)sm_count() * occ;
+    const long xy = (long)((a.nx + 7) / 8) * ((a.ny + 15) / 16);
+    /* z-chunk: long enough to amortise the two halo slices, short enough
+     * for two work items per CTA */
+    const long zc = std::max<long>(1, std::min<long>(64, ((long)a.nz * xy) / (2 * grid0)));
+    const long items = xy * ((a.nz + zc - 1) / zc);
+    const long grid = std::min<long>(items, grid0);
+    k_conv_halo<KP, NP, EPI><<<(int)grid, kConvThreads, bytes, s>>>(a, (int)zc);
     return cudaGetLastError();
 }
 
@@ -575,9 +653,9 @@ cudaError_t launch_fwd(int KP, int NP, int epi, const ConvArgs &a, cudaStream_t 
 #define XR_FWD(kp, np)                                                       \
     if (KP == kp && NP == np) {                                              \
         switch (epi) {                                                       \
-            case EPI_BIAS: return launch_fwd_t<kp, np, EPI_BIAS>(a, s);      \
-            case EPI_RELU: return launch_fwd_t<kp, np, EPI_RELU>(a, s);      \
-            case EPI_MASK: return launch_fwd_t<kp, np, EPI_MASK>(a, s);      \
+            case EPI_BIAS: return launch_halo_t<kp, np, EPI_BIAS>(a, s);     \
+            case EPI_RELU: return launch_halo_t<kp, np, EPI_RELU>(a, s);     \
+            case EPI_MASK: return launch_halo_t<kp, np, EPI_MASK>(a, s);     \
             default: break;                                                  \
         }                                                                    \
     }
@@ -587,8 +665,8 @@ cudaError_t launch_fwd(int KP, int NP, int epi, const ConvArgs &a, cudaStream_t 
     XR_FWD(32, 32)
 #undef XR_FWD
     if (epi == EPI_RESID && NP == 16) {
-        if (KP == 16) return launch_fwd_t<16, 16, EPI_RESID>(a, s);
-        if (KP == 32) return launch_fwd_t<32, 16, EPI_RESID>(a, s);
+        if (KP == 16) return launch_halo_t<16, 16, EPI_RESID>(a, s);
+        if (KP == 32) return launch_halo_t<32, 16, EPI_RESID>(a, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -597,10 +675,11 @@ template <int KP, int NP>
 cudaError_t launch_wgrad_t(WgradArgs a, cudaStream_t s) {
     const int bytes = WgSmem<KP, NP>::bytes;
     cudaError_t e = cudaFuncSetAttribute(k_conv_wgrad<KP, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_conv_wgrad<KP, NP>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
-    int occ = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv_wgrad<KP, NP>, kConvThreads, bytes);
-    if (e != cudaSuccess) return e;
+    int occ = 233472 / (bytes + 1024);
     occ = occ < 1 ? 1 : (occ > 4 ? 4 : occ);
     const int tbs = (27 + 128 / KP - 1) / (128 / KP);
     const long nvox = (long)a.nx * a.ny * a.nz;
