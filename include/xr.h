@@ -224,6 +224,24 @@ xr_status xr_dev_session_end(xr_ctx *ctx, float *d_md, float *d_evalue);
 /* The session's current ratio images (C*V*Nd^2 floats, device pointer). */
 xr_status xr_dev_session_proj(xr_ctx *ctx, const float **d_proj);
 
+/* ---- regularisers (solver/, reconstruct/src/quadfilt.cpp) --------------- */
+/* totalVariationMinimized(vol, rho, lambda, iter), solver/src/tvmin.cpp:6-98:
+ * anisotropic TV denoising by ADMM of a device volume (nx*ny*nz floats, x
+ * fastest), in place.  The linear step (I + rho F^T F) x = F^T(rho y - u) + x0
+ * is solved by conjugate gradients on the GPU to a relative residual of 1e-6
+ * (FP64 inner products) where the reference runs Eigen's BiCGSTAB to machine
+ * precision; F, the initial y = u = 1 and the updates are the reference's. */
+xr_status xr_tv_minimize(void *stream, float *d_vol, int nx, int ny, int nz, float rho, float lambda, int iter);
+/* quadlicFormFilterCPU(voxel[3], coefficient, lambda), quadfilt.cpp:11-134:
+ * d_voxel 3 planes (the orthogonal coefficients), d_coef 2 planes (phi, cos
+ * theta), both updated in place; each of the 6 tensor elements is TV-filtered
+ * with rho 3 and 20 iterations. */
+xr_status xr_quad_form_filter(void *stream, float *d_voxel, float *d_coef, int nx, int ny, int nz, float lambda);
+/* Host-buffer forms of the two (copy in, run on `device`, copy out). */
+xr_status xr_tv_minimize_host(int device, float *vol, int nx, int ny, int nz, float rho, float lambda, int iter);
+xr_status xr_quad_form_filter_host(int device, float *const *voxel, float *const *coef, int nx, int ny, int nz,
+                                   float lambda);
+
 /* ---- several specimens at once (no reference counterpart) -------------- */
 /* A batch runs the OS-EM sessions of several independent specimens (each its
  * own context: geometry, size, storage options) together: one epoch of every

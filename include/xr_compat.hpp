@@ -342,4 +342,18 @@ inline void directionNormalization(Volume<float> md[3]) {
     xr::check(xr_direction_normalization(xr::need(), m), "directionNormalization");
 }
 
+/* solver/src/tvmin.cpp:6-98, on the GPU (device 0). */
+inline void totalVariationMinimized(Volume<float> &vol, float rho, float lambda, int iter) {
+    xr::check(xr_tv_minimize_host(0, vol.get(), vol.x(), vol.y(), vol.z(), rho, lambda, iter),
+              "totalVariationMinimized");
+}
+
+/* reconstruct/src/quadfilt.cpp:11-134, on the GPU (device 0). */
+inline void quadlicFormFilterCPU(Volume<float> voxel[3], Volume<float> *coefficient, float lambda) {
+    float *v[3] = {voxel[0].get(), voxel[1].get(), voxel[2].get()};
+    float *c[2] = {coefficient[0].get(), coefficient[1].get()};
+    xr::check(xr_quad_form_filter_host(0, v, c, voxel[0].x(), voxel[0].y(), voxel[0].z(), lambda),
+              "quadlicFormFilterCPU");
+}
+
 #endif /* XR_COMPAT_HPP */

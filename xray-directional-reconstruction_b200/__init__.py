@@ -143,6 +143,14 @@ _SIGS = {
     "xr_dev_session_proj": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "xr_dev_forward_proj_only_static": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                          ctypes.c_void_p], ctypes.c_int),
+    "xr_tv_minimize": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                        ctypes.c_float, ctypes.c_int], ctypes.c_int),
+    "xr_quad_form_filter": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                             ctypes.c_int, ctypes.c_float], ctypes.c_int),
+    "xr_tv_minimize_host": ([ctypes.c_int, _F, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                             ctypes.c_float, ctypes.c_int], ctypes.c_int),
+    "xr_quad_form_filter_host": ([ctypes.c_int, ctypes.POINTER(_F), ctypes.POINTER(_F), ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_float], ctypes.c_int),
     "xr_batch_create": ([ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
                         ctypes.c_int),
     "xr_batch_destroy": ([ctypes.c_void_p], None),
@@ -582,6 +590,31 @@ def directionNormalization(md: Sequence[Volume]) -> None:
     m = ctx.direction_normalization(np.stack([v.get() for v in md[:3]]))
     for i in range(3):
         md[i].data = m[i]
+
+
+def totalVariationMinimized(vol: Volume, rho: float, lam: float, iters: int, device: int = 0) -> None:
+    """totalVariationMinimized (solver/src/tvmin.cpp:6-98), in place, on the GPU."""
+    a = _f32(vol.get()).copy()
+    Z, Y, X = a.shape
+    st = lib().xr_tv_minimize_host(int(device), a.ctypes.data_as(_F), X, Y, Z, float(rho), float(lam), int(iters))
+    if st:
+        raise XRError(st, "xr_tv_minimize_host")
+    vol.data = a
+
+
+def quadlicFormFilterCPU(voxel: Sequence[Volume], coefficient: Sequence[Volume], lam: float,
+                         device: int = 0) -> None:
+    """quadlicFormFilterCPU (reconstruct/src/quadfilt.cpp:11-134), in place, on the GPU."""
+    v = [_f32(x.get()).copy() for x in voxel[:3]]
+    c = [_f32(x.get()).copy() for x in coefficient[:2]]
+    Z, Y, X = v[0].shape
+    st = lib().xr_quad_form_filter_host(int(device), _ptrs(v), _ptrs(c), X, Y, Z, float(lam))
+    if st:
+        raise XRError(st, "xr_quad_form_filter_host")
+    for i in range(3):
+        voxel[i].data = v[i]
+    for i in range(2):
+        coefficient[i].data = c[i]
 
 
 def version() -> str:

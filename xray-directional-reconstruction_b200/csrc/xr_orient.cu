@@ -13,50 +13,11 @@
 #include <cuda_runtime.h>
 
 #include "xr_internal.h"
+#include "xr_eig3.cuh"
 #include "xr_storage.cuh"
 
 namespace xr {
 namespace {
-
-__device__ void jacobi3(double A[9], double w[3], double V[9]) {
-#pragma unroll
-    for (int i = 0; i < 9; i++) V[i] = (i % 4 == 0) ? 1.0 : 0.0;
-    for (int sweep = 0; sweep < 50; sweep++) {
-        const double off = A[1] * A[1] + A[2] * A[2] + A[5] * A[5];
-        const double dia = A[0] * A[0] + A[4] * A[4] + A[8] * A[8];
-        if (off <= 1e-300 || off <= 1e-34 * dia) break;
-#pragma unroll
-        for (int pq = 0; pq < 3; pq++) {
-            const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
-            const double apq = A[3 * p + q];
-            if (apq == 0.0) continue;
-            const double theta = (A[3 * q + q] - A[3 * p + p]) / (2.0 * apq);
-            const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-            const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                const double akp = A[3 * k + p], akq = A[3 * k + q];
-                A[3 * k + p] = c * akp - s * akq;
-                A[3 * k + q] = s * akp + c * akq;
-            }
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                const double apk = A[3 * p + k], aqk = A[3 * q + k];
-                A[3 * p + k] = c * apk - s * aqk;
-                A[3 * q + k] = s * apk + c * aqk;
-            }
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                const double vkp = V[3 * k + p], vkq = V[3 * k + q];
-                V[3 * k + p] = c * vkp - s * vkq;
-                V[3 * k + q] = s * vkp + c * vkq;
-            }
-        }
-    }
-    w[0] = A[0];
-    w[1] = A[4];
-    w[2] = A[8];
-}
 
 template <typename TS>
 __global__ void k_orientation(long nvox, int K, const BasisConst *B, const TS *mu, float *md, float *ev) {
