@@ -102,6 +102,20 @@ class Oracle:
         self._fn("forward_view", dt)(ctypes.byref(self._scan(s)), cond, n, _p(vol, dt), _p(proj, dt),
                                      _p(factor, dt), int(xtt))
 
+    def forward_orth_view(self, s, cond, n, vol, coef, proj, dt=np.float32):
+        """forwardOrth (ir.cu:294-364) of one view into proj (axis block, all views)."""
+        self._fn("forward_orth_view", dt)(ctypes.byref(self._scan(s)), cond, n, _p(vol, dt), _p(coef, dt),
+                                          _p(proj, dt))
+
+    def backward_orth_slab(self, s, cond, y, n, proj, coef, tmp, factor, dt=np.float32):
+        """backwardOrth (ir.cu:366-423) of slab y, view n."""
+        self._fn("backward_orth_slab", dt)(ctypes.byref(self._scan(s)), cond, y, n, _p(proj, dt), _p(coef, dt),
+                                           _p(tmp, dt), _p(factor, dt))
+
+    def normal_three(self, s, vol, coef, loss, rot, dt=np.float32):
+        """calcNormalVectorThreeDirec (ir.cu:856-974): coef and loss updated in place."""
+        self._fn("normal_three", dt)(ctypes.byref(self._scan(s)), _p(vol, dt), _p(coef, dt), _p(loss, dt), int(rot))
+
     def correlation(self, s, cond, n, proj, factor, dt=np.float32):
         self._fn("correlation", dt)(ctypes.byref(self._scan(s)), cond, n, _p(proj, dt), _p(factor, dt))
 
@@ -220,6 +234,15 @@ class RefHost:
 
     def correlation(self, cond, n, proj, factor):
         self.lib.xr_ref_correlation(cond, n, _p(proj), _p(factor))
+
+    def forward_orth(self, cond, n, vol, coef, proj):
+        self.lib.xr_ref_forward_orth(cond, n, _p(vol), _p(coef), _p(proj))
+
+    def backward_orth(self, cond, y, n, proj, coef, tmp, factor):
+        self.lib.xr_ref_backward_orth(cond, y, n, _p(proj), _p(coef), _p(tmp), _p(factor))
+
+    def normal_three(self, vol, coef, loss, rot):
+        self.lib.xr_ref_normal_three(_p(vol), _p(coef), _p(loss), int(rot))
 
     def ratio(self, n, proj, sino, art):
         return float(self.lib.xr_ref_ratio(n, _p(proj), _p(sino), int(art)))

@@ -113,6 +113,25 @@ void xr_ref_forward_view(int cond, int n, float *vol, float *proj, float *factor
     }
 }
 
+/* forwardOrth (ir.cu:294-364): one view, every y slab, basis rotated per voxel
+ * by the coefficient planes (phi, cos theta); no weight image. */
+void xr_ref_forward_orth(int cond, int n, float *vol, const float *coef, float *proj) {
+    Geometry *geom = &g.geom;
+    for (int y = 0; y < geom->voxel; y++)
+        launch2d(g.gridV, g.blockV, forwardOrth, proj, (const float *)vol, coef, cond, y, n, 0, geom);
+}
+
+/* backwardOrth (ir.cu:366-423): slab y, view n; tmp / factor K planes of N*N. */
+void xr_ref_backward_orth(int cond, int y, int n, const float *proj, const float *coef, float *tmp, float *factor) {
+    launch2d(g.gridV, g.blockV, backwardOrth, proj, coef, tmp, factor, (const Geometry *)&g.geom, cond, y, n, 0);
+}
+
+/* calcNormalVectorThreeDirec (ir.cu:856-974), every y slab. */
+void xr_ref_normal_three(float *vol, float *coef, float *loss, int rot) {
+    for (int y = 0; y < g.geom.voxel; y++)
+        launch2d(g.gridV, g.blockV, calcNormalVectorThreeDirec, vol, coef, y, (const Geometry *)&g.geom, loss, rot);
+}
+
 void xr_ref_correlation(int cond, int n, float *proj, const float *factor) {
     launch2d(g.gridD, g.blockD, correlationProjByLength, proj, factor, &g.geom, cond, n);
 }

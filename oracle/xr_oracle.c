@@ -19,6 +19,11 @@
 #define OR_CAT2(a, b) a##b
 #define OR_CAT(a, b) OR_CAT2(a, b)
 
+/* The reference's atan2(float, float) in host code resolves to the double
+ * function (its <cmath> float overloads are not brought in for atan2), so
+ * the FP32 restatement rounds the double result. */
+static float or_atan2f(float y, float x) { return (float)atan2((double)y, (double)x); }
+
 /* ---- FP32 instantiation ---- */
 #define real float
 #define OR_PFX or32_
@@ -28,6 +33,7 @@
 #define RSQRT sqrtf
 #define RFLOOR floorf
 #define RFABS fabsf
+#define RATAN2 or_atan2f
 #include "xr_oracle_impl.h"
 #undef real
 #undef OR_PFX
@@ -37,6 +43,7 @@
 #undef RSQRT
 #undef RFLOOR
 #undef RFABS
+#undef RATAN2
 
 /* ---- FP64 instantiation ---- */
 #define real double
@@ -47,6 +54,7 @@
 #define RSQRT sqrt
 #define RFLOOR floor
 #define RFABS fabs
+#define RATAN2 atan2
 #include "xr_oracle_impl.h"
 
 /* Cyclic Jacobi eigen-decomposition of a symmetric 3x3 matrix (FP64),

@@ -133,6 +133,30 @@ static real RV(xtt_weight)(const real *B, const real *S, const real *G) {
     return vkm * vkm;
 }
 
+/* rodriguesRotation, ir.cu:597-623: rotation about (x, y, z) normalised by
+ * the angle with the given cosine / sine (identity below |n| < 1e-8), as
+ * (1 - cos) n n^T + [cos, -nz sin, ny sin; nz sin, cos, -nx sin; -ny sin, nx sin, cos]. */
+static void RV(rodrigues)(real x, real y, real z, real c, real sn, real *R) {
+    if (RSQRT(x * x + y * y + z * z) < (real)1e-8f) {
+        for (int i = 0; i < 9; i++) R[i] = (i % 4 == 0) ? (real)1 : (real)0;
+        return;
+    }
+    const real nx = x / RSQRT(x * x + y * y + z * z);
+    const real ny = y / RSQRT(x * x + y * y + z * z);
+    const real nz = z / RSQRT(x * x + y * y + z * z);
+    const real r1[9] = {nx * nx, nx * ny, nx * nz, nx * ny, ny * ny, ny * nz, nx * nz, ny * nz, nz * nz};
+    const real r2[9] = {c, -nz * sn, ny * sn, nz * sn, c, -nx * sn, -ny * sn, nx * sn, c};
+    for (int i = 0; i < 9; i++) R[i] = ((real)1 - c) * r1[i] + r2[i];
+}
+
+/* The per-voxel rotation of the orientation-parametrised projectors
+ * (ir.cu:319-331, :390-395): coef planes (phi, cos theta) ->
+ * rodrigues(cos phi, sin phi, 0, cos theta, sqrt(1 - cos^2 theta)). */
+static void RV(orth_rotation)(const real *coef, long N3, long idx, real *R) {
+    const real phi = coef[idx], ct = coef[N3 + idx];
+    RV(rodrigues)(RCOS(phi), RSIN(phi), (real)0, ct, RSQRT((real)1 - ct * ct), R);
+}
+
 /* forwardProj/forwardonDevice (ir.cu:1480-1531, xtt == 0) or
  * forwardProjXTT/forwardXTTonDevice (ir.cu:133-141,1753-1804, xtt != 0) for
  * one view over every y slab, in the reference's launch order (y, then z, then
@@ -178,6 +202,43 @@ void RV(forward_view)(const or_scan *s, int cond, int n, const real *vol, real *
                 factor[(iu + 1) + Nd * (iv + 1)] += c[1];
                 factor[(iu + 1) + Nd * iv] += c[2];
                 factor[iu + Nd * iv] += c[3];
+            }
+}
+
+/* forwardOrth, ir.cu:294-364: the XTT forward of one view with every voxel's
+ * basis rotated by its coefficient planes (S <- R S), no weight image. */
+void RV(forward_orth_view)(const or_scan *s, int cond, int n, const real *vol, const real *coef, real *proj) {
+    RV(frame) f;
+    RV(view_frame)(s, cond, n, 0, &f);
+    const long N = s->N, Nd = s->Nd, N3 = N * N * N;
+    const long nn = n < 0 ? -n : n;
+    const real vs = RV(vox_size)(s);
+    const real ratio = (vs * vs) / ((real)s->det * ((real)s->sod / (real)s->sdd) * (real)s->det *
+                                    ((real)s->sod / (real)s->sdd));
+    real G[3];
+    { const real bz[3] = {(real)0, (real)0, (real)1}; RV(mat3vec)(f.R, bz, G); }
+    for (long y = 0; y < N; y++)
+        for (long z = 0; z < N; z++)
+            for (long x = 0; x < N; x++) {
+                real u, v, B[3], c[4], R[9];
+                long iu, iv;
+                RV(raycast)(s, &f, 0, (int)x, (int)y, (int)z, &u, &v, B, 0);
+                if (!RV(taps)(s, u, v, &iu, &iv, c)) continue;
+                const long idx = x + N * y + N * N * z;
+                RV(orth_rotation)(coef, N3, idx, R);
+                real pr = (real)0;
+                for (int k = 0; k < s->K; k++) {
+                    const real S0[3] = {(real)s->basis[3 * k], (real)s->basis[3 * k + 1], (real)s->basis[3 * k + 2]};
+                    real S[3];
+                    RV(mat3vec)(R, S0, S);
+                    const real w = RV(xtt_weight)(B, S, G);
+                    pr += w * vs * ratio * vol[idx + (long)k * N3];
+                }
+                const long base = Nd * Nd * nn;
+                proj[iu + Nd * (iv + 1) + base] += c[0] * pr;
+                proj[(iu + 1) + Nd * (iv + 1) + base] += c[1] * pr;
+                proj[(iu + 1) + Nd * iv + base] += c[2] * pr;
+                proj[iu + Nd * iv + base] += c[3] * pr;
             }
 }
 
@@ -285,6 +346,90 @@ void RV(backward_slab)(const or_scan *s, int cond, int y, int n, const real *pro
                 }
             }
         }
+}
+
+/* backwardOrth, ir.cu:366-423: backward_slab's XTT form with the rotated basis. */
+void RV(backward_orth_slab)(const or_scan *s, int cond, int y, int n, const real *proj, const real *coef,
+                            real *tmp, real *factor) {
+    RV(frame) f;
+    RV(view_frame)(s, cond, n, 0, &f);
+    const long N = s->N, Nd = s->Nd, N3 = N * N * N;
+    const long nn = n < 0 ? -n : n;
+    real G[3];
+    { const real bz[3] = {(real)0, (real)0, (real)1}; RV(mat3vec)(f.R, bz, G); }
+    for (long z = 0; z < N; z++)
+        for (long x = 0; x < N; x++) {
+            real u, v, B[3], c[4], R[9];
+            long iu, iv;
+            RV(raycast)(s, &f, 0, (int)x, y, (int)z, &u, &v, B, 0);
+            if (!RV(taps)(s, u, v, &iu, &iv, c)) continue;
+            RV(orth_rotation)(coef, N3, x + N * y + N * N * z, R);
+            const long base = Nd * Nd * nn;
+            const real p0 = proj[iu + Nd * (iv + 1) + base], p1 = proj[(iu + 1) + Nd * (iv + 1) + base];
+            const real p2 = proj[(iu + 1) + Nd * iv + base], p3 = proj[iu + Nd * iv + base];
+            const long idx = x + N * z;
+            for (int k = 0; k < s->K; k++) {
+                const real S0[3] = {(real)s->basis[3 * k], (real)s->basis[3 * k + 1], (real)s->basis[3 * k + 2]};
+                real S[3];
+                RV(mat3vec)(R, S0, S);
+                const real w = RV(xtt_weight)(B, S, G);
+                const real bf = w * c[0] * p0 + w * c[1] * p1 + w * c[2] * p2 + w * c[3] * p3;
+                factor[idx + (long)k * N * N] += w;
+                tmp[idx + (long)k * N * N] += bf;
+            }
+        }
+}
+
+/* Vector3X::normalize (vec.h:94-106): divide by the norm above 1e-8, else zero. */
+static void RV(normalize3)(real *v) {
+    const real l = RSQRT(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (l > (real)1e-8f) {
+        v[0] /= l; v[1] /= l; v[2] /= l;
+    } else {
+        v[0] = v[1] = v[2] = (real)0;
+    }
+}
+
+/* calcNormalVectorThreeDirec, ir.cu:856-974: from the three orthogonal
+ * coefficients mu (planes 0..2) and the sign pattern rot, the plane normal
+ * (mu0 S0 - mu1' S1) x (mu0 S0 - mu2' S2), rotated by the voxel's current R,
+ * z >= 0, gives the new (phi, cos theta); loss = |(R e_z) x norm|. */
+void RV(normal_three)(const or_scan *s, const real *vol, real *coef, real *loss, int rot) {
+    const long N3 = (long)s->N * s->N * s->N;
+    for (long i = 0; i < N3; i++) {
+        real R[9];
+        RV(orth_rotation)(coef, N3, i, R);
+        const real mu0 = vol[i], m1 = vol[N3 + i], m2 = vol[2 * N3 + i];
+        real mu1 = m1, mu2 = m2;
+        if (rot == 1) { mu1 = -m1; mu2 = m2; }
+        else if (rot == 2) { mu1 = -m1; mu2 = -m2; }
+        else if (rot == 3) { mu1 = m1; mu2 = -m2; }
+        const float *b = s->basis;
+        real v1[3], v2[3], nrm[3];
+        for (int j = 0; j < 3; j++) {
+            v1[j] = mu0 * (real)b[j] - mu1 * (real)b[3 + j];
+            v2[j] = mu0 * (real)b[j] - mu2 * (real)b[6 + j];
+        }
+        nrm[0] = v1[1] * v2[2] - v1[2] * v2[1];
+        nrm[1] = v1[2] * v2[0] - v1[0] * v2[2];
+        nrm[2] = v1[0] * v2[1] - v1[1] * v2[0];
+        RV(normalize3)(nrm);
+        real rn[3];
+        RV(mat3vec)(R, nrm, rn);
+        /* norm + 0 * base */
+        for (int j = 0; j < 3; j++) rn[j] = rn[j] + (real)0 * (j == 2 ? (real)1 : (real)0);
+        if (rn[2] < (real)0) { rn[0] = -rn[0]; rn[1] = -rn[1]; rn[2] = -rn[2]; }
+        RV(normalize3)(rn);
+        real be[3];
+        { const real bz[3] = {(real)0, (real)0, (real)1}; RV(mat3vec)(R, bz, be); }
+        const real dx = be[1] * rn[2] - be[2] * rn[1], dy = be[2] * rn[0] - be[0] * rn[2],
+                   dz = be[0] * rn[1] - be[1] * rn[0];
+        /* rotAxis = base x norm */
+        const real ax = (real)0 * rn[2] - (real)1 * rn[1], ay = (real)1 * rn[0] - (real)0 * rn[2];
+        loss[i] = RSQRT(dx * dx + dy * dy + dz * dz);
+        coef[i] = RATAN2(ay, ax);
+        coef[N3 + i] = (real)0 * rn[0] + (real)0 * rn[1] + (real)1 * rn[2];
+    }
 }
 
 /* voxelProduct (ir.cu:1637-1654, MLEM) or voxelPlus (ir.cu:1682-1693, ART)
