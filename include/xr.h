@@ -224,6 +224,26 @@ xr_status xr_dev_session_end(xr_ctx *ctx, float *d_md, float *d_evalue);
 /* The session's current ratio images (C*V*Nd^2 floats, device pointer). */
 xr_status xr_dev_session_proj(xr_ctx *ctx, const float **d_proj);
 
+/* ---- orientation-parametrised XTT (ir.cu:294-423, :856-974) ------------- */
+/* The XTT operators with every voxel's scattering basis rotated by its own
+ * Rodrigues rotation rodriguesRotation(cos phi, sin phi, 0, cos theta,
+ * sin theta) (ir.cu:597-623); d_coef holds the phi plane then the cos theta
+ * plane (2 * N^3 floats, FP32).  The forward is the reference's forwardOrth
+ * (ir.cu:294-364): no chord-length normalisation. */
+xr_status xr_dev_forward_orth(xr_ctx *ctx, const void *d_vol, const float *d_coef, float *d_sino, xr_rotate dir);
+/* An XTT session (xr_dev_session_epoch / _end as usual) whose forward,
+ * ratio and back-projection are forwardOrth -> projRatio -> backwardOrth with
+ * voxelProduct / voxelPlus, the loop of orthTwiceReconstruct's inner epochs
+ * (reconstruct.cu:1067-1127); the planes stay fixed during the session.  The
+ * subset order is the XTT session's (a default std::mt19937_64 each epoch),
+ * where the reference seeds its engine from std::random_device. */
+xr_status xr_dev_session_begin_orth(xr_ctx *ctx, const void *d_sino, void *d_vol, const float *d_coef, int epochs,
+                                    int batch, xr_rotate dir, xr_method method, float lambda);
+/* calcNormalVectorThreeDirec (ir.cu:856-974) on every voxel: d_vol holds the
+ * three coefficients (FP32, K >= 3, basis vectors 0..2), d_coef is updated in
+ * place, d_loss (N^3) receives |(R e_z) x n|; rot in 0..3 picks the signs. */
+xr_status xr_orth_normal_update(xr_ctx *ctx, const float *d_vol, float *d_coef, float *d_loss, int rot);
+
 /* ---- regularisers (solver/, reconstruct/src/quadfilt.cpp) --------------- */
 /* totalVariationMinimized(vol, rho, lambda, iter), solver/src/tvmin.cpp:6-98:
  * anisotropic TV denoising by ADMM of a device volume (nx*ny*nz floats, x

@@ -26,6 +26,12 @@ def basis13() -> np.ndarray:
     return np.array([np.asarray(v, np.float64) / np.linalg.norm(v) for v in d], np.float32)
 
 
+def oblique_rot(seed: int, n: int) -> np.ndarray:
+    """n rotation matrices in general position (not grid-aligned), rows of 9."""
+    rng = np.random.default_rng(seed)
+    return np.array([_rot_from(rng).ravel() for _ in range(n)], np.float32)
+
+
 def _rot_from(rng) -> np.ndarray:
     q = rng.normal(size=4)
     q /= np.linalg.norm(q)

@@ -143,6 +143,12 @@ _SIGS = {
     "xr_dev_session_proj": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "xr_dev_forward_proj_only_static": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                          ctypes.c_void_p], ctypes.c_int),
+    "xr_dev_forward_orth": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int],
+                            ctypes.c_int),
+    "xr_dev_session_begin_orth": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float], ctypes.c_int),
+    "xr_orth_normal_update": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int],
+                              ctypes.c_int),
     "xr_tv_minimize": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                         ctypes.c_float, ctypes.c_int], ctypes.c_int),
     "xr_quad_form_filter": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
@@ -461,6 +467,23 @@ class Context:
         self._check(lib().xr_dev_session_begin(self._h, ctypes.c_void_p(d_sino), ctypes.c_void_p(d_vol),
                                                int(bool(xtt)), int(epochs), int(batch), int(rotate), int(method),
                                                float(lam)))
+
+    def dev_forward_orth(self, d_vol: int, d_coef: int, d_sino: int, rotate=Rotate.CW):
+        """forwardOrth over every axis and view (ir.cu:294-364), device buffers."""
+        self._check(lib().xr_dev_forward_orth(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_coef),
+                                              ctypes.c_void_p(d_sino), int(rotate)))
+
+    def dev_session_begin_orth(self, d_sino: int, d_vol: int, d_coef: int, epochs: int, batch: int,
+                               rotate=Rotate.CW, method=Method.MLEM, lam=1e-2):
+        """Orientation-parametrised XTT session (forwardOrth / backwardOrth)."""
+        self._check(lib().xr_dev_session_begin_orth(self._h, ctypes.c_void_p(d_sino), ctypes.c_void_p(d_vol),
+                                                    ctypes.c_void_p(d_coef), int(epochs), int(batch), int(rotate),
+                                                    int(method), float(lam)))
+
+    def orth_normal_update(self, d_vol: int, d_coef: int, d_loss: int, rot: int = 0):
+        """calcNormalVectorThreeDirec (ir.cu:856-974) on device buffers."""
+        self._check(lib().xr_orth_normal_update(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_coef),
+                                                ctypes.c_void_p(d_loss), int(rot)))
 
     def dev_session_epoch(self, want_loss: bool = False):
         if not want_loss:

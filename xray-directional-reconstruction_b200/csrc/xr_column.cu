@@ -26,6 +26,7 @@
 #include "xr_internal.h"
 #include "xr_storage.cuh"
 #include "xr_tile.cuh"
+#include "xr_orth.cuh"
 
 namespace xr {
 namespace {
@@ -119,6 +120,7 @@ struct FwdColArgs {
     const void *vol;          /* storage type T                              */
     float *out;
     const BasisConst *basis;
+    const float *coef;        /* mode 3: per-voxel rotation planes (phi, cos) */
     int nbg, nba;             /* bricks along g and a                        */
 };
 
@@ -211,6 +213,8 @@ __global__ void __launch_bounds__(kFwdThreads, 3) k_fwd_col(FwdColArgs a) {
             val[q] = ldgf<T>(vol + idx);
         } else if (MODE == 2) {
             val[q] = 1.0f;
+        } else if (MODE == 3) {   /* XTT with the voxel's rotated basis (forwardOrth, ir.cu:294-364) */
+            orth_moments<T>(a.basis, cond, g.K, __fmul_rn(g.vs, g.ratio), vol, a.coef, idx, N3, val[q], m[q]);
         } else {
             const BasisConst *Bc = a.basis;
             const float sc = __fmul_rn(g.vs, g.ratio);
@@ -239,7 +243,7 @@ __global__ void __launch_bounds__(kFwdThreads, 3) k_fwd_col(FwdColArgs a) {
     for (int q = 0; q < 4; q++) {
         if (!okv[q]) continue;
         float bq = (MODE == 0) ? fabsf(val[q]) * g.ratio : (MODE == 2 ? 1.0f : fabsf(val[q]));
-        if (MODE == 1)
+        if (MODE == 1 || MODE == 3)
 #pragma unroll
             for (int e = 0; e < 6; e++) bq += fabsf(m[q][e]);
         bound = fmaxf(bound, bq * 1.001f);
@@ -360,6 +364,7 @@ struct BackColArgs {
     int art;
     float alpha;
     int sr;                   /* 16-bit volumes: stochastic rounding of updates */
+    const float *coef;        /* non-null: per-voxel rotated basis (backwardOrth) */
 };
 
 /* One view of one axis for a thread's column segment of 4 voxels: the ray
@@ -490,6 +495,24 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
             xyz_of<G>(ca, cb, sg * 4 + q, lx, ly, lz);
             const int lv = lx + 8 * ly + 64 * lz;
             const BasisConst *Bc = a.basis;
+            if (a.coef) {   /* backwardOrth (ir.cu:366-423): the voxel's rotated basis */
+                int x, y, z;
+                xyz_of<G>(ia, ib, igb + q, x, y, z);
+                float R[9];
+                orth_rotation(a.coef, NN * N, (size_t)x + (size_t)N * y + NN * z, R);
+                const float G0 = Bc->G[3 * cond], G1 = Bc->G[3 * cond + 1], G2 = Bc->G[3 * cond + 2];
+                for (int k = 0; k < K; k++) {
+                    float S[3];
+                    orth_basis(Bc, k, R, S);
+                    const float h = S[0] * G0 + S[1] * G1 + S[2] * G2;
+                    const float sAs = S[0] * S[0] * acc[q][0] + S[1] * S[1] * acc[q][1] + S[2] * S[2] * acc[q][2] +
+                                      2.f * (S[0] * S[1] * acc[q][3] + S[0] * S[2] * acc[q][4] +
+                                             S[1] * S[2] * acc[q][5]);
+                    sacc[k * 512 + lv] +=
+                        (h * h) * fmaf(S[0] * S[0] + S[1] * S[1] + S[2] * S[2], acc[q][6], -sAs);
+                }
+                continue;
+            }
             for (int k = 0; k < K; k++) {
                 const float gk = Bc->g[cond * K + k];
                 if (gk == 0.f) continue;
@@ -581,8 +604,9 @@ cudaError_t check_exact_rdet(float det, float rdet, unsigned *d_flag, unsigned *
 cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, const int *d_conds, int n_cond, int G,
                                const float *d_magsig, const void *vol, float *out, int mode, int views_per_cta,
-                               int storage, cudaStream_t s) {
+                               int storage, cudaStream_t s, const float *coef) {
     if (n_views <= 0 || n_cond <= 0) return cudaSuccess;
+    if (coef && mode == 1) mode = 3;
     FwdColArgs a;
     a.g = g;
     a.frames = frames;
@@ -593,6 +617,7 @@ cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, co
     a.vol = vol;
     a.out = out;
     a.basis = d_basis;
+    a.coef = coef;
     a.nbg = (g.N + 15) / 16;
     a.nba = (g.N + 7) / 8;
     const int nbb = (g.N + 7) / 8;
@@ -622,11 +647,17 @@ cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, co
     if (mode == 2) {
         XR_FWD_COL_G(2, float);
     } else if (storage == kBF16) {
-        if (mode == 0) XR_FWD_COL_G(0, __nv_bfloat16); else XR_FWD_COL_G(1, __nv_bfloat16);
+        if (mode == 0) XR_FWD_COL_G(0, __nv_bfloat16);
+        else if (mode == 3) XR_FWD_COL_G(3, __nv_bfloat16);
+        else XR_FWD_COL_G(1, __nv_bfloat16);
     } else if (storage == kF16) {
-        if (mode == 0) XR_FWD_COL_G(0, __half); else XR_FWD_COL_G(1, __half);
+        if (mode == 0) XR_FWD_COL_G(0, __half);
+        else if (mode == 3) XR_FWD_COL_G(3, __half);
+        else XR_FWD_COL_G(1, __half);
     } else {
-        if (mode == 0) XR_FWD_COL_G(0, float); else XR_FWD_COL_G(1, float);
+        if (mode == 0) XR_FWD_COL_G(0, float);
+        else if (mode == 3) XR_FWD_COL_G(3, float);
+        else XR_FWD_COL_G(1, float);
     }
 #undef XR_FWD_COL_G
 #undef XR_FWD_COL
@@ -636,8 +667,9 @@ cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, co
 cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                             const int *view_list, int n_views, const int *d_conds, int n_cond, const int *d_axis_g,
                             const float *d_magsig, const float *proj, void *vol, const float *fac_in, float *fac_out,
-                            int mode, int art, float alpha, int storage, cudaStream_t s) {
+                            int mode, int art, float alpha, int storage, cudaStream_t s, const float *coef) {
     BackColArgs a;
+    a.coef = coef;
     a.sr = (storage & kStoreStochastic) != 0;
     storage &= ~kStoreStochastic;
     a.g = g;

@@ -191,6 +191,7 @@ static void fill_consts(xr_ctx *c) {
         /* G = Rotate * e_z = elemR[cond] * e_z for every view (Rz fixes e_z);
          * |S . G| as ir.cu:1786, squared. */
         const ViewFrame f = make_frame(c, cond, 0, false);
+        for (int j = 0; j < 3; j++) b.G[3 * cond + j] = f.ev[j];
         for (int k = 0; k < c->K; k++) {
             const float h = std::fabs(b.S[3 * k] * f.ev[0] + b.S[3 * k + 1] * f.ev[1] + b.S[3 * k + 2] * f.ev[2]);
             b.g[cond * c->K + k] = h * h;
@@ -282,7 +283,8 @@ static const ColInfo *dcol(xr_ctx *c) { return (const ColInfo *)c->colinfo.p; }
  * column-aligned axes (grouped by column axis), the general kernel else.
  * vol is the channel base (plain: the axis's own volume when one axis). */
 static cudaError_t forward_dispatch(xr_ctx *c, const int *vl, int n_views, const std::vector<int> &conds,
-                                    const void *vol, float *out, int mode, int storage) {
+                                    const void *vol, float *out, int mode, int storage,
+                                    const float *coef = nullptr) {
     const ViewFrame *fr = (const ViewFrame *)c->frames.p;
     const ColInfo *ci = dcol(c);
     std::vector<int> grp[3];
@@ -290,7 +292,7 @@ static cudaError_t forward_dispatch(xr_ctx *c, const int *vl, int n_views, const
         const int g = c->axis_g[cond];
         if (g < 0) {
             cudaError_t e = launch_forward(c->gc, dbasis(c), fr, vl, n_views, cond, 1, vol, out, mode,
-                                           c->views_per_cta, storage, c->stream);
+                                           c->views_per_cta, storage, c->stream, coef);
             if (e != cudaSuccess) return e;
         } else {
             grp[g].push_back(cond);
@@ -308,14 +310,14 @@ static cudaError_t forward_dispatch(xr_ctx *c, const int *vl, int n_views, const
                 for (int cond : grp[g]) {
                     cudaError_t e = launch_forward_col(c->gc, dbasis(c), fr, vl, n_views, &ci->all[cond], 1, g,
                                                        ci->magsig, vol, out, mode, c->views_per_cta, storage,
-                                                       c->stream);
+                                                       c->stream, coef);
                     if (e != cudaSuccess) return e;
                 }
                 continue;
             }
         }
         cudaError_t e = launch_forward_col(c->gc, dbasis(c), fr, vl, n_views, dl, (int)grp[g].size(), g, ci->magsig,
-                                           vol, out, mode, c->views_per_cta, storage, c->stream);
+                                           vol, out, mode, c->views_per_cta, storage, c->stream, coef);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -453,13 +455,15 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
             {
                 Timed t(c, XR_T_FORWARD);
                 if ((st = cuda_check(c, forward_dispatch(c, vl, s.subset_size, all_conds(c), s.d_vol, proj, 1,
-                                                         s.storage), "XTT forward")))
+                                                         s.storage, s.coef), "XTT forward")))
                     return st;
             }
             {
                 Timed t(c, XR_T_RATIO);
-                if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, norm, s.d_sino, s.art,
-                                                     dl, s.sino_storage, str), "ratio")))
+                /* the orientation-parametrised forward is not chord-normalised
+                 * (forwardOrth -> projRatio, reconstruct.cu:1086-1099) */
+                if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, s.coef ? nullptr : norm,
+                                                     s.d_sino, s.art, dl, s.sino_storage, str), "ratio")))
                     return st;
             }
             {
@@ -471,10 +475,10 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                         s.art ? nullptr : (const float *)c->sens.p + (size_t)orders[b] * c->K * N3;
                     e = launch_back_col(c->gc, dbasis(c), fr, vl, s.subset_size, ci->all, c->C, ci->axis_g,
                                         ci->magsig, proj, s.d_vol, sens, nullptr, 1, s.art, alpha, s.update_storage,
-                                        str);
+                                        str, s.coef);
                 } else {
                     e = launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, 0, c->C, proj, s.d_vol, 1, s.art,
-                                           alpha, s.update_storage, str);
+                                           alpha, s.update_storage, str, s.coef);
                 }
                 if ((st = cuda_check(c, e, "XTT back"))) return st;
             }
@@ -815,8 +819,8 @@ xr_status xr_reset_timings(xr_ctx *c) {
 
 /* ------------------------------------------------------------- sessions */
 
-xr_status xr_dev_session_begin(xr_ctx *c, const void *d_sino, void *d_vol, int xtt, int epochs, int batch,
-                               xr_rotate dir, xr_method method, float lambda) {
+static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, int xtt, int epochs, int batch,
+                                    xr_rotate dir, xr_method method, float lambda, const float *coef) {
     if (!c || !d_sino || !d_vol) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
     if (batch < 1 || batch > c->V) return fail(c, XR_ERR_ARG, "batch must be in [1, num_proj]");
     if (method != XR_METHOD_MLEM && method != XR_METHOD_ART && method != XR_METHOD_XTT)
@@ -843,6 +847,7 @@ xr_status xr_dev_session_begin(xr_ctx *c, const void *d_sino, void *d_vol, int x
     s.storage = c->storage;
     s.sino_storage = sino_st(c);
     s.update_storage = s.storage | ((c->stochastic && s.storage != 0) ? kStoreStochastic : 0);
+    s.coef = coef;
     std::vector<int> lists((size_t)batch * s.subset_size);
     for (int sub = 0; sub < batch; sub++)
         for (int j = 0; j < s.subset_size; j++)   /* n = (sub + batch*j) % nProj, reconstruct.cu:89 */
@@ -877,7 +882,8 @@ xr_status xr_dev_session_begin(xr_ctx *c, const void *d_sino, void *d_vol, int x
             st = cuda_check(c, launch_back_col(c->gc, dbasis(c), (const ViewFrame *)c->frames.p,
                                                (const int *)c->subsets.p + (size_t)sub * s.subset_size, s.subset_size,
                                                ci->all, c->C, ci->axis_g, ci->magsig, nullptr, nullptr, nullptr,
-                                               (float *)c->sens.p + (size_t)sub * c->K * N3, 2, 0, 0.f, 0, c->stream),
+                                               (float *)c->sens.p + (size_t)sub * c->K * N3, 2, 0, 0.f, 0, c->stream,
+                                               coef),
                             "sensitivity");
             if (st) return st;
         }
@@ -886,6 +892,17 @@ xr_status xr_dev_session_begin(xr_ctx *c, const void *d_sino, void *d_vol, int x
     if (st) return st;
     s.active = true;
     return XR_OK;
+}
+
+xr_status xr_dev_session_begin(xr_ctx *c, const void *d_sino, void *d_vol, int xtt, int epochs, int batch,
+                               xr_rotate dir, xr_method method, float lambda) {
+    return session_begin_impl(c, d_sino, d_vol, xtt, epochs, batch, dir, method, lambda, nullptr);
+}
+
+xr_status xr_dev_session_begin_orth(xr_ctx *c, const void *d_sino, void *d_vol, const float *d_coef, int epochs,
+                                    int batch, xr_rotate dir, xr_method method, float lambda) {
+    if (!c || !d_coef) return c ? fail(c, XR_ERR_ARG, "null coefficient planes") : XR_ERR_ARG;
+    return session_begin_impl(c, d_sino, d_vol, 1, epochs, batch, dir, method, lambda, d_coef);
 }
 
 xr_status xr_dev_session_epoch(xr_ctx *c, double *loss) {
@@ -960,7 +977,7 @@ xr_status xr_dev_session_proj(xr_ctx *c, const float **d_proj) {
 /* ---------------------------------------------------- device-buffer calls */
 
 static xr_status forward_into(xr_ctx *c, const void *d_vol, float *d_out, int rotation, int mode, bool normalise,
-                              int storage) {
+                              int storage, const float *coef = nullptr) {
     xr_status st;
     if ((st = ensure_frames(c, rotation))) return st;
     const size_t npx = (size_t)c->C * c->V * c->Nd * c->Nd;
@@ -972,7 +989,8 @@ static xr_status forward_into(xr_ctx *c, const void *d_vol, float *d_out, int ro
     cudaMemsetAsync(d_out, 0, npx * sizeof(float), c->stream);
     {
         Timed t(c, XR_T_FORWARD);
-        st = cuda_check(c, forward_dispatch(c, (const int *)lst.p, c->V, all_conds(c), d_vol, d_out, mode, storage),
+        st = cuda_check(c, forward_dispatch(c, (const int *)lst.p, c->V, all_conds(c), d_vol, d_out, mode, storage,
+                                            coef),
                         "forward");
     }
     if (!st && normalise) {
@@ -981,6 +999,25 @@ static xr_status forward_into(xr_ctx *c, const void *d_vol, float *d_out, int ro
     }
     cudaStreamSynchronize(c->stream);
     release(lst);
+    return st;
+}
+
+xr_status xr_dev_forward_orth(xr_ctx *c, const void *d_vol, const float *d_coef, float *d_sino, xr_rotate dir) {
+    if (!c || !d_vol || !d_coef || !d_sino) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = check_xtt_k(c))) return st;
+    if ((st = ensure_device(c))) return st;
+    return forward_into(c, d_vol, d_sino, dir == XR_ROTATE_CCW ? -1 : 1, 1, false, c->storage, d_coef);
+}
+
+xr_status xr_orth_normal_update(xr_ctx *c, const float *d_vol, float *d_coef, float *d_loss, int rot) {
+    if (!c || !d_vol || !d_coef || !d_loss) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    if (c->K < 3) return fail(c, XR_ERR_CONFIG, "the normal update needs three basis vectors");
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    st = cuda_check(c, launch_normal_three((long)c->N * c->N * c->N, dbasis(c), d_vol, d_coef, d_loss, rot, c->stream),
+                    "normal update");
+    if (!st) st = cuda_check(c, cudaStreamSynchronize(c->stream), "normal update");
     return st;
 }
 

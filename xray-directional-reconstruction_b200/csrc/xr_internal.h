@@ -63,6 +63,7 @@ struct BasisConst {
     float S[3 * kMaxBasis];
     float S2[kMaxBasis];
     float g[kMaxCond * kMaxBasis];  /* g[c*K + k] */
+    float G[3 * kMaxCond];          /* per axis: grating direction elemR_c e_z */
 };
 
 struct Timing {
@@ -91,6 +92,7 @@ struct Session {
     int storage = 0;                  /* volume                      */
     int sino_storage = 0;             /* measured sinogram           */
     int update_storage = 0;           /* volume, | kStoreStochastic  */
+    const float *coef = nullptr;      /* orientation-parametrised XTT: (phi, cos) planes */
     std::vector<int> order;            /* persistent subset order (XTT)     */
     std::vector<int> ir_orders;        /* C*epochs rows (IR)                */
     std::map<std::vector<int>, cudaGraphExec_t> graphs;  /* per subset order */
@@ -158,17 +160,21 @@ void timing_begin(xr_ctx *c, int cls, cudaEvent_t *ev);
 void timing_end(xr_ctx *c, int cls, cudaEvent_t ev);
 
 /* ---- kernel launchers (xr_kernels.cu) ---- */
+/* coef (the forward / back launchers): non-null selects the orientation-
+ * parametrised XTT of the reference's forwardOrth / backwardOrth (ir.cu:
+ * 294-423), every voxel's basis rotated by its (phi, cos theta) planes. */
 /* Forward splat of one set of views (all listed views of every listed axis).
  * mode 0: plain, value = ratio * vol[0]; mode 1: XTT K channels; mode 2:
  * weights only (value 1, the reference's devProjFactor).  out: C blocks of
  * V*Nd*Nd, accumulated with float atomics. */
 cudaError_t launch_forward(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                            const int *view_list, int n_views, int cond0, int n_cond, const void *vol,
-                           float *out, int mode, int views_per_cta, int storage, cudaStream_t s);
+                           float *out, int mode, int views_per_cta, int storage, cudaStream_t s,
+                           const float *coef = nullptr);
 /* Chord-length normaliser: norm = L / (norm + 1e-5) in place, every view. */
 cudaError_t launch_chord(const GeomConst &g, const ViewFrame *frames, float *norm, int n_cond, cudaStream_t s);
-/* Normalise + ratio (MLEM) or subtract (ART) on listed views of every axis,
- * FP64 loss sum added to *loss. */
+/* Normalise (skipped when norm is null) + ratio (MLEM) or subtract (ART) on
+ * listed views of every axis, FP64 loss sum added to *loss. */
 cudaError_t launch_ratio(const GeomConst &g, const int *view_list, int n_views, int n_cond, float *proj,
                          const float *norm, const void *sino, int art, double *loss, int storage, cudaStream_t s);
 /* Normalise only (proj *= norm) on every view: the forward operator A. */
@@ -176,7 +182,8 @@ cudaError_t launch_normalize(const GeomConst &g, int n_cond, float *proj, const 
 /* Back-projection of the listed views fused with the MLEM / ART update. */
 cudaError_t launch_back_update(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, int cond0, int n_cond, const float *proj,
-                               void *vol, int xtt, int art, float alpha, int storage, cudaStream_t s);
+                               void *vol, int xtt, int art, float alpha, int storage, cudaStream_t s,
+                               const float *coef = nullptr);
 /* FP64 sums: out[0] += sum (p-b)^2, out[1] += sum b^2, out[2] += sum |p-b|. */
 cudaError_t launch_residual(long n, const float *p, const void *b, double *out, int storage, cudaStream_t s);
 /* mu = sqrt|mu| over n values. */
@@ -189,15 +196,20 @@ cudaError_t check_exact_rdet(float det, float rdet, unsigned *d_flag, unsigned *
 cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, const int *d_conds, int n_cond, int G,
                                const float *d_magsig, const void *vol, float *out, int mode, int views_per_cta,
-                               int storage, cudaStream_t s);
+                               int storage, cudaStream_t s, const float *coef = nullptr);
 /* mode 0: plain (one axis, update in place); 1: XTT (fac_in = sensitivity);
  * 2: sensitivity of the listed views into fac_out. */
 cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                             const int *view_list, int n_views, const int *d_conds, int n_cond, const int *d_axis_g,
                             const float *d_magsig, const float *proj, void *vol, const float *fac_in, float *fac_out,
-                            int mode, int art, float alpha, int storage, cudaStream_t s);
+                            int mode, int art, float alpha, int storage, cudaStream_t s,
+                            const float *coef = nullptr);
 
 /* ---- xr_orient.cu ---- */
+/* calcNormalVectorThreeDirec (ir.cu:856-974) on every voxel: vol holds the
+ * three coefficients (FP32), coef (phi, cos theta) is updated, loss |(R e_z) x n|. */
+cudaError_t launch_normal_three(long nvox, const BasisConst *d_basis, const float *vol, float *coef, float *loss,
+                                int rot, cudaStream_t s);
 cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, const void *mu, float *md,
                                float *ev, int storage, cudaStream_t s);
 cudaError_t launch_angle_from_md(long nvox, const float *md, float *angle, cudaStream_t s);

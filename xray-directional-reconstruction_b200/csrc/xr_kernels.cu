@@ -36,6 +36,7 @@
 #include "xr_internal.h"
 #include "xr_storage.cuh"
 #include "xr_tile.cuh"
+#include "xr_orth.cuh"
 
 namespace xr {
 namespace {
@@ -114,6 +115,7 @@ struct FwdArgs {
     const void *vol;          /* mode 0: N^3; mode 1: K*N^3 (type T) */
     float *out;               /* C blocks of V*Nd*Nd         */
     const BasisConst *basis;  /* device                      */
+    const float *coef;        /* mode 3: rotation planes     */
     int nbx, nby;             /* bricks along x, y           */
 };
 
@@ -206,6 +208,8 @@ __global__ void __launch_bounds__(kFwdThreads, 3) k_forward(FwdArgs a) {
             val[q] = ldgf<T>(vol + idx);
         } else if (MODE == 2) {
             val[q] = 1.0f;
+        } else if (MODE == 3) {   /* forwardOrth (ir.cu:294-364) */
+            orth_moments<T>(a.basis, cond, g.K, __fmul_rn(g.vs, g.ratio), vol, a.coef, idx, N3, val[q], m[q]);
         } else {
             const BasisConst *B = a.basis;
             const float sc = __fmul_rn(g.vs, g.ratio);
@@ -233,7 +237,7 @@ __global__ void __launch_bounds__(kFwdThreads, 3) k_forward(FwdArgs a) {
     for (int q = 0; q < 4; q++) {
         if (!okv[q]) continue;
         float bq = (MODE == 0) ? fabsf(val[q]) * g.ratio : (MODE == 2 ? 1.0f : fabsf(val[q]));
-        if (MODE == 1)
+        if (MODE == 1 || MODE == 3)
 #pragma unroll
             for (int e = 0; e < 6; e++) bq += fabsf(m[q][e]);
         bound = fmaxf(bound, bq * 1.001f);
@@ -268,7 +272,7 @@ __global__ void __launch_bounds__(kFwdThreads, 3) k_forward(FwdArgs a) {
                 float c1, c2, c3, c4;
                 if (!taps(g, u, v, iu, iv, c1, c2, c3, c4)) continue;
                 float pv;
-                if (MODE == 1) {
+                if (MODE == 1 || MODE == 3) {
                     const float dd = fmaf(d0, d0, fmaf(d1, d1, d2 * d2));
                     const float q2 = m[q][0] * d0 * d0 + m[q][1] * d1 * d1 + m[q][2] * d2 * d2 +
                                      m[q][3] * d0 * d1 + m[q][4] * d0 * d2 + m[q][5] * d1 * d2;
@@ -410,7 +414,7 @@ __global__ void k_ratio(GeomConst g, const int *view_list, int n_views, float *p
     double acc = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < NdNd; i += (size_t)gridDim.x * blockDim.x) {
         const size_t idx = base + i;
-        float p = __fmul_rn(proj[idx], norm[idx]);
+        float p = norm ? __fmul_rn(proj[idx], norm[idx]) : proj[idx];
         const float b = ldgf<T>(sino + idx);
         acc += (double)fabsf(__fsub_rn(b, p));
         if (art) {
@@ -449,6 +453,7 @@ struct BackArgs {
     int art;
     float alpha;
     int sr;                   /* 16-bit volumes: stochastic rounding of updates */
+    const float *coef;        /* non-null: per-voxel rotated basis (backwardOrth) */
 };
 
 template <bool XTT, typename T>
@@ -515,7 +520,26 @@ __global__ void __launch_bounds__(kBackThreads) k_back_update(BackArgs a) {
                 }
             }
         }
-        if (XTT && ok) {
+        if (XTT && ok && a.coef) {   /* backwardOrth (ir.cu:366-423): the voxel's rotated basis */
+            const BasisConst *B = a.basis;
+            float R[9];
+            orth_rotation(a.coef, (size_t)N * N * N, (size_t)x + (size_t)N * y + (size_t)N * N * z, R);
+            const float G0 = B->G[3 * cond], G1 = B->G[3 * cond + 1], G2 = B->G[3 * cond + 2];
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                if (k >= g.K) break;
+                float S[3];
+                orth_basis(B, k, R, S);
+                const float h = S[0] * G0 + S[1] * G1 + S[2] * G2, gk = h * h;
+                const float s2 = S[0] * S[0] + S[1] * S[1] + S[2] * S[2];
+                const float sAs = S[0] * S[0] * A[0] + S[1] * S[1] * A[1] + S[2] * S[2] * A[2] +
+                                  2.f * (S[0] * S[1] * A[3] + S[0] * S[2] * A[4] + S[1] * S[2] * A[5]);
+                const float sFs = S[0] * S[0] * F[0] + S[1] * S[1] * F[1] + S[2] * S[2] * F[2] +
+                                  2.f * (S[0] * S[1] * F[3] + S[0] * S[2] * F[4] + S[1] * S[2] * F[5]);
+                tmpk[k] = fmaf(gk, fmaf(s2, A0, -sAs), tmpk[k]);
+                fack[k] = fmaf(gk, fmaf(s2, F0, -sFs), fack[k]);
+            }
+        } else if (XTT && ok) {
             const BasisConst *B = a.basis;
 #pragma unroll
             for (int k = 0; k < 16; k++) {
@@ -600,9 +624,11 @@ int grid_for(size_t n, int threads) {
 
 cudaError_t launch_forward(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                            const int *view_list, int n_views, int cond0, int n_cond, const void *vol, float *out,
-                           int mode, int views_per_cta, int storage, cudaStream_t s) {
+                           int mode, int views_per_cta, int storage, cudaStream_t s, const float *coef) {
     if (n_views <= 0 || n_cond <= 0) return cudaSuccess;
+    if (coef && mode == 1) mode = 3;
     FwdArgs a;
+    a.coef = coef;
     a.g = g;
     a.frames = frames;
     a.view_list = view_list;
@@ -633,9 +659,13 @@ cudaError_t launch_forward(const GeomConst &g, const BasisConst *d_basis, const 
         if (e == cudaSuccess) k_forward<M, TT><<<grid, kFwdThreads, smem, s>>>(a);                                \
     } while (0)
     if (mode == 2) XR_FWD(2, float);
-    else if (storage == kBF16) { if (mode == 0) XR_FWD(0, __nv_bfloat16); else XR_FWD(1, __nv_bfloat16); }
-    else if (storage == kF16) { if (mode == 0) XR_FWD(0, __half); else XR_FWD(1, __half); }
-    else { if (mode == 0) XR_FWD(0, float); else XR_FWD(1, float); }
+    else if (storage == kBF16) {
+        if (mode == 0) XR_FWD(0, __nv_bfloat16); else if (mode == 3) XR_FWD(3, __nv_bfloat16); else XR_FWD(1, __nv_bfloat16);
+    } else if (storage == kF16) {
+        if (mode == 0) XR_FWD(0, __half); else if (mode == 3) XR_FWD(3, __half); else XR_FWD(1, __half);
+    } else {
+        if (mode == 0) XR_FWD(0, float); else if (mode == 3) XR_FWD(3, float); else XR_FWD(1, float);
+    }
 #undef XR_FWD
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
@@ -672,8 +702,10 @@ cudaError_t launch_normalize(const GeomConst &g, int n_cond, float *proj, const 
 
 cudaError_t launch_back_update(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, int cond0, int n_cond, const float *proj,
-                               void *vol, int xtt, int art, float alpha, int storage, cudaStream_t s) {
+                               void *vol, int xtt, int art, float alpha, int storage, cudaStream_t s,
+                               const float *coef) {
     BackArgs a;
+    a.coef = coef;
     a.sr = (storage & kStoreStochastic) != 0;
     storage &= ~kStoreStochastic;
     a.g = g;

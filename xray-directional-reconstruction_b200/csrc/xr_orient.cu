@@ -14,6 +14,7 @@
 
 #include "xr_internal.h"
 #include "xr_eig3.cuh"
+#include "xr_orth.cuh"
 #include "xr_storage.cuh"
 
 namespace xr {
@@ -88,6 +89,51 @@ __global__ void k_direction_normalization(long nvox, float *md) {
     }
 }
 
+/* Vector3X::normalize (reconstruct/include/vec.h:94-106). */
+__device__ __forceinline__ void normalize3(float v[3]) {
+    const float l = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (l > 1e-8f) {
+        v[0] /= l; v[1] /= l; v[2] /= l;
+    } else {
+        v[0] = v[1] = v[2] = 0.f;
+    }
+}
+
+/* calcNormalVectorThreeDirec, ir.cu:856-974: the plane normal
+ * (mu0 S0 - mu1' S1) x (mu0 S0 - mu2' S2) (signs of mu1, mu2 by rot), turned
+ * by the voxel's current rotation, z >= 0, becomes the new (phi, cos theta);
+ * loss = |(R e_z) x normal|. */
+__global__ void k_normal_three(long nvox, const BasisConst *B, const float *vol, float *coef, float *loss, int rot) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nvox; i += (long)gridDim.x * blockDim.x) {
+        float R[9];
+        orth_rotation(coef, (size_t)nvox, (size_t)i, R);
+        const float mu0 = vol[i], m1 = vol[nvox + i], m2 = vol[2 * nvox + i];
+        float mu1 = m1, mu2 = m2;
+        if (rot == 1) { mu1 = -m1; }
+        else if (rot == 2) { mu1 = -m1; mu2 = -m2; }
+        else if (rot == 3) { mu2 = -m2; }
+        float v1[3], v2[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            v1[j] = mu0 * B->S[j] - mu1 * B->S[3 + j];
+            v2[j] = mu0 * B->S[j] - mu2 * B->S[6 + j];
+        }
+        float n[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2], v1[0] * v2[1] - v1[1] * v2[0]};
+        normalize3(n);
+        float r[3] = {R[0] * n[0] + R[1] * n[1] + R[2] * n[2], R[3] * n[0] + R[4] * n[1] + R[5] * n[2],
+                      R[6] * n[0] + R[7] * n[1] + R[8] * n[2]};
+        if (r[2] < 0.f) { r[0] = -r[0]; r[1] = -r[1]; r[2] = -r[2]; }
+        normalize3(r);
+        /* (R e_z) x r */
+        const float be0 = R[2], be1 = R[5], be2 = R[8];
+        const float dx = be1 * r[2] - be2 * r[1], dy = be2 * r[0] - be0 * r[2], dz = be0 * r[1] - be1 * r[0];
+        loss[i] = sqrtf(dx * dx + dy * dy + dz * dz);
+        /* e_z x r = (-r1, r0, 0) */
+        coef[i] = atan2f(r[0], -r[1]);
+        coef[nvox + i] = r[2];
+    }
+}
+
 int grid_for(long n, int threads) {
     long b = (n + threads - 1) / threads;
     if (b > 148 * 16) b = 148 * 16;
@@ -102,6 +148,12 @@ cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, cons
     if (storage == kBF16) k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const __nv_bfloat16 *)mu, md, ev);
     else if (storage == kF16) k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const __half *)mu, md, ev);
     else k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const float *)mu, md, ev);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_normal_three(long nvox, const BasisConst *d_basis, const float *vol, float *coef, float *loss,
+                                int rot, cudaStream_t s) {
+    k_normal_three<<<grid_for(nvox, 256), 256, 0, s>>>(nvox, d_basis, vol, coef, loss, rot);
     return cudaGetLastError();
 }
 
