@@ -144,7 +144,7 @@ def conv_roofline(local: int, N: int = 256, reps: int = 3):
     flops = 2.0 * N ** 3 * macs
     peak, kind = measured_tensor_peak()
     net.close()
-    return {"bound": "tensor", "kernel": "k_conv_halo (tcgen05, BF16 x BF16 -> FP32)", "achieved": flops / ms / 1e9,
+    return {"bound": "tensor", "kernel": "k_conv_ws (tcgen05, BF16 x BF16 -> FP32)", "achieved": flops / ms / 1e9,
             "peak": peak, "unit": "TFLOP/s", "frac": flops / ms / 1e9 / peak, "peak_kind": kind,
             "infer_ms": ms, "flops_per_inference": flops, "workload": f"{N}^3 x {channels}, depth {depth}, width {width}"}
 

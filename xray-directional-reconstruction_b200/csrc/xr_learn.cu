@@ -10,7 +10,7 @@
  * channels are 32 or 64 contiguous bytes: exactly the 16-byte rows the tensor
  * core's shared-memory operands are built of.
  *
- *  k_conv_halo (fprop and dgrad): M = 128 voxels (an 8 x 16 patch of one
+ *  k_conv_ws (fprop and dgrad): M = 128 voxels (an 8 x 16 patch of one
  *    z-slice), N = output channels, K = 27 taps x input channels.  A CTA keeps
  *    all 27 taps of the weights in shared memory (K-major core matrices) and
  *    a ring of halo slices; every tap's operand is a shifted window of the
@@ -27,6 +27,7 @@
  * the error flag, waits (bounded) for its MMAs in flight, frees its tensor
  * memory and leaves.
  */
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -95,30 +96,54 @@ __device__ __forceinline__ uint8_t *align1k(uint8_t *p) {
     return p + (((s + 1023u) & ~1023u) - s);
 }
 
-/* Output of one voxel's NP accumulators (row of the M = 128 tile). */
+/* What the epilogue of one voxel reads from global memory, fetched before
+ * its accumulators are ready: the residual input (EPI_RESID; it may be the
+ * output itself, each element read by the thread that then writes it) or
+ * the ReLU mask (EPI_MASK). */
 template <int NP, int EPI>
-__device__ __forceinline__ void conv_epilogue(const ConvArgs &a, long v, long nvox, const float *acc) {
+struct EpiIn {
+    float r[EPI == EPI_RESID ? NP : 1];
+    uint4 m[EPI == EPI_MASK ? NP / 8 : 1];
+};
+
+template <int NP, int EPI>
+__device__ __forceinline__ void epi_fetch(const ConvArgs &a, long v, long nvox, EpiIn<NP, EPI> &in) {
+    if (EPI == EPI_RESID) {
+#pragma unroll
+        for (int n = 0; n < NP; n++) {
+            const size_t i = (size_t)n * nvox + v;
+            float r = 0.f;
+            if (n < a.nout) {
+                if (a.storage == kBF16) r = ldf(reinterpret_cast<const __nv_bfloat16 *>(a.res) + i);
+                else if (a.storage == kF16) r = ldf(reinterpret_cast<const __half *>(a.res) + i);
+                else r = ldf(reinterpret_cast<const float *>(a.res) + i);
+            }
+            in.r[n] = r;
+        }
+    } else if (EPI == EPI_MASK) {
+        const uint4 *mk = reinterpret_cast<const uint4 *>(a.mask + (size_t)v * NP);
+#pragma unroll
+        for (int j = 0; j < NP / 8; j++) in.m[j] = __ldg(mk + j);
+    }
+}
+
+/* Output of one voxel's NP accumulators (row of the M = 128 tile); `bias`
+ * holds NP values (zeros when the layer has none). */
+template <int NP, int EPI>
+__device__ __forceinline__ void conv_epilogue(const ConvArgs &a, const float *bias, long v, long nvox,
+                                              const float *acc, const EpiIn<NP, EPI> &in) {
     if (EPI == EPI_RESID) {
 #pragma unroll
         for (int n = 0; n < NP; n++) {
             if (n >= a.nout) break;
             const size_t i = (size_t)n * nvox + v;
-            float val = acc[n] + (a.bias ? a.bias[n] : 0.f);
-            if (a.storage == kBF16) {
-                val = fmaxf(ldf(reinterpret_cast<const __nv_bfloat16 *>(a.res) + i) + val * a.inv_scale,
-                            a.floor_value);
-                stf(reinterpret_cast<__nv_bfloat16 *>(a.out) + i, val);
-            } else if (a.storage == kF16) {
-                val = fmaxf(ldf(reinterpret_cast<const __half *>(a.res) + i) + val * a.inv_scale, a.floor_value);
-                stf(reinterpret_cast<__half *>(a.out) + i, val);
-            } else {
-                val = fmaxf(ldf(reinterpret_cast<const float *>(a.res) + i) + val * a.inv_scale, a.floor_value);
-                stf(reinterpret_cast<float *>(a.out) + i, val);
-            }
+            const float val = fmaxf(in.r[n] + (acc[n] + bias[n]) * a.inv_scale, a.floor_value);
+            if (a.storage == kBF16) stf(reinterpret_cast<__nv_bfloat16 *>(a.out) + i, val);
+            else if (a.storage == kF16) stf(reinterpret_cast<__half *>(a.out) + i, val);
+            else stf(reinterpret_cast<float *>(a.out) + i, val);
         }
     } else {
         uint4 *yo = reinterpret_cast<uint4 *>(a.y + (size_t)v * NP);
-        const uint4 *mk = reinterpret_cast<const uint4 *>(a.mask + (size_t)v * NP);
 #pragma unroll
         for (int j = 0; j < NP / 8; j++) {
             float o[8];
@@ -126,12 +151,11 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs &a, long v, long nv
             for (int i = 0; i < 8; i++) {
                 const int n = 8 * j + i;
                 o[i] = acc[n];
-                if (EPI != EPI_MASK && a.bias) o[i] += a.bias[n];
+                if (EPI != EPI_MASK) o[i] += bias[n];
                 if (EPI == EPI_RELU) o[i] = fmaxf(o[i], 0.f);
             }
             if (EPI == EPI_MASK) {
-                const uint4 m = mk[j];
-                const uint32_t mw[4] = {m.x, m.y, m.z, m.w};
+                const uint32_t mw[4] = {in.m[j].x, in.m[j].y, in.m[j].z, in.m[j].w};
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
                     if (!(bf_lo(mw[i]) > 0.f)) o[2 * i] = 0.f;
@@ -151,49 +175,94 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs &a, long v, long nv
 /* channels 8j..8j+7 of every halo voxel, x fastest).  For tap (dz,dy,dx)  */
 /* the A operand is then a window of the halo: 8 consecutive 16-byte rows  */
 /* are the 8 x-voxels of one y-row (a core matrix), y-rows are 160 bytes   */
-/* apart (SBO), planes PLANE bytes apart (LBO) - the descriptor's start    */
-/* address moves by (dy * 10 + dx) * 16 bytes and by one slice for dz.     */
-/* No per-tap loads or barriers: each input slice is loaded once (zero     */
-/* outside the volume) into a 4-slot ring and serves three output slices;  */
-/* the 27 x KP/16 MMAs of a slice are issued back to back into one of two  */
-/* tensor-memory accumulators while the previous slice's epilogue runs.    */
+/* apart (SBO), planes kPlane bytes apart (LBO) - the descriptor's start   */
+/* address moves by (dy * 10 + dx) * 16 bytes.                             */
+/*                                                                         */
+/* Each input slice is read once and feeds three output slices: the three  */
+/* dz taps of one (dy, dx) are stacked along N (the weights of tap         */
+/* (dz, dy, dx) sit at block dz of group dy * 3 + dx), so one MMA with     */
+/* N = 3 x NP multiplies the window by all three and adds into the         */
+/* accumulators of output slices z + 1, z and z - 1 at once.  Those live   */
+/* in a ring of tensor-memory blocks of NP columns whose position falls as */
+/* the output index rises (block CR - 1 - o % CR), so the three are        */
+/* adjacent columns in the order of the stacked weights; at the ring's     */
+/* wrap the MMA is split per block.  An input slice costs 9 x KP/16 MMAs   */
+/* and its window bytes are read from shared memory once instead of three  */
+/* times.  A slice's first MMA overwrites (accumulate = 0) the blocks of   */
+/* the output slices it starts.                                            */
+/*                                                                         */
+/* The CTA is warp-specialised, with no CTA-wide barrier in the loop:      */
+/* warp 5 (one thread) loads halo slices with tensor-map copies (zero fill */
+/* outside the volume) into a ring of R slots, warp 4 (one thread) issues  */
+/* the MMAs, warps 0-3 read the accumulators out and run the epilogue.     */
+/* They hand off through mbarriers:                                        */
+/*   full[s]   slot s holds its slice    (copy transaction bytes)          */
+/*   empty[s]  slot s may be refilled    (MMA commit)                      */
+/*   acc[p]    ring block p complete     (MMA commit)                      */
+/*   free[p]   ring block p read out     (128 epilogue arrivals)           */
+/* Every CTA walks the same static item sequence (an xy tile and a range   */
+/* of z); slice and output counters run on across items, which fixes each  */
+/* barrier's phase.  Input slices outside the volume are not loaded and    */
+/* issue no MMAs.                                                          */
 /* ---------------------------------------------------------------------- */
-constexpr int kHX = 10, kHY = 18, kHV = kHX * kHY;   /* halo slice: 180 voxels */
-constexpr int kRing = 4;
+constexpr int kHX = 10, kHY = 18, kHV = kHX * kHY;   /* halo slice: 180 voxels   */
+constexpr int kPlane = 2944;                         /* 2880 bytes, 128-aligned */
+constexpr int kConvWsThreads = 192;
+constexpr int kConvSmemBudget = 115712;              /* two CTAs per SM          */
+constexpr int kConvTmemCols = 256;
 
 template <int KP, int NP>
-struct HaloSmem {
-    static constexpr int BT = NP * KP * 2;
+struct ConvSmem {
+    static constexpr int BT = NP * KP * 2;                        /* one tap's weights  */
     static constexpr int BB = ((27 * BT + 1023) / 1024) * 1024;
-    static constexpr int PLANE = kHV * 16;                       /* 2880 bytes */
-    static constexpr int SLOT = (KP / 8) * PLANE;
-    static constexpr int bytes = 1024 + BB + kRing * SLOT + 2 * 8 + 16;
-    static constexpr int LOADS = (kHV * KP / 8 + kConvThreads - 1) / kConvThreads;   /* 16-byte loads per thread */
+    static constexpr int SLOT = (KP / 8) * kPlane;
+    static constexpr int CR = kConvTmemCols / NP;                 /* accumulator ring   */
+    static constexpr int RR = (kConvSmemBudget - 1024 - BB - 8 * (2 * CR + 1) - 16) / (SLOT + 16);
+    static constexpr int R = RR > 16 ? 16 : RR;                   /* halo-slice ring    */
+    static constexpr int NBAR = 2 * R + 2 * CR + 1;               /* full, empty, acc, free, drain */
+    static constexpr int bytes = 1024 + BB + R * SLOT + NBAR * 8 + 16;
+    static constexpr uint32_t TX = (KP / 8) * kHV * 16;           /* bytes per slice    */
+    static_assert(R >= 3, "halo ring too shallow");
+    static_assert(bytes <= kConvSmemBudget, "shared memory over budget");
+    static_assert(3 * (bytes + 1024) > 233472, "a third CTA per SM would exceed tensor memory");
 };
 
 template <int KP, int NP, int EPI>
-__global__ void __launch_bounds__(kConvThreads) k_conv_halo(ConvArgs a, int zchunk) {
-    using L = HaloSmem<KP, NP>;
+__global__ void __launch_bounds__(kConvWsThreads) k_conv_ws(const __grid_constant__ CUtensorMap xmap, ConvArgs a,
+                                                            int zchunk) {
+    using L = ConvSmem<KP, NP>;
+    constexpr int R = L::R, CR = L::CR;
     constexpr uint32_t SBO_B = (KP / 8) * 128;
-    constexpr uint32_t IDESC = tc::idesc_bf16(128, NP, 0, 0);
     extern __shared__ uint8_t smem_raw[];
     uint8_t *sm = align1k(smem_raw);
     uint8_t *sB = sm, *ring = sm + L::BB;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(ring + kRing * L::SLOT);   /* one per accumulator */
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
-    __shared__ int s_abort;
+    uint64_t *full = reinterpret_cast<uint64_t *>(ring + R * L::SLOT);
+    uint64_t *empty = full + R, *accb = empty + R, *freeb = accb + CR, *drain = freeb + CR;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
+    __shared__ volatile int s_abort;
+    __shared__ float s_bias[NP];
 
     const int tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) {
-        tc::mbar_init(&bar[0], 1);
-        tc::mbar_init(&bar[1], 1);
+        for (int i = 0; i < R; i++) {
+            tc::mbar_init(&full[i], 1);
+            tc::mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < CR; i++) {
+            tc::mbar_init(&accb[i], 1);
+            tc::mbar_init(&freeb[i], 128);
+        }
+        tc::mbar_init(drain, 1);
         tc::fence_mbar_init();
         s_abort = 0;
     }
-    if (warp == 0) tc::tmem_alloc(tslot, 2 * kTmemCols);
-    for (int c = tid; c < 27 * NP * KP / 8; c += kConvThreads) {
+    if (tid < NP) s_bias[tid] = (EPI != EPI_MASK && a.bias && (EPI != EPI_RESID || tid < a.nout)) ? a.bias[tid] : 0.f;
+    if (warp == 0) tc::tmem_alloc(tslot, kConvTmemCols);
+    /* weights of tap t = (dz, dy, dx) at block dz of group dy * 3 + dx */
+    for (int c = tid; c < 27 * NP * KP / 8; c += kConvWsThreads) {
         const int j = c % (KP / 8), n = (c / (KP / 8)) % NP, t = c / (NP * KP / 8);
-        *reinterpret_cast<uint4 *>(sB + t * L::BT + (n >> 3) * SBO_B + j * 128 + (n & 7) * 16) =
+        const int pos = (t % 9) * 3 + t / 9;
+        *reinterpret_cast<uint4 *>(sB + pos * L::BT + (n >> 3) * SBO_B + j * 128 + (n & 7) * 16) =
             __ldg(reinterpret_cast<const uint4 *>(a.w) + c);
     }
     tc::fence_async_smem();
@@ -206,124 +275,153 @@ __global__ void __launch_bounds__(kConvThreads) k_conv_halo(ConvArgs a, int zchu
     const long nvox = (long)nx * ny * nz;
     const int ntx = (nx + 7) / 8, nty = (ny + 15) / 16, ntz = (nz + zchunk - 1) / zchunk;
     const long items = (long)ntx * nty * ntz;
-    uint32_t uses0 = 0, uses1 = 0;        /* completions waited for, per accumulator   */
-    uint32_t commits0 = 0, commits1 = 0;  /* commits issued (by thread 0; tracked by all) */
-    bool aborted = false;
 
-    /* 16-byte halo loads of input slice zin into registers */
-    auto fetch = [&](int x0, int y0, int zin, uint4 *r) {
-#pragma unroll
-        for (int u = 0; u < L::LOADS; u++) {
-            const int e = tid + u * kConvThreads;
-            r[u] = make_uint4(0u, 0u, 0u, 0u);
-            if (e < kHV * KP / 8 && zin >= 0 && zin < nz) {
-                const int j = e % (KP / 8), hv = e / (KP / 8);
-                const int gx = x0 - 1 + hv % kHX, gy = y0 - 1 + hv / kHX;
-                if (gx >= 0 && gx < nx && gy >= 0 && gy < ny)
-                    r[u] = __ldg(reinterpret_cast<const uint4 *>(
-                                     a.x + ((size_t)gx + (size_t)nx * (gy + (size_t)ny * zin)) * KP) + j);
-            }
-        }
-    };
-    auto stash = [&](uint8_t *slot, const uint4 *r) {
-#pragma unroll
-        for (int u = 0; u < L::LOADS; u++) {
-            const int e = tid + u * kConvThreads;
-            if (e < kHV * KP / 8) {
-                const int j = e % (KP / 8), hv = e / (KP / 8);
-                *reinterpret_cast<uint4 *>(slot + j * L::PLANE + hv * 16) = r[u];
-            }
-        }
-    };
-
-    for (long item = blockIdx.x; item < items && !aborted; item += gridDim.x) {
-        const int tx = (int)(item % ntx), ty = (int)((item / ntx) % nty), tz = (int)(item / ((long)ntx * nty));
-        const int x0 = tx * 8, y0 = ty * 16, z0 = tz * zchunk;
-        const int nzs = min(zchunk, nz - z0);      /* output slices of this item */
-        const int ox = x0 + (tid & 7), oy = y0 + (tid >> 3);
-        /* input slice k (z = z0 - 1 + k) lives in ring slot k % 4; prologue: k = 0, 1 */
-        uint4 r[L::LOADS];
-        fetch(x0, y0, z0 - 1, r);
-        stash(ring + 0 * L::SLOT, r);
-        fetch(x0, y0, z0, r);
-        stash(ring + 1 * L::SLOT, r);
-        fetch(x0, y0, z0 + 1, r);                 /* slice k = 2, stored in iteration 0 */
-        for (int i = 0; i <= nzs; i++) {
-            if (i < nzs) {
-                /* slot (i+2) % 4 held slice i-2, whose last reader (output i-1... i-2)
-                 * completed: output i-2's epilogue waited for its MMAs, and output
-                 * i-1 reads slices i-1..i+1 only */
-                stash(ring + ((i + 2) % kRing) * L::SLOT, r);
-                if (i + 1 < nzs) fetch(x0, y0, z0 + i + 2, r);
-                tc::fence_async_smem();
-                tc::fence_before_sync();
-                __syncthreads();
-                if (s_abort) { aborted = true; break; }
-                if (tid == 0) {
-                    tc::fence_after_sync();
-                    const int buf = i & 1;
-                    const uint32_t d = tmem + buf * kTmemCols;
-                    /* descriptors: a base per input slice (dz), the tap's (dy, dx)
-                     * window and the K step added to the start-address field
-                     * (16-byte units; no carry: shared addresses < 256 KB) */
-                    uint64_t aS[3];
-#pragma unroll
-                    for (int dz = 0; dz < 3; dz++)
-                        aS[dz] = tc::sdesc(tc::smem_u32(ring + ((i + dz) % kRing) * L::SLOT), L::PLANE, kHX * 16);
-                    const uint64_t bS = tc::sdesc(tc::smem_u32(sB), 128, SBO_B);
-#pragma unroll
-                    for (int t = 0; t < 27; t++) {
-                        const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-                        const uint64_t at = aS[dz] + (uint64_t)(dy * kHX + dx);
-                        const uint64_t bt = bS + (uint64_t)(t * (L::BT >> 4));
-#pragma unroll
-                        for (int kk = 0; kk < KP / 16; kk++)
-                            tc::mma_bf16(d, at + (uint64_t)(kk * (2 * L::PLANE >> 4)), bt + (uint64_t)(kk * 16), IDESC,
-                                         (t | kk) != 0);
+    if (warp == 5) {
+        /* ---------------- halo loads (one thread) ---------------- */
+        if ((tid & 31) == 0) {
+            uint32_t gs = 0;
+            bool ok = true;
+            for (long item = blockIdx.x; item < items && ok; item += gridDim.x) {
+                const int tx = (int)(item % ntx), ty = (int)((item / ntx) % nty), tz = (int)(item / ((long)ntx * nty));
+                const int z0 = tz * zchunk, nzs = min(zchunk, nz - z0);
+                for (int li = -1; li <= nzs && ok; li++, gs++) {
+                    const int slot = gs % R;
+                    if (gs >= (uint32_t)R &&
+                        (s_abort || !tc::mbar_wait(&empty[slot], ((gs / R) - 1) & 1, kWaitCycles))) {
+                        ok = false;
+                        break;
                     }
-                    tc::mma_commit(&bar[buf]);
-                }
-                if (i & 1) commits1++;
-                else commits0++;
-            }
-            if (i >= 1) {   /* epilogue of output slice i - 1 */
-                const int buf = (i - 1) & 1;
-                const uint32_t k_use = buf ? uses1++ : uses0++;
-                /* a wait that runs out is seen by every thread at the next barrier */
-                if (!tc::mbar_wait(&bar[buf], k_use & 1, kWaitCycles)) {
-                    s_abort = 1;
-                } else {
-                    tc::fence_after_sync();
-                    float acc[NP];
-                    const uint32_t taddr = tmem + buf * kTmemCols + ((uint32_t)(warp * 32) << 16);
-                    if (NP == 16) tc::tmem_ld16(taddr, acc);
-                    else tc::tmem_ld32(taddr, acc);
-                    tc::fence_before_sync();
-                    const int oz = z0 + i - 1;
-                    if (ox < nx && oy < ny)
-                        conv_epilogue<NP, EPI>(a, (long)ox + (long)nx * (oy + (long)ny * oz), nvox, acc);
+                    const int z = z0 + li;
+                    if (z >= 0 && z < nz) {
+                        tc::mbar_arrive_tx(&full[slot], L::TX);
+                        uint8_t *dst = ring + slot * L::SLOT;
+#pragma unroll
+                        for (int j = 0; j < KP / 8; j++)
+                            tc::tma_load_4d(dst + j * kPlane, &xmap, &full[slot], 8 * j, tx * 8 - 1, ty * 16 - 1, z);
+                    } else {
+                        tc::mbar_arrive(&full[slot]);
+                    }
                 }
             }
-            if (aborted) break;
+            /* no copy may still be writing when the CTA leaves */
+            for (uint32_t g = gs > (uint32_t)R ? gs - R : 0; g < gs; g++)
+                if (!tc::mbar_wait(&full[g % R], (g / R) & 1, kWaitCycles)) ok = false;
+            if (!ok) s_abort = 1;
         }
-        if (aborted) break;
+    } else if (warp == 4) {
+        /* ---------------- MMA issue (one thread) ---------------- */
+        if ((tid & 31) == 0) {
+            uint32_t gs = 0, ob = 0;   /* slices and outputs so far */
+            bool ok = true;
+            const uint64_t bS = tc::sdesc(tc::smem_u32(sB), 128, SBO_B);
+            for (long item = blockIdx.x; item < items && ok; item += gridDim.x) {
+                const int tz = (int)(item / ((long)ntx * nty));
+                const int z0 = tz * zchunk, nzs = min(zchunk, nz - z0);
+                for (int li = -1; li <= nzs && ok; li++, gs++) {
+                    const int slot = gs % R, z = z0 + li;
+                    if (s_abort || !tc::mbar_wait(&full[slot], (gs / R) & 1, kWaitCycles)) {
+                        ok = false;
+                        break;
+                    }
+                    if (z >= 0 && z < nz) {
+                        /* outputs olo..ohi (item-local) take blocks j = li + 1 - o; the ones this
+                         * slice starts (no earlier slice inside the volume) are the top nf */
+                        const int olo = max(0, li - 1), ohi = min(nzs - 1, li + 1);
+                        const int nf = (li + 1 <= nzs - 1) + (li >= 0 && li <= nzs - 1 && z == 0);
+                        for (int f = 0; f < nf && ok; f++) {
+                            const uint32_t O = ob + (uint32_t)(ohi - f);
+                            if (O >= (uint32_t)CR &&
+                                (s_abort || !tc::mbar_wait(&freeb[CR - 1 - O % CR], ((O / CR) - 1) & 1, kWaitCycles)))
+                                ok = false;
+                        }
+                        if (!ok) break;
+                        tc::fence_after_sync();
+                        const uint64_t aS = tc::sdesc(tc::smem_u32(ring + slot * L::SLOT), kPlane, kHX * 16);
+                        const int jlo = li + 1 - ohi, jhi = li + 1 - olo;
+                        const uint32_t Otop = ob + (uint32_t)ohi;   /* output of block jlo */
+                        /* first MMA of the slice: one per block, overwriting the started outputs */
+                        for (int j = jlo; j <= jhi; j++) {
+                            const uint32_t O = Otop - (uint32_t)(j - jlo);
+                            tc::mma_bf16(tmem + (CR - 1 - O % CR) * NP, aS, bS + (uint64_t)(j * (L::BT >> 4)),
+                                         tc::idesc_bf16(128, NP, 0, 0), j < jlo + nf ? 0u : 1u);
+                        }
+                        /* the rest: blocks jlo..jw in one MMA, and jw+1..jhi in a second where the
+                         * ring wraps between them */
+                        const int jw = min(jhi, jlo + (int)(Otop % CR));
+                        const uint32_t dA = tmem + (CR - 1 - Otop % CR) * NP, dB = tmem;
+                        const uint64_t bA = bS + (uint64_t)(jlo * (L::BT >> 4)), bB = bS + (uint64_t)((jw + 1) * (L::BT >> 4));
+                        const uint32_t iA = tc::idesc_bf16(128, NP * (jw - jlo + 1), 0, 0);
+                        const uint32_t iB = tc::idesc_bf16(128, NP * max(1, jhi - jw), 0, 0);
+                        if (jw == jhi) {
+#pragma unroll
+                            for (int m = 1; m < 9 * (KP / 16); m++) {
+                                const int g = m / (KP / 16), kk = m % (KP / 16);
+                                const uint64_t ao = (uint64_t)((g / 3) * kHX + g % 3 + kk * (2 * kPlane >> 4));
+                                const uint64_t bo = (uint64_t)(g * 3 * (L::BT >> 4) + kk * 16);
+                                tc::mma_bf16(dA, aS + ao, bA + bo, iA, 1u);
+                            }
+                        } else {
+#pragma unroll
+                            for (int m = 1; m < 9 * (KP / 16); m++) {
+                                const int g = m / (KP / 16), kk = m % (KP / 16);
+                                const uint64_t ao = (uint64_t)((g / 3) * kHX + g % 3 + kk * (2 * kPlane >> 4));
+                                const uint64_t bo = (uint64_t)(g * 3 * (L::BT >> 4) + kk * 16);
+                                tc::mma_bf16(dA, aS + ao, bA + bo, iA, 1u);
+                                tc::mma_bf16(dB, aS + ao, bB + bo, iB, 1u);
+                            }
+                        }
+                        tc::mma_commit(&empty[slot]);
+                    } else {
+                        tc::mbar_arrive(&empty[slot]);   /* nothing was loaded or read */
+                    }
+                    if (li >= 1) tc::mma_commit(&accb[CR - 1 - (ob + li - 1) % CR]);   /* output li - 1 complete */
+                }
+                ob += (uint32_t)nzs;
+            }
+            if (!ok) s_abort = 1;
+            tc::mma_commit(drain);   /* arrives once every MMA issued here has completed */
+        }
+    } else {
+        /* ---------------- epilogue (warps 0-3) ---------------- */
+        uint32_t O = 0;
+        bool ok = true;
+        for (long item = blockIdx.x; item < items && ok; item += gridDim.x) {
+            const int tx = (int)(item % ntx), ty = (int)((item / ntx) % nty), tz = (int)(item / ((long)ntx * nty));
+            const int z0 = tz * zchunk, nzs = min(zchunk, nz - z0);
+            const int ox = tx * 8 + (tid & 7), oy = ty * 16 + (tid >> 3);
+            const bool in_tile = ox < nx && oy < ny;
+            for (int o = 0; o < nzs; o++, O++) {
+                const int p = CR - 1 - (int)(O % CR);
+                const long v = (long)ox + (long)nx * (oy + (long)ny * (z0 + o));
+                EpiIn<NP, EPI> in;
+                if (in_tile) epi_fetch<NP, EPI>(a, v, nvox, in);
+                if (s_abort || !tc::mbar_wait(&accb[p], (O / CR) & 1, kWaitCycles)) {
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                float acc[NP];
+                const uint32_t taddr = tmem + p * NP + ((uint32_t)(warp * 32) << 16);
+                if (NP == 16) tc::tmem_ld16(taddr, acc);
+                else tc::tmem_ld32(taddr, acc);
+                tc::fence_before_sync();
+                tc::mbar_arrive(&freeb[p]);
+                if (in_tile) conv_epilogue<NP, EPI>(a, s_bias, v, nvox, acc, in);
+            }
+        }
+        if (!ok) s_abort = 1;
     }
-    tc::fence_before_sync();
-    __syncthreads();
-    if (s_abort) aborted = true;
-    /* a wait that ran out leaves MMAs possibly in flight: wait (bounded) for
-     * each accumulator's last commit */
-    if (aborted) {
-        if (commits0 > 0) tc::mbar_wait(&bar[0], (commits0 - 1) & 1, kWaitCycles);
-        if (commits1 > 0) tc::mbar_wait(&bar[1], (commits1 - 1) & 1, kWaitCycles);
+    /* every MMA complete before the tensor memory is freed */
+    if (tid == 0) {
+        if (!tc::mbar_wait(drain, 0, kWaitCycles)) s_abort = 1;
     }
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, 2 * kTmemCols);
+        tc::tmem_dealloc(tmem, kConvTmemCols);
     }
-    if (aborted && tid == 0) atomicExch(a.err, 1);
+    if (s_abort && tid == 0) atomicExch(a.err, 1);
 }
 
 struct WgradArgs {
@@ -626,26 +724,74 @@ int sm_count() {
     return g_sms;
 }
 
+/* cuTensorMapEncodeTiled through the runtime's driver entry point (no
+ * link-time dependency on the driver library). */
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static const EncodeTiledFn fn = []() -> EncodeTiledFn {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+/* Tensor map of a channels-last BF16 activation [nz][ny][nx][KP]: boxes of
+ * 8 channels x 10 x 18 voxels x 1 slice, i.e. one plane of a halo slice. */
+cudaError_t halo_map(const bf16 *x, int KP, int nx, int ny, int nz, CUtensorMap *m) {
+    const EncodeTiledFn enc = encode_tiled();
+    if (!enc || (reinterpret_cast<uintptr_t>(x) & 15u)) return cudaErrorInvalidValue;
+    const cuuint64_t dims[4] = {(cuuint64_t)KP, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t strides[3] = {(cuuint64_t)KP * 2, (cuuint64_t)KP * 2 * nx, (cuuint64_t)KP * 2 * nx * ny};
+    const cuuint32_t box[4] = {8, kHX, kHY, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(x), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+/* z-chunk of the work items: the fewest slices on the busiest CTA, counting
+ * one slice of overhead per item for its two halo slices. */
+long conv_zchunk(long xy, int nz, long grid0) {
+    long best = nz, best_cost = -1;
+    for (long ntz = 1; ntz <= nz; ntz++) {
+        const long zc = (nz + ntz - 1) / ntz;
+        if (zc > 64) continue;
+        const long items = xy * ((nz + zc - 1) / zc);
+        const long cost = ((items + grid0 - 1) / grid0) * (zc + 1);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = zc;
+        }
+    }
+    return best;
+}
+
 template <int KP, int NP, int EPI>
 cudaError_t launch_halo_t(const ConvArgs &a, cudaStream_t s) {
-    const int bytes = HaloSmem<KP, NP>::bytes;
-    cudaError_t e = cudaFuncSetAttribute(k_conv_halo<KP, NP, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    using L = ConvSmem<KP, NP>;
+    CUtensorMap map;
+    cudaError_t e = halo_map(a.x, KP, a.nx, a.ny, a.nz, &map);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_ws<KP, NP, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_conv_halo<KP, NP, EPI>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        e = cudaFuncSetAttribute(k_conv_ws<KP, NP, EPI>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
-    /* CTAs per SM from shared memory (228 KB per SM, 1 KB reserved per CTA),
-     * at most 4 (tensor memory: 4 x 64 of 512 columns) */
-    int occ = 233472 / (bytes + 1024);
-    occ = occ < 1 ? 1 : (occ > 4 ? 4 : occ);
-    const long grid0 = (long)sm_count() * occ;
+    /* two CTAs per SM: shared memory and the 2 x 256 tensor-memory columns */
+    const long grid0 = (long)sm_count() * 2;
     const long xy = (long)((a.nx + 7) / 8) * ((a.ny + 15) / 16);
-    /* z-chunk: long enough to amortise the two halo slices, short enough
-     * for two work items per CTA */
-    const long zc = std::max<long>(1, std::min<long>(64, ((long)a.nz * xy) / (2 * grid0)));
+    const long zc = conv_zchunk(xy, a.nz, grid0);
     const long items = xy * ((a.nz + zc - 1) / zc);
     const long grid = std::min<long>(items, grid0);
-    k_conv_halo<KP, NP, EPI><<<(int)grid, kConvThreads, bytes, s>>>(a, (int)zc);
+    k_conv_ws<KP, NP, EPI><<<(int)grid, kConvWsThreads, L::bytes, s>>>(map, a, (int)zc);
     return cudaGetLastError();
 }
 

@@ -59,6 +59,30 @@ __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
+/* One arrival on the mbarrier (release semantics at CTA scope). */
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+/* One arrival that also expects `bytes` more transaction bytes this phase. */
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+/* Tensor-map (TMA) load of one 4-D box into shared memory (128-byte aligned
+ * destination); its bytes complete a transaction on the mbarrier.  Elements
+ * outside the tensor are filled with zeros.  `map` is the generic address of
+ * a __grid_constant__ kernel parameter. */
+__device__ __forceinline__ void tma_load_4d(void *dst, const void *map, uint64_t *bar, int c0, int c1, int c2,
+                                            int c3) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, "
+        "%6}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+
 /* Waits for the phase of the given parity to complete; gives up after about
  * `limit` clock cycles (false). */
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
