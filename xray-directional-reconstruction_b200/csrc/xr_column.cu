@@ -125,7 +125,7 @@ struct FwdColArgs {
 };
 
 template <int MODE, int G, typename T>
-__global__ void __launch_bounds__(kFwdThreads, 3) k_fwd_col(FwdColArgs a) {
+__global__ void __launch_bounds__(kFwdThreads, 4) k_fwd_col(FwdColArgs a) {
     const T *vol = reinterpret_cast<const T *>(a.vol);
     constexpr int A = Ax<G>::A, B = Ax<G>::B;
     /* Two detector tiles (double-buffered over views) in two-word fixed
@@ -178,6 +178,11 @@ __global__ void __launch_bounds__(kFwdThreads, 3) k_fwd_col(FwdColArgs a) {
         iu1 = min(iu1, Nd - 1); iv1 = min(iv1, Nd - 1);
         int W = iu1 - iu0 + 1, H = iv1 - iv0 + 1;
         if (!ok) { W = 1 << 20; H = 1; }
+        {   /* row stride = 6 mod 8: four rows apart (the thread segments of a warp)
+             * lie 24 banks apart, spreading the warp's atomics over the banks */
+            const int Wp = W + (((6 - W) % 8) + 8) % 8;
+            if (Wp * H <= kTileCap) W = Wp;
+        }
         if (iu1 < iu0 || iv1 < iv0) { W = 0; H = 0; }
         bbox[i] = make_int4(iu0, iv0, W, H);
     }
@@ -237,6 +242,17 @@ __global__ void __launch_bounds__(kFwdThreads, 3) k_fwd_col(FwdColArgs a) {
             for (int e = 0; e < 6; e++) m[q][e] = mm[e];
         }
     }
+    if (MODE == 1 || MODE == 3) {
+        /* M in the column frame: (aa, bb, ab, ag, bg, gg), so that per view
+         * d^T M d = aa da^2 + bb db^2 + ab da db + dg (ag da + bg db + gg dg) */
+        constexpr int AB = 3 + A + B - 1, AG = 3 + A + G - 1, BG = 3 + B + G - 1;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float t[6] = {m[q][A], m[q][B], m[q][AB], m[q][AG], m[q][BG], m[q][G]};
+#pragma unroll
+            for (int e = 0; e < 6; e++) m[q][e] = t[e];
+        }
+    }
     /* bound on |contribution| over the CTA's voxels (weights c <= 1) */
     float bound = 0.f;
 #pragma unroll
@@ -275,6 +291,7 @@ __global__ void __launch_bounds__(kFwdThreads, 3) k_fwd_col(FwdColArgs a) {
             col_ray<G>(f, g, ba, bb, u, coeff, da, db);
             if (tap1(g, u, iu, fu, gu)) {
                 const float dab2 = fmaf(da, da, db * db);
+                const float daa = da * da, dbb = db * db, dab = da * db;
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     if (!okv[q]) continue;
@@ -295,11 +312,10 @@ __global__ void __launch_bounds__(kFwdThreads, 3) k_fwd_col(FwdColArgs a) {
                     } else if (MODE == 2) {
                         w1 = c1; w2 = c2; w3 = c3; w4 = c4;
                     } else {
-                        float d[3];
-                        d[A] = da; d[B] = db; d[G] = dg;
                         const float dd = fmaf(dg, dg, dab2);
-                        const float q2 = m[q][0] * d[0] * d[0] + m[q][1] * d[1] * d[1] + m[q][2] * d[2] * d[2] +
-                                         m[q][3] * d[0] * d[1] + m[q][4] * d[0] * d[2] + m[q][5] * d[1] * d[2];
+                        const float al = fmaf(m[q][0], daa, fmaf(m[q][1], dbb, m[q][2] * dab));
+                        const float be = fmaf(m[q][3], da, fmaf(m[q][4], db, m[q][5] * dg));
+                        const float q2 = fmaf(dg, be, al);
                         const float pv = val[q] - __fdividef(q2, dd);
                         w1 = __fmul_rn(c1, pv); w2 = __fmul_rn(c2, pv);
                         w3 = __fmul_rn(c3, pv); w4 = __fmul_rn(c4, pv);
@@ -367,6 +383,12 @@ struct BackColArgs {
     const float *coef;        /* non-null: per-voxel rotated basis (backwardOrth) */
 };
 
+/* Shared-memory slot of brick voxel lv (x + 8y + 64z) in the per-voxel
+ * accumulators: lv with bits 5-7 folded into bits 0-2 and bits 6-7 into bits
+ * 3-4, so that for every column axis the 32 lanes of a warp (8 x 4 columns)
+ * and the brick-linear final pass all hit 32 different banks. */
+__device__ __forceinline__ int sacc_slot(int lv) { return lv ^ ((lv >> 5) & 7) ^ (((lv >> 6) & 3) << 3); }
+
 /* One view of one axis for a thread's column segment of 4 voxels: the ray
  * set-up once, then per voxel v, the taps and the 4-tap gather from the
  * (L2-resident) ratio image. */
@@ -417,7 +439,7 @@ __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f
         } else {
             float d[3];
             d[A] = da; d[B] = db; d[G] = dg[q];
-            const float inv = __frcp_rn(fmaf(dg[q], dg[q], dab2));
+            const float inv = __fdividef(1.0f, fmaf(dg[q], dg[q], dab2));   /* approximate reciprocal, ~2 ulp */
             float wgt;
             if (MODE == B_XTT) {
                 acc[q][6] += nb;
@@ -493,7 +515,7 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
         } else {
             int lx, ly, lz;
             xyz_of<G>(ca, cb, sg * 4 + q, lx, ly, lz);
-            const int lv = lx + 8 * ly + 64 * lz;
+            const int lv = sacc_slot(lx + 8 * ly + 64 * lz);
             const BasisConst *Bc = a.basis;
             if (a.coef) {   /* backwardOrth (ir.cu:366-423): the voxel's rotated basis */
                 int x, y, z;
@@ -555,7 +577,7 @@ __global__ void __launch_bounds__(kBackThreads, 4) k_back_col(BackColArgs a) {
         if (x >= N || y >= N || z >= N) continue;
         const size_t idx = (size_t)x + (size_t)N * y + NN * z;
         for (int k = 0; k < K; k++) {
-            const float t = sacc[k * 512 + lv];
+            const float t = sacc[k * 512 + sacc_slot(lv)];
             if (MODE == B_SENS) {
                 a.fac_out[idx + (size_t)k * N3] = t;
             } else {

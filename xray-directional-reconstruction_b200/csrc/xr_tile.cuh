@@ -21,11 +21,29 @@ namespace xr {
 constexpr float kFixLoScale = 2097152.0f;           /* 2^21 */
 constexpr double kFixLoInv = 1.0 / 2097152.0;
 
+/* Rounding to the nearest integer (ties to even) without the conversion
+ * unit: for |x| < 2^22, t = x + 1.5 * 2^23 lies in [2^23, 2^24), where the
+ * float spacing is 1, so the addition itself rounds x, and t's bit pattern
+ * minus that of 1.5 * 2^23 is the integer (the magic-number method). */
+constexpr float kRoundMagic = 12582912.0f;          /* 1.5 * 2^23 */
+constexpr int kRoundMagicBits = 0x4B400000;
+
+/* The two words of one contribution |xs| < 2^20: h = rint(xs) and
+ * l = rint((xs - h) * 2^21), as integers. */
+__device__ __forceinline__ void fix_split(float xs, int &h, int &l) {
+    const float t = __fadd_rn(xs, kRoundMagic);
+    const float hf = __fsub_rn(t, kRoundMagic);
+    h = __float_as_int(t) - kRoundMagicBits;
+    /* (xs - hf) is exact and so is its product with 2^21: one rounding */
+    l = __float_as_int(__fmaf_rn(__fsub_rn(xs, hf), kFixLoScale, kRoundMagic)) - kRoundMagicBits;
+}
+
 /* tile word layout per buffer: [hi: cap ints][lo: cap ints] */
 __device__ __forceinline__ void fix_add(int *hi, int cap, float xs) {
-    const float h = rintf(xs);
-    atomicAdd(hi, (int)h);
-    atomicAdd(hi + cap, __float2int_rn(__fsub_rn(xs, h) * kFixLoScale));
+    int h, l;
+    fix_split(xs, h, l);
+    atomicAdd(hi, h);
+    atomicAdd(hi + cap, l);
 }
 
 /* Reads and clears one pixel's two words; returns the sum unscaled by 2^-sh. */
