@@ -31,8 +31,8 @@
 namespace xr {
 namespace {
 
-constexpr int kTileCap = 48 * 48;
-constexpr int kFwdThreads = 256;               /* forward: 16 (g) x 8 x 8 brick, 4 voxels/thread */
+constexpr int kTileCap = 64 * 64;
+constexpr int kFwdThreads = 512;               /* forward: 16 (g) x 16 x 8 brick, 4 voxels/thread */
 constexpr int kBackThreads = 128;              /* back: 8 x 8 x 8 brick, 4 voxels/thread          */
 constexpr int kFrameChunk = 128;
 
@@ -107,8 +107,8 @@ __device__ __forceinline__ void xyz_of(int ia, int ib, int ig, int &x, int &y, i
 }
 
 /* ------------------------------------------------------------------------ */
-/* Forward splat, column form.  Brick: 16 along g, 8 along a, 8 along b.     */
-/* Warp = 4 segments x 4 (a) x 2 (b) columns; 8 warps tile 8 x 8 columns.    */
+/* Forward splat, column form.  Brick: 16 along g, 16 along a, 8 along b.    */
+/* Warp = 4 segments x 4 (a) x 2 (b) columns; 16 warps tile 16 x 8 columns.  */
 /* ------------------------------------------------------------------------ */
 struct FwdColArgs {
     GeomConst g;
@@ -125,12 +125,12 @@ struct FwdColArgs {
 };
 
 template <int MODE, int G, typename T>
-__global__ void __launch_bounds__(kFwdThreads, 4) k_fwd_col(FwdColArgs a) {
+__global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
     const T *vol = reinterpret_cast<const T *>(a.vol);
     constexpr int A = Ax<G>::A, B = Ax<G>::B;
     /* Two detector tiles (double-buffered over views) in two-word fixed
      * point, xr_tile.cuh: native 32-bit shared atomics, per-CTA sums exact
-     * to 2^-41 of the brick's largest contribution. */
+     * to 2^-39 of the brick's largest contribution. */
     extern __shared__ int smem[];
     __shared__ float s_red[kFwdThreads / 32];
     int4 *bbox = reinterpret_cast<int4 *>(smem + 4 * kTileCap);
@@ -145,8 +145,8 @@ __global__ void __launch_bounds__(kFwdThreads, 4) k_fwd_col(FwdColArgs a) {
     if (nv <= 0) return;
 
     const int brick = blockIdx.x;
-    const int g0 = (brick % a.nbg) * 16, a0 = ((brick / a.nbg) % a.nba) * 8, b0 = (brick / (a.nbg * a.nba)) * 8;
-    const int g1 = min(g0 + 16, N) - 1, a1 = min(a0 + 8, N) - 1, b1 = min(b0 + 8, N) - 1;
+    const int g0 = (brick % a.nbg) * 16, a0 = ((brick / a.nbg) % a.nba) * 16, b0 = (brick / (a.nbg * a.nba)) * 8;
+    const int g1 = min(g0 + 16, N) - 1, a1 = min(a0 + 16, N) - 1, b1 = min(b0 + 8, N) - 1;
 
     const int tid = threadIdx.x;
     for (int i = tid; i < 4 * kTileCap; i += kFwdThreads) smem[i] = 0;
@@ -189,8 +189,8 @@ __global__ void __launch_bounds__(kFwdThreads, 4) k_fwd_col(FwdColArgs a) {
 
     const int lane = tid & 31, w = tid >> 5;
     const int seg = lane & 3;
-    const int ia = a0 + (w & 1) * 4 + ((lane >> 2) & 3);
-    const int ib = b0 + (w >> 1) * 2 + (lane >> 4);
+    const int ia = a0 + (w & 3) * 4 + ((lane >> 2) & 3);
+    const int ib = b0 + (w >> 2) * 2 + (lane >> 4);
     const int igb = g0 + seg * 4;
     const bool col_ok = ia < N && ib < N;
     const float ba = vox_base(ia, N, g.vs), bb = vox_base(ib, N, g.vs);
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(kFwdThreads, 4) k_fwd_col(FwdColArgs a) {
     if (!(S > 0.f) || !(S < 3e38f)) return;      /* nothing to splat (or non-finite input) */
     const int sh = fix_shift(S);
     const float fscale = ldexpf(1.0f, sh);
-    const double finv = ldexp(1.0, -sh);
+    const float finv = ldexpf(1.0f, -sh);
 
     const size_t NdNd = (size_t)Nd * Nd;
     float *outc = a.out + (size_t)cond * g.V * NdNd;
@@ -641,7 +641,7 @@ cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, co
     a.basis = d_basis;
     a.coef = coef;
     a.nbg = (g.N + 15) / 16;
-    a.nba = (g.N + 7) / 8;
+    a.nba = (g.N + 15) / 16;
     const int nbb = (g.N + 7) / 8;
     const long bricks = (long)a.nbg * a.nba * nbb;
     int vpc = views_per_cta;

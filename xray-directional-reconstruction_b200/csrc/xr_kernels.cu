@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kFwdThreads, 3) k_forward(FwdArgs a) {
     if (!(S > 0.f) || !(S < 3e38f)) return;
     const int sh = fix_shift(S);
     const float fscale = ldexpf(1.0f, sh);
-    const double finv = ldexp(1.0, -sh);
+    const float finv = ldexpf(1.0f, -sh);
 
     const size_t NdNd = (size_t)Nd * Nd;
     float *outc = a.out + (size_t)cond * g.V * NdNd;

@@ -3,13 +3,13 @@
  *
  * A 32-bit integer atomicAdd on shared memory is a native instruction, a
  * float (or 64-bit) one runs as a compare-and-swap loop.  Each contribution
- * x, scaled by the CTA's power of two (xs = x * 2^sh, |xs| < 2^20), is split
+ * x, scaled by the CTA's power of two (xs = x * 2^sh, |xs| < 2^19), is split
  * into an integer part h = rint(xs) and a remainder r = xs - h (exact, Sterbenz)
- * kept to 2^-21 in a second word: two native atomics per tap, a per-CTA sum
- * exact to 2^-41 of the CTA's largest contribution, i.e. below the FP32 rounding
- * of every pixel the reference itself accumulates.  With at most 1024
- * contributions per pixel (one tap per voxel of a brick) both words stay below
- * 2^30.  A pixel's relative precision matters: the normalised projection
+ * kept to 2^-20 in a second word: two native atomics per tap, each term of a
+ * per-CTA sum exact to 2^-39 of the CTA's largest contribution, i.e. below the
+ * FP32 rounding of every pixel the reference itself accumulates.  With at most
+ * 2048 contributions per pixel (one tap per voxel of a brick) both words stay
+ * below 2^30.  A pixel's relative precision matters: the normalised projection
  * divides by the weight image, so footprint-edge pixels with small sums are
  * amplified to the scale of the largest ones.
  */
@@ -18,8 +18,8 @@
 
 namespace xr {
 
-constexpr float kFixLoScale = 2097152.0f;           /* 2^21 */
-constexpr double kFixLoInv = 1.0 / 2097152.0;
+constexpr float kFixLoScale = 1048576.0f;           /* 2^20  */
+constexpr float kFixLoInvF = 9.5367431640625e-07f;  /* 2^-20 */
 
 /* Rounding to the nearest integer (ties to even) without the conversion
  * unit: for |x| < 2^22, t = x + 1.5 * 2^23 lies in [2^23, 2^24), where the
@@ -28,13 +28,13 @@ constexpr double kFixLoInv = 1.0 / 2097152.0;
 constexpr float kRoundMagic = 12582912.0f;          /* 1.5 * 2^23 */
 constexpr int kRoundMagicBits = 0x4B400000;
 
-/* The two words of one contribution |xs| < 2^20: h = rint(xs) and
- * l = rint((xs - h) * 2^21), as integers. */
+/* The two words of one contribution |xs| < 2^19: h = rint(xs) and
+ * l = rint((xs - h) * 2^20), as integers. */
 __device__ __forceinline__ void fix_split(float xs, int &h, int &l) {
     const float t = __fadd_rn(xs, kRoundMagic);
     const float hf = __fsub_rn(t, kRoundMagic);
     h = __float_as_int(t) - kRoundMagicBits;
-    /* (xs - hf) is exact and so is its product with 2^21: one rounding */
+    /* (xs - hf) is exact and so is its product with 2^20: one rounding */
     l = __float_as_int(__fmaf_rn(__fsub_rn(xs, hf), kFixLoScale, kRoundMagic)) - kRoundMagicBits;
 }
 
@@ -47,12 +47,12 @@ __device__ __forceinline__ void fix_add(int *hi, int cap, float xs) {
 }
 
 /* Reads and clears one pixel's two words; returns the sum unscaled by 2^-sh. */
-__device__ __forceinline__ bool fix_take(int *hi, int cap, double finv, float &out) {
+__device__ __forceinline__ bool fix_take(int *hi, int cap, float finv, float &out) {
     const int h = *hi, l = hi[cap];
     if ((h | l) == 0) return false;
     *hi = 0;
     hi[cap] = 0;
-    out = (float)(((double)h + (double)l * kFixLoInv) * finv);
+    out = __fmul_rn(__fmaf_rn((float)l, kFixLoInvF, (float)h), finv);
     return true;
 }
 
@@ -60,7 +60,7 @@ __device__ __forceinline__ bool fix_take(int *hi, int cap, double finv, float &o
 __device__ __forceinline__ int fix_shift(float S) {
     int ex;
     frexpf(S, &ex);          /* S < 2^ex */
-    return max(-126, min(126, 20 - ex));
+    return max(-126, min(126, 19 - ex));
 }
 
 }  // namespace xr
