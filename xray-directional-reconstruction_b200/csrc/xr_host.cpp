@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -729,6 +730,9 @@ void xr_destroy(xr_ctx *c) {
     release(c->fdk_sf);
     if (c->h_loss) cudaFreeHost(c->h_loss);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    for (cudaEvent_t e : c->copy_ev)
+        if (e) cudaEventDestroy(e);
     delete c;
 }
 
@@ -945,7 +949,11 @@ xr_status xr_dev_session_epoch(xr_ctx *c, double *loss) {
     return cuda_check(c, cudaGetLastError(), "epoch");
 }
 
-xr_status xr_dev_session_end(xr_ctx *c, float *d_md, float *d_ev) {
+/* Session end; `after` (if set) is called once the volume is final on the
+ * compute stream (phase 0, after the voxelSqrt) and once the orientation is
+ * (phase 1), before the host waits for the stream. */
+static xr_status session_end_impl(xr_ctx *c, float *d_md, float *d_ev,
+                                  const std::function<xr_status(int)> &after) {
     if (!c) return XR_ERR_ARG;
     Session &s = c->sess;
     if (!s.active) return fail(c, XR_ERR_STATE, "no active session");
@@ -956,16 +964,22 @@ xr_status xr_dev_session_end(xr_ctx *c, float *d_md, float *d_ev) {
             Timed t(c, XR_T_ORIENT);
             st = cuda_check(c, launch_sqrt_abs(nvox * c->K, s.d_vol, s.storage, c->stream), "sqrt");   /* reconstruct.cu:919-922 */
         }
+        if (!st && after) st = after(0);
         if (!st && d_md) {
             Timed t(c, XR_T_ORIENT);
             st = cuda_check(c, launch_orientation(nvox, c->K, dbasis(c), s.d_vol, d_md, d_ev, s.storage, c->stream),
                             "orientation");
         }
+        if (!st && after) st = after(1);
     }
-    if (!st) st = cuda_check(c, cudaStreamSynchronize(c->stream), "session end");
+    xr_status st2 = cuda_check(c, cudaStreamSynchronize(c->stream), "session end");
     drop_graphs(c);
     s.active = false;
-    return st;
+    return st ? st : st2;
+}
+
+xr_status xr_dev_session_end(xr_ctx *c, float *d_md, float *d_ev) {
+    return session_end_impl(c, d_md, d_ev, nullptr);
 }
 
 xr_status xr_dev_session_proj(xr_ctx *c, const float **d_proj) {
@@ -1070,15 +1084,32 @@ xr_status xr_dev_orientation(xr_ctx *c, const void *d_mu, float *d_md, float *d_
 
 /* ------------------------------------------------------ host-buffer calls */
 
-static xr_status upload_planes(xr_ctx *c, DevBuf &b, const float *const *src, int planes, size_t plane_elems,
-                               const char *what) {
+static xr_status upload_planes_on(xr_ctx *c, DevBuf &b, const float *const *src, int planes, size_t plane_elems,
+                                  const char *what, cudaStream_t str) {
     for (int i = 0; i < planes; i++)
         if (!src[i]) return fail(c, XR_ERR_ARG, std::string("null host pointer: ") + what);
     xr_status st;
     if ((st = ensure(c, b, (size_t)planes * plane_elems * sizeof(float), what))) return st;
     for (int i = 0; i < planes; i++) {
         st = cuda_check(c, cudaMemcpyAsync((float *)b.p + i * plane_elems, src[i], plane_elems * sizeof(float),
-                                           cudaMemcpyHostToDevice, c->stream), what);
+                                           cudaMemcpyHostToDevice, str), what);
+        if (st) return st;
+    }
+    return XR_OK;
+}
+
+static xr_status upload_planes(xr_ctx *c, DevBuf &b, const float *const *src, int planes, size_t plane_elems,
+                               const char *what) {
+    return upload_planes_on(c, b, src, planes, plane_elems, what, c->stream);
+}
+
+/* Device planes into host planes, enqueued on `str` without waiting. */
+static xr_status download_planes_async(xr_ctx *c, const float *d, float *const *dst, int planes, size_t plane_elems,
+                                       const char *what, cudaStream_t str) {
+    for (int i = 0; i < planes; i++) {
+        if (!dst[i]) return fail(c, XR_ERR_ARG, std::string("null host pointer: ") + what);
+        xr_status st = cuda_check(c, cudaMemcpyAsync(dst[i], d + i * plane_elems, plane_elems * sizeof(float),
+                                                     cudaMemcpyDeviceToHost, str), what);
         if (st) return st;
     }
     return XR_OK;
@@ -1086,35 +1117,62 @@ static xr_status upload_planes(xr_ctx *c, DevBuf &b, const float *const *src, in
 
 static xr_status download_planes(xr_ctx *c, const float *d, float *const *dst, int planes, size_t plane_elems,
                                  const char *what) {
-    for (int i = 0; i < planes; i++) {
-        if (!dst[i]) return fail(c, XR_ERR_ARG, std::string("null host pointer: ") + what);
-        xr_status st = cuda_check(c, cudaMemcpyAsync(dst[i], d + i * plane_elems, plane_elems * sizeof(float),
-                                                     cudaMemcpyDeviceToHost, c->stream), what);
-        if (st) return st;
-    }
+    xr_status st = download_planes_async(c, d, dst, planes, plane_elems, what, c->stream);
+    if (st) return st;
     return cuda_check(c, cudaStreamSynchronize(c->stream), what);
 }
 
 /* Host float planes into `b` in the storage type (through the FP32 staging
  * buffer when the storage is 16-bit), and back. */
-static xr_status upload_planes_s(xr_ctx *c, DevBuf &b, const float *const *src, int planes, size_t plane_elems,
-                                 int storage, const char *what) {
-    if (storage == 0) return upload_planes(c, b, src, planes, plane_elems, what);
+static xr_status upload_planes_s_on(xr_ctx *c, DevBuf &b, const float *const *src, int planes, size_t plane_elems,
+                                    int storage, const char *what, cudaStream_t str) {
+    if (storage == 0) return upload_planes_on(c, b, src, planes, plane_elems, what, str);
     xr_status st;
     const size_t n = (size_t)planes * plane_elems;
-    if ((st = upload_planes(c, c->stage, src, planes, plane_elems, what))) return st;
+    if ((st = upload_planes_on(c, c->stage, src, planes, plane_elems, what, str))) return st;
     if ((st = ensure(c, b, n * storage_bytes(storage), what))) return st;
-    return cuda_check(c, launch_convert((long)n, c->stage.p, 0, b.p, storage, c->stream), what);
+    return cuda_check(c, launch_convert((long)n, c->stage.p, 0, b.p, storage, str), what);
+}
+
+static xr_status upload_planes_s(xr_ctx *c, DevBuf &b, const float *const *src, int planes, size_t plane_elems,
+                                 int storage, const char *what) {
+    return upload_planes_s_on(c, b, src, planes, plane_elems, storage, what, c->stream);
+}
+
+static xr_status download_planes_s_async(xr_ctx *c, const void *d, float *const *dst, int planes,
+                                         size_t plane_elems, int storage, const char *what, cudaStream_t str) {
+    if (storage == 0) return download_planes_async(c, (const float *)d, dst, planes, plane_elems, what, str);
+    xr_status st;
+    const size_t n = (size_t)planes * plane_elems;
+    if ((st = ensure(c, c->stage, n * sizeof(float), what))) return st;
+    if ((st = cuda_check(c, launch_convert((long)n, d, storage, c->stage.p, 0, str), what))) return st;
+    return download_planes_async(c, (const float *)c->stage.p, dst, planes, plane_elems, what, str);
 }
 
 static xr_status download_planes_s(xr_ctx *c, const void *d, float *const *dst, int planes, size_t plane_elems,
                                    int storage, const char *what) {
-    if (storage == 0) return download_planes(c, (const float *)d, dst, planes, plane_elems, what);
+    xr_status st = download_planes_s_async(c, d, dst, planes, plane_elems, storage, what, c->stream);
+    if (st) return st;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), what);
+}
+
+/* The transfer stream and its events (created on first use). */
+static xr_status ensure_copy_stream(xr_ctx *c) {
     xr_status st;
-    const size_t n = (size_t)planes * plane_elems;
-    if ((st = ensure(c, c->stage, n * sizeof(float), what))) return st;
-    if ((st = cuda_check(c, launch_convert((long)n, d, storage, c->stage.p, 0, c->stream), what))) return st;
-    return download_planes(c, (const float *)c->stage.p, dst, planes, plane_elems, what);
+    if (!c->copy_stream &&
+        (st = cuda_check(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate")))
+        return st;
+    for (cudaEvent_t &e : c->copy_ev)
+        if (!e && (st = cuda_check(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")))
+            return st;
+    return XR_OK;
+}
+
+/* Makes `to` wait for the work enqueued on `from` so far. */
+static xr_status stream_after(xr_ctx *c, cudaStream_t to, cudaStream_t from, cudaEvent_t e) {
+    xr_status st = cuda_check(c, cudaEventRecord(e, from), "cudaEventRecord");
+    if (st) return st;
+    return cuda_check(c, cudaStreamWaitEvent(to, e, 0), "cudaStreamWaitEvent");
 }
 
 xr_status xr_forward(xr_ctx *c, const float *const *voxel, float *const *sino, xr_rotate dir, int xtt) {
@@ -1177,10 +1235,26 @@ xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
     if ((st = check_xtt_k(c))) return st;
     if ((st = ensure_device(c))) return st;
     const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
-    if ((st = upload_planes_s(c, c->scratch_sino, sino, c->C, blk, sino_st(c), "sinogram"))) return st;
-    if ((st = upload_planes_s(c, c->scratch_vol, voxel, c->K, N3, c->storage, "volume"))) return st;
+    if ((st = ensure_copy_stream(c))) return st;
+    cudaStream_t cs = c->copy_stream;
+    /* Transfers run on the copy stream beside the compute stream: the uploads
+     * overlap the per-subset sensitivity (geometry only) of the session start,
+     * the downloads the voxelSqrt and the orientation of its end.  Every exit
+     * waits for the copy stream, so no transfer outlives the call. */
+    struct CopyWait {
+        cudaStream_t s;
+        ~CopyWait() { cudaStreamSynchronize(s); }
+    } copy_wait{cs};
+    if ((st = stream_after(c, cs, c->stream, c->copy_ev[0]))) return st;   /* earlier work on the buffers */
+    if ((st = upload_planes_s_on(c, c->scratch_vol, voxel, c->K, N3, c->storage, "volume", cs))) return st;
+    if ((st = upload_planes_s_on(c, c->scratch_sino, sino, c->C, blk, sino_st(c), "sinogram", cs))) return st;
+    if ((st = cuda_check(c, cudaEventRecord(c->copy_ev[1], cs), "cudaEventRecord"))) return st;
     if ((st = xr_dev_session_begin(c, c->scratch_sino.p, c->scratch_vol.p, 1, epoch, batch, dir, method, lambda)))
         return st;
+    if ((st = cuda_check(c, cudaStreamWaitEvent(c->stream, c->copy_ev[1], 0), "cudaStreamWaitEvent"))) {
+        xr_dev_session_end(c, nullptr, nullptr);
+        return st;
+    }
     for (int ep = 0; ep < epoch; ep++) {
         double l = 0;
         if ((st = xr_dev_session_epoch(c, losses ? &l : nullptr))) return st;
@@ -1192,14 +1266,20 @@ xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
         d_md = (float *)c->scratch_md.p;
         d_ev = evalue ? d_md + 3 * N3 : nullptr;
     }
-    if ((st = xr_dev_session_end(c, d_md, d_ev))) return st;
-    if ((st = download_planes_s(c, c->scratch_vol.p, voxel, c->K, N3, c->storage, "volume"))) return st;
-    if ((st = download_planes(c, (const float *)c->proj.p, sino, c->C, blk, "ratio images"))) return st;
-    if (md) {
-        if ((st = download_planes(c, d_md, md, 3, N3, "md"))) return st;
-        if (evalue && (st = download_planes(c, d_ev, evalue, 3, N3, "evalue"))) return st;
-    }
-    return XR_OK;
+    /* the ratio images are final after the last epoch */
+    if ((st = stream_after(c, cs, c->stream, c->copy_ev[0]))) return st;
+    if ((st = download_planes_async(c, (const float *)c->proj.p, sino, c->C, blk, "ratio images", cs))) return st;
+    const void *d_vol = c->scratch_vol.p;
+    auto after = [&](int phase) -> xr_status {
+        xr_status s2 = stream_after(c, cs, c->stream, c->copy_ev[1 + phase]);
+        if (s2) return s2;
+        if (phase == 0) return download_planes_s_async(c, d_vol, voxel, c->K, N3, c->storage, "volume", cs);
+        if (!md) return XR_OK;
+        if ((s2 = download_planes_async(c, d_md, md, 3, N3, "md", cs))) return s2;
+        return evalue ? download_planes_async(c, d_ev, evalue, 3, N3, "evalue", cs) : XR_OK;
+    };
+    if ((st = session_end_impl(c, d_md, d_ev, after))) return st;
+    return cuda_check(c, cudaStreamSynchronize(cs), "downloads");
 }
 
 xr_status xr_orientation(xr_ctx *c, const float *const *mu, float *const *md, float *const *evalue) {

@@ -104,6 +104,8 @@ struct xr_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  /* host-buffer calls: transfers beside the compute stream */
+    cudaEvent_t copy_ev[3] = {nullptr, nullptr, nullptr};
     std::string err;
 
     float sdd = 0, sod = 0, det = 0;
