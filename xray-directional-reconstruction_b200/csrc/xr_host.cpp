@@ -461,6 +461,11 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
             }
             {
                 Timed t(c, XR_T_RATIO);
+                if (s.sino_ready) {
+                    if ((st = cuda_check(c, cudaStreamWaitEvent(str, s.sino_ready, 0), "cudaStreamWaitEvent")))
+                        return st;
+                    s.sino_ready = nullptr;
+                }
                 /* the orientation-parametrised forward is not chord-normalised
                  * (forwardOrth -> projRatio, reconstruct.cu:1086-1099) */
                 if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, s.coef ? nullptr : norm,
@@ -1247,11 +1252,19 @@ xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
     } copy_wait{cs};
     if ((st = stream_after(c, cs, c->stream, c->copy_ev[0]))) return st;   /* earlier work on the buffers */
     if ((st = upload_planes_s_on(c, c->scratch_vol, voxel, c->K, N3, c->storage, "volume", cs))) return st;
-    if ((st = upload_planes_s_on(c, c->scratch_sino, sino, c->C, blk, sino_st(c), "sinogram", cs))) return st;
     if ((st = cuda_check(c, cudaEventRecord(c->copy_ev[1], cs), "cudaEventRecord"))) return st;
+    if ((st = upload_planes_s_on(c, c->scratch_sino, sino, c->C, blk, sino_st(c), "sinogram", cs))) return st;
+    if ((st = cuda_check(c, cudaEventRecord(c->copy_ev[2], cs), "cudaEventRecord"))) return st;
     if ((st = xr_dev_session_begin(c, c->scratch_sino.p, c->scratch_vol.p, 1, epoch, batch, dir, method, lambda)))
         return st;
-    if ((st = cuda_check(c, cudaStreamWaitEvent(c->stream, c->copy_ev[1], 0), "cudaStreamWaitEvent"))) {
+    /* the first subset's forward needs only the volume; its ratio waits for
+     * the sinogram (inside a captured epoch graph the wait comes first) */
+    st = cuda_check(c, cudaStreamWaitEvent(c->stream, c->copy_ev[1], 0), "cudaStreamWaitEvent");
+    if (!st && (c->use_graphs || epoch == 0))
+        st = cuda_check(c, cudaStreamWaitEvent(c->stream, c->copy_ev[2], 0), "cudaStreamWaitEvent");
+    else if (!st)
+        c->sess.sino_ready = c->copy_ev[2];
+    if (st) {
         xr_dev_session_end(c, nullptr, nullptr);
         return st;
     }

@@ -93,6 +93,7 @@ struct Session {
     int sino_storage = 0;             /* measured sinogram           */
     int update_storage = 0;           /* volume, | kStoreStochastic  */
     const float *coef = nullptr;      /* orientation-parametrised XTT: (phi, cos) planes */
+    cudaEvent_t sino_ready = nullptr; /* set: the first ratio launch waits for it (sinogram upload) */
     std::vector<int> order;            /* persistent subset order (XTT)     */
     std::vector<int> ir_orders;        /* C*epochs rows (IR)                */
     std::map<std::vector<int>, cudaGraphExec_t> graphs;  /* per subset order */
