@@ -339,12 +339,6 @@ __global__ void __launch_bounds__(kConvWsThreads) k_conv_ws(const __grid_constan
                         const uint64_t aS = tc::sdesc(tc::smem_u32(ring + slot * L::SLOT), kPlane, kHX * 16);
                         const int jlo = li + 1 - ohi, jhi = li + 1 - olo;
                         const uint32_t Otop = ob + (uint32_t)ohi;   /* output of block jlo */
-                        /* first MMA of the slice: one per block, overwriting the started outputs */
-                        for (int j = jlo; j <= jhi; j++) {
-                            const uint32_t O = Otop - (uint32_t)(j - jlo);
-                            tc::mma_bf16(tmem + (CR - 1 - O % CR) * NP, aS, bS + (uint64_t)(j * (L::BT >> 4)),
-                                         tc::idesc_bf16(128, NP, 0, 0), j < jlo + nf ? 0u : 1u);
-                        }
                         /* the rest: blocks jlo..jw in one MMA, and jw+1..jhi in a second where the
                          * ring wraps between them */
                         const int jw = min(jhi, jlo + (int)(Otop % CR));
@@ -352,6 +346,22 @@ __global__ void __launch_bounds__(kConvWsThreads) k_conv_ws(const __grid_constan
                         const uint64_t bA = bS + (uint64_t)(jlo * (L::BT >> 4)), bB = bS + (uint64_t)((jw + 1) * (L::BT >> 4));
                         const uint32_t iA = tc::idesc_bf16(128, NP * (jw - jlo + 1), 0, 0);
                         const uint32_t iB = tc::idesc_bf16(128, NP * max(1, jhi - jw), 0, 0);
+                        /* first MMA of the slice: it overwrites (accumulate = 0) the blocks of the
+                         * outputs it starts, the top nf; in one or two MMAs where the blocks are
+                         * adjacent, else one per block */
+                        if (jw == jhi) {
+                            const int nb = jhi - jlo + 1;
+                            if (nf > 0) tc::mma_bf16(dA, aS, bA, tc::idesc_bf16(128, NP * nf, 0, 0), 0u);
+                            if (nf < nb)
+                                tc::mma_bf16(dA + nf * NP, aS, bA + (uint64_t)(nf * (L::BT >> 4)),
+                                             tc::idesc_bf16(128, NP * (nb - nf), 0, 0), 1u);
+                        } else {
+                            for (int j = jlo; j <= jhi; j++) {
+                                const uint32_t O = Otop - (uint32_t)(j - jlo);
+                                tc::mma_bf16(tmem + (CR - 1 - O % CR) * NP, aS, bS + (uint64_t)(j * (L::BT >> 4)),
+                                             tc::idesc_bf16(128, NP, 0, 0), j < jlo + nf ? 0u : 1u);
+                            }
+                        }
                         if (jw == jhi) {
 #pragma unroll
                             for (int m = 1; m < 9 * (KP / 16); m++) {
