@@ -116,6 +116,33 @@ class Oracle:
         """calcNormalVectorThreeDirec (ir.cu:856-974): coef and loss updated in place."""
         self._fn("normal_three", dt)(ctypes.byref(self._scan(s)), _p(vol, dt), _p(coef, dt), _p(loss, dt), int(rot))
 
+    def forward_md_view(self, s, cond, n, vol, md, proj, factor, dt=np.float32):
+        """forwardOrthByMD (ir.cu:154-231) of one view; factor accumulates the weights."""
+        self._fn("forward_md_view", dt)(ctypes.byref(self._scan(s)), cond, n, _p(vol, dt), _p(md, dt),
+                                        _p(proj, dt), _p(factor, dt))
+
+    def backward_md_slab(self, s, cond, y, n, proj, md, tmp, factor, dt=np.float32):
+        """backwardOrthByMD (ir.cu:233-292) of slab y, view n."""
+        self._fn("backward_md_slab", dt)(ctypes.byref(self._scan(s)), cond, y, n, _p(proj, dt), _p(md, dt),
+                                         _p(tmp, dt), _p(factor, dt))
+
+    def md_filter_slab(self, s, y, md, out, coef, dt=np.float32):
+        """meanFiltFiberMD (ir.cu:1304-1363) of slab y into out."""
+        c = ctypes.c_float(coef) if dt == np.float32 else ctypes.c_double(coef)
+        self._fn("md_filter_slab", dt)(ctypes.byref(self._scan(s)), int(y), _p(md, dt), _p(out, dt), c)
+
+    def main_direction(self, s, vol, md, iteration, dt=np.float32):
+        """calcMainDirection (ir.cu:624-710): md updated in place."""
+        self._fn("main_direction", dt)(ctypes.byref(self._scan(s)), _p(vol, dt), _p(md, dt), int(iteration))
+
+    def md_with_estimate(self, s, vol, md, est, dt=np.float32):
+        """calcMDWithEst (ir.cu:712-789): md updated in place."""
+        self._fn("md_with_estimate", dt)(ctypes.byref(self._scan(s)), _p(vol, dt), _p(md, dt), _p(est, dt))
+
+    def update_estimation(self, s, vol, est, iteration, dt=np.float32):
+        """updateEstimation (ir.cu:791-844): est (2 planes) updated in place."""
+        self._fn("update_estimation", dt)(ctypes.byref(self._scan(s)), _p(vol, dt), _p(est, dt), int(iteration))
+
     def correlation(self, s, cond, n, proj, factor, dt=np.float32):
         self._fn("correlation", dt)(ctypes.byref(self._scan(s)), cond, n, _p(proj, dt), _p(factor, dt))
 
@@ -243,6 +270,26 @@ class RefHost:
 
     def normal_three(self, vol, coef, loss, rot):
         self.lib.xr_ref_normal_three(_p(vol), _p(coef), _p(loss), int(rot))
+
+    def forward_md(self, cond, n, vol, md, proj, factor):
+        self.lib.xr_ref_forward_md(cond, n, _p(vol), _p(md), _p(proj), _p(factor))
+
+    def backward_md(self, cond, y, n, proj, md, tmp, factor):
+        self.lib.xr_ref_backward_md(cond, y, n, _p(proj), _p(md), _p(tmp), _p(factor))
+
+    def md_filter(self, y, md, out, coef):
+        self.lib.xr_ref_md_filter(int(y), _p(md), _p(out), ctypes.c_float(coef))
+
+    def main_direction(self, vol, md, iteration):
+        loss = np.zeros(self.s.N ** 3, np.float32)
+        self.lib.xr_ref_main_direction(_p(vol), _p(md), _p(loss), int(iteration))
+
+    def md_with_estimate(self, vol, md, est):
+        self.lib.xr_ref_md_with_estimate(_p(vol), _p(md), _p(est))
+
+    def update_estimation(self, vol, md, est, iteration):
+        loss = np.zeros(self.s.N ** 3, np.float32)
+        self.lib.xr_ref_update_estimation(_p(vol), _p(md), _p(loss), _p(est), int(iteration))
 
     def ratio(self, n, proj, sino, art):
         return float(self.lib.xr_ref_ratio(n, _p(proj), _p(sino), int(art)))

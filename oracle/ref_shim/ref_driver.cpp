@@ -132,6 +132,45 @@ void xr_ref_normal_three(float *vol, float *coef, float *loss, int rot) {
         launch2d(g.gridV, g.blockV, calcNormalVectorThreeDirec, vol, coef, y, (const Geometry *)&g.geom, loss, rot);
 }
 
+/* forwardOrthByMD (ir.cu:154-231): one view, every y slab, basis rotated per
+ * voxel by its main direction; the weight image factor is zeroed here first
+ * (reconstruct.cu:1494). */
+void xr_ref_forward_md(int cond, int n, float *vol, const float *md, float *proj, float *factor) {
+    Geometry *geom = &g.geom;
+    std::memset(factor, 0, sizeof(float) * geom->detect * geom->detect);
+    for (int y = 0; y < geom->voxel; y++)
+        launch2d(g.gridV, g.blockV, forwardOrthByMD, proj, factor, (const float *)vol, md, geom, cond, 0, n, y);
+}
+
+/* backwardOrthByMD (ir.cu:233-292): slab y, view n. */
+void xr_ref_backward_md(int cond, int y, int n, const float *proj, const float *md, float *tmp, float *factor) {
+    launch2d(g.gridV, g.blockV, backwardOrthByMD, proj, md, tmp, factor, (const Geometry *)&g.geom, cond, y, n, 0);
+}
+
+/* meanFiltFiberMD (ir.cu:1304-1363), slab y into out. */
+void xr_ref_md_filter(int y, const float *md, float *out, float coef) {
+    launch2d(g.gridV, g.blockV, meanFiltFiberMD, md, out, (const Geometry *)&g.geom, y, coef);
+}
+
+/* calcMainDirection (ir.cu:624-710), every y slab; loss is the unused
+ * norm_loss argument (N^3 floats). */
+void xr_ref_main_direction(float *vol, float *md, float *loss, int iter) {
+    for (int y = 0; y < g.geom.voxel; y++)
+        launch2d(g.gridV, g.blockV, calcMainDirection, vol, md, y, (const Geometry *)&g.geom, loss, iter);
+}
+
+/* calcMDWithEst (ir.cu:712-789), every y slab. */
+void xr_ref_md_with_estimate(float *vol, float *md, const float *est) {
+    for (int y = 0; y < g.geom.voxel; y++)
+        launch2d(g.gridV, g.blockV, calcMDWithEst, vol, md, y, (const Geometry *)&g.geom, est);
+}
+
+/* updateEstimation (ir.cu:791-844), every y slab. */
+void xr_ref_update_estimation(const float *vol, float *md, float *loss, float *est, int iter) {
+    for (int y = 0; y < g.geom.voxel; y++)
+        launch2d(g.gridV, g.blockV, updateEstimation, vol, md, y, (const Geometry *)&g.geom, loss, est, iter);
+}
+
 void xr_ref_correlation(int cond, int n, float *proj, const float *factor) {
     launch2d(g.gridD, g.blockD, correlationProjByLength, proj, factor, &g.geom, cond, n);
 }

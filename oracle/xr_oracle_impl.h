@@ -432,6 +432,184 @@ void RV(normal_three)(const or_scan *s, const real *vol, real *coef, real *loss,
     }
 }
 
+/* The per-voxel rotation by main direction (forwardOrthByMD ir.cu:183-189,
+ * backwardOrthByMD :262-268, calcMainDirection :693-700): md planes
+ * (m0, m1, m2) -> rodrigues(-m1, m0, 0, m2 / |m|, sqrt(m0^2 + m1^2) / |m|). */
+static void RV(md_rotation)(const real *md, long N3, long idx, real *R) {
+    const real m0 = md[idx], m1 = md[N3 + idx], m2 = md[2 * N3 + idx];
+    RV(rodrigues)(-m1, m0, (real)0, m2 / RSQRT(m0 * m0 + m1 * m1 + m2 * m2),
+                  RSQRT(m0 * m0 + m1 * m1) / RSQRT(m0 * m0 + m1 * m1 + m2 * m2), R);
+}
+
+/* forwardOrthByMD, ir.cu:154-231: one view over every y slab with each
+ * voxel's basis rotated by its main direction, accumulating the weight image
+ * like forwardProjXTT; unlike the other forwards it applies no vs * ratio
+ * factor (ir.cu:180-181 computes the ratio and never uses it). */
+void RV(forward_md_view)(const or_scan *s, int cond, int n, const real *vol, const real *md, real *proj,
+                         real *factor) {
+    RV(frame) f;
+    RV(view_frame)(s, cond, n, 0, &f);
+    const long N = s->N, Nd = s->Nd, N3 = N * N * N;
+    const long nn = n < 0 ? -n : n;
+    real G[3];
+    { const real bz[3] = {(real)0, (real)0, (real)1}; RV(mat3vec)(f.R, bz, G); }
+    for (long y = 0; y < N; y++)
+        for (long z = 0; z < N; z++)
+            for (long x = 0; x < N; x++) {
+                real u, v, B[3], c[4], R[9];
+                long iu, iv;
+                RV(raycast)(s, &f, 0, (int)x, (int)y, (int)z, &u, &v, B, 0);
+                if (!RV(taps)(s, u, v, &iu, &iv, c)) continue;
+                const long idx = x + N * y + N * N * z;
+                RV(md_rotation)(md, N3, idx, R);
+                real pr = (real)0;
+                for (int k = 0; k < s->K; k++) {
+                    const real S0[3] = {(real)s->basis[3 * k], (real)s->basis[3 * k + 1], (real)s->basis[3 * k + 2]};
+                    real S[3];
+                    RV(mat3vec)(R, S0, S);
+                    pr += RV(xtt_weight)(B, S, G) * vol[idx + (long)k * N3];
+                }
+                const long base = Nd * Nd * nn;
+                proj[iu + Nd * (iv + 1) + base] += c[0] * pr;
+                proj[(iu + 1) + Nd * (iv + 1) + base] += c[1] * pr;
+                proj[(iu + 1) + Nd * iv + base] += c[2] * pr;
+                proj[iu + Nd * iv + base] += c[3] * pr;
+                factor[iu + Nd * (iv + 1)] += c[0];
+                factor[(iu + 1) + Nd * (iv + 1)] += c[1];
+                factor[(iu + 1) + Nd * iv] += c[2];
+                factor[iu + Nd * iv] += c[3];
+            }
+}
+
+/* backwardOrthByMD, ir.cu:233-292: backward_orth_slab with the rotation by
+ * main direction. */
+void RV(backward_md_slab)(const or_scan *s, int cond, int y, int n, const real *proj, const real *md, real *tmp,
+                          real *factor) {
+    RV(frame) f;
+    RV(view_frame)(s, cond, n, 0, &f);
+    const long N = s->N, Nd = s->Nd, N3 = N * N * N;
+    const long nn = n < 0 ? -n : n;
+    real G[3];
+    { const real bz[3] = {(real)0, (real)0, (real)1}; RV(mat3vec)(f.R, bz, G); }
+    for (long z = 0; z < N; z++)
+        for (long x = 0; x < N; x++) {
+            real u, v, B[3], c[4], R[9];
+            long iu, iv;
+            RV(raycast)(s, &f, 0, (int)x, y, (int)z, &u, &v, B, 0);
+            if (!RV(taps)(s, u, v, &iu, &iv, c)) continue;
+            RV(md_rotation)(md, N3, x + N * y + N * N * z, R);
+            const long base = Nd * Nd * nn;
+            const real p0 = proj[iu + Nd * (iv + 1) + base], p1 = proj[(iu + 1) + Nd * (iv + 1) + base];
+            const real p2 = proj[(iu + 1) + Nd * iv + base], p3 = proj[iu + Nd * iv + base];
+            const long idx = x + N * z;
+            for (int k = 0; k < s->K; k++) {
+                const real S0[3] = {(real)s->basis[3 * k], (real)s->basis[3 * k + 1], (real)s->basis[3 * k + 2]};
+                real S[3];
+                RV(mat3vec)(R, S0, S);
+                const real w = RV(xtt_weight)(B, S, G);
+                const real bf = w * c[0] * p0 + w * c[1] * p1 + w * c[2] * p2 + w * c[3] * p3;
+                factor[idx + (long)k * N * N] += w;
+                tmp[idx + (long)k * N * N] += bf;
+            }
+        }
+}
+
+/* meanFiltFiberMD, ir.cu:1304-1363, on slab y (2 <= y < N-2, as the driver
+ * reconstruct.cu:1458-1461 calls it) for 2 <= x, z < N-2: the 27 neighbours
+ * signed by their agreement with the centre (dot > 0 added, < 0 subtracted,
+ * weight coef), normalised (zero -> e_z), scaled to the centre's length. */
+void RV(md_filter_slab)(const or_scan *s, int y, const real *md, real *out, real coef) {
+    const long N = s->N, N3 = N * N * N;
+    for (long z = 2; z < N - 2; z++)
+        for (long x = 2; x < N - 2; x++) {
+            const long c = x + N * y + N * N * z;
+            const real c0 = md[c], c1 = md[N3 + c], c2 = md[2 * N3 + c];
+            real nv[3] = {(real)0, (real)0, (real)0};
+            const real len = RSQRT(c0 * c0 + c1 * c1 + c2 * c2);
+            for (int i = -1; i < 2; i++)
+                for (int j = -1; j < 2; j++)
+                    for (int k = -1; k < 2; k++) {
+                        const long o = (x - i) + N * (y - j) + N * N * (z - k);
+                        const real o0 = md[o], o1 = md[N3 + o], o2 = md[2 * N3 + o];
+                        const real d = c0 * o0 + c1 * o1 + c2 * o2;
+                        if (d > (real)0) {
+                            nv[0] = nv[0] + coef * o0; nv[1] = nv[1] + coef * o1; nv[2] = nv[2] + coef * o2;
+                        } else if (d < -(real)0) {
+                            nv[0] = nv[0] - coef * o0; nv[1] = nv[1] - coef * o1; nv[2] = nv[2] - coef * o2;
+                        }
+                    }
+            RV(normalize3)(nv);
+            if (RSQRT(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]) < (real)1e-8f) {
+                nv[0] = (real)0; nv[1] = (real)0; nv[2] = (real)1;
+            }
+            out[c] = len * nv[0];
+            out[N3 + c] = len * nv[1];
+            out[2 * N3 + c] = len * nv[2];
+        }
+}
+
+/* The main direction shared by calcMainDirection (ir.cu:624-710) and
+ * calcMDWithEst (:712-789) for voxel i: from mu (planes 0..2) the in-plane
+ * magnitudes (fx, fy, fz) after removing the (+-1, +-1, +-1) component,
+ * signed by `sgn` (0: none, 1: -fx, 2: -fx -fy, 3: -fy), times half the sum
+ * of mu, rotated by the voxel's previous md and turned to z >= 0. */
+static void RV(main_direction_voxel)(const real *vol, real *md, long N3, long i, int sgn) {
+    const real mu0 = vol[i], mu1 = vol[N3 + i], mu2 = vol[2 * N3 + i];
+    real n0 = (real)0, n1 = (real)0, n2 = (real)0;
+    if (mu2 + mu1 - mu0 < (real)0) { n0 = -(real)1; n1 = (real)1; n2 = (real)1; }
+    else if (mu0 + mu2 - mu1 < (real)0) { n0 = (real)1; n1 = -(real)1; n2 = (real)1; }
+    else if (mu1 + mu0 - mu2 < (real)0) { n0 = (real)1; n1 = (real)1; n2 = -(real)1; }
+    const real co = (mu0 * n0 + mu1 * n1 + mu2 * n2) / (real)3.f;
+    const real v0 = mu0 - co * n0, v1 = mu1 - co * n1, v2 = mu2 - co * n2;
+    real fx = RSQRT((real)0.5f * RFABS(v2 + v1 - v0)), fy = RSQRT((real)0.5f * RFABS(v0 + v2 - v1));
+    const real fz = RSQRT((real)0.5f * RFABS(v1 + v0 - v2));
+    if (sgn == 1) fx = -fx;
+    else if (sgn == 2) { fx = -fx; fy = -fy; }
+    else if (sgn == 3) fy = -fy;
+    const real mean = (mu0 + mu1 + mu2) / (real)2.0f;
+    const real m[3] = {mean * fx, mean * fy, mean * fz};
+    real R[9], r[3];
+    RV(md_rotation)(md, N3, i, R);
+    RV(mat3vec)(R, m, r);
+    if (r[2] < (real)0) { r[0] = -r[0]; r[1] = -r[1]; r[2] = -r[2]; }
+    md[i] = r[0];
+    md[N3 + i] = r[1];
+    md[2 * N3 + i] = r[2];
+}
+
+/* calcMainDirection, ir.cu:624-710, every voxel (sign pattern = iter). */
+void RV(main_direction)(const or_scan *s, const real *vol, real *md, int iter) {
+    const long N3 = (long)s->N * s->N * s->N;
+    for (long i = 0; i < N3; i++) RV(main_direction_voxel)(vol, md, N3, i, iter);
+}
+
+/* calcMDWithEst, ir.cu:712-789: the sign pattern of each voxel from its
+ * estimate plane 1 (< 0.5, < 1.5, < 2.5, else). */
+void RV(md_with_estimate)(const or_scan *s, const real *vol, real *md, const real *est) {
+    const long N3 = (long)s->N * s->N * s->N;
+    for (long i = 0; i < N3; i++) {
+        const real rot = est[N3 + i];
+        const int sgn = rot < (real)0.5f ? 0 : (rot < (real)1.50f ? 1 : (rot < (real)2.50f ? 2 : 3));
+        RV(main_direction_voxel)(vol, md, N3, i, sgn);
+    }
+}
+
+/* updateEstimation, ir.cu:791-844: loss = mu2^2 + (1 - lo/hi)^2 of the first
+ * two channels; where it beats estimate plane 0, planes 0/1 <- (loss, iter). */
+void RV(update_estimation)(const or_scan *s, const real *vol, real *est, int iter) {
+    const long N3 = (long)s->N * s->N * s->N;
+    for (long i = 0; i < N3; i++) {
+        const real mu0 = vol[i], mu1 = vol[N3 + i], mu2 = vol[2 * N3 + i];
+        real lo, hi;
+        if (mu0 < mu1) { lo = mu0; hi = mu1; } else { lo = mu1; hi = mu0; }
+        const real loss = mu2 * mu2 + ((real)1.0f - lo / hi) * ((real)1.0f - lo / hi);
+        if (loss < est[i]) {
+            est[i] = loss;
+            est[N3 + i] = (real)iter;
+        }
+    }
+}
+
 /* voxelProduct (ir.cu:1637-1654, MLEM) or voxelPlus (ir.cu:1682-1693, ART)
  * on slab y of one channel. */
 void RV(voxel_update)(const or_scan *s, int y, real *vol, const real *tmp, const real *factor, int art,
