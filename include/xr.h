@@ -244,6 +244,41 @@ xr_status xr_dev_session_begin_orth(xr_ctx *ctx, const void *d_sino, void *d_vol
  * place, d_loss (N^3) receives |(R e_z) x n|; rot in 0..3 picks the signs. */
 xr_status xr_orth_normal_update(xr_ctx *ctx, const float *d_vol, float *d_coef, float *d_loss, int rot);
 
+/* ---- main-direction XTT (circleEstReconstruct, reconstruct.cu:1373-1649) -- */
+/* The XTT operators with every voxel's basis rotated by its main direction
+ * m (d_md: three planes m_x, m_y, m_z of N^3 floats, FP32): about (-m_y, m_x, 0)
+ * by the angle of cosine m_z / |m| (identity where m_x = m_y = 0).  The
+ * forward is forwardOrthByMD (ir.cu:154-231) followed by the chord-length
+ * normalisation (correlationProjByLength, reconstruct.cu:1505-1506); like the
+ * reference it carries no vs * ratio factor. */
+xr_status xr_dev_forward_md(xr_ctx *ctx, const void *d_vol, const float *d_md, float *d_sino, xr_rotate dir);
+/* An XTT session (xr_dev_session_epoch / _end as usual) of circleEstReconstruct's
+ * inner epochs (reconstruct.cu:1486-1543): forwardOrthByMD -> normalisation ->
+ * projRatio / projSubtract, backwardOrthByMD -> voxelProduct / voxelPlus; the
+ * main direction stays fixed during the session.  Subset order as
+ * xr_dev_session_begin_orth. */
+xr_status xr_dev_session_begin_md(xr_ctx *ctx, const void *d_sino, void *d_vol, const float *d_md, int epochs,
+                                  int batch, xr_rotate dir, xr_method method, float lambda);
+/* meanFiltFiberMD (ir.cu:1304-1363), `passes` times: each voxel with
+ * 2 <= x, y, z < N-2 becomes the sum of its 27 neighbours signed by their
+ * agreement with it (weight `weight`), normalised (zero -> e_z) and scaled
+ * to its own length; d_tmp (3 N^3 floats) is scratch.  The outer two-voxel
+ * border keeps its values (the reference copies its uninitialised scratch
+ * there, reconstruct.cu:1462). */
+xr_status xr_md_filter(xr_ctx *ctx, float *d_md, float *d_tmp, float weight, int passes);
+/* calcMainDirection (ir.cu:624-710): d_md <- main direction of the three
+ * coefficients d_vol (FP32, K >= 3) with sign pattern iter (0..3), turned by
+ * the previous d_md. */
+xr_status xr_md_main_direction(xr_ctx *ctx, const float *d_vol, float *d_md, int iter);
+/* calcMDWithEst (ir.cu:712-789): as xr_md_main_direction with each voxel's
+ * sign pattern from plane 1 of d_est (2 N^3 floats: loss, pattern). */
+xr_status xr_md_with_estimate(xr_ctx *ctx, const float *d_vol, float *d_md, const float *d_est);
+/* updateEstimation (ir.cu:791-844): where mu_2^2 + (1 - lo/hi)^2 of the
+ * coefficients is below d_est plane 0, planes 0 / 1 <- (that loss, iter). */
+xr_status xr_md_update_estimation(xr_ctx *ctx, const float *d_vol, float *d_est, int iter);
+/* fillVolume (ir.cu:846-854): n device floats <- value. */
+xr_status xr_dev_fill(xr_ctx *ctx, float *d, size_t n, float value);
+
 /* ---- regularisers (solver/, reconstruct/src/quadfilt.cpp) --------------- */
 /* totalVariationMinimized(vol, rho, lambda, iter), solver/src/tvmin.cpp:6-98:
  * anisotropic TV denoising by ADMM of a device volume (nx*ny*nz floats, x

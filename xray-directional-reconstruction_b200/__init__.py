@@ -149,6 +149,15 @@ _SIGS = {
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float], ctypes.c_int),
     "xr_orth_normal_update": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int],
                               ctypes.c_int),
+    "xr_dev_forward_md": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int],
+                          ctypes.c_int),
+    "xr_dev_session_begin_md": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                 ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float], ctypes.c_int),
+    "xr_md_filter": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_int], ctypes.c_int),
+    "xr_md_main_direction": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "xr_md_with_estimate": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "xr_md_update_estimation": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "xr_dev_fill": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_float], ctypes.c_int),
     "xr_tv_minimize": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                         ctypes.c_float, ctypes.c_int], ctypes.c_int),
     "xr_quad_form_filter": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
@@ -484,6 +493,42 @@ class Context:
         """calcNormalVectorThreeDirec (ir.cu:856-974) on device buffers."""
         self._check(lib().xr_orth_normal_update(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_coef),
                                                 ctypes.c_void_p(d_loss), int(rot)))
+
+    def dev_forward_md(self, d_vol: int, d_md: int, d_sino: int, rotate=Rotate.CW):
+        """forwardOrthByMD + chord normalisation over every axis and view (ir.cu:154-231)."""
+        self._check(lib().xr_dev_forward_md(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_md),
+                                            ctypes.c_void_p(d_sino), int(rotate)))
+
+    def dev_session_begin_md(self, d_sino: int, d_vol: int, d_md: int, epochs: int, batch: int,
+                             rotate=Rotate.CW, method=Method.MLEM, lam=1e-2):
+        """Main-direction XTT session (circleEstReconstruct's inner epochs)."""
+        self._check(lib().xr_dev_session_begin_md(self._h, ctypes.c_void_p(d_sino), ctypes.c_void_p(d_vol),
+                                                  ctypes.c_void_p(d_md), int(epochs), int(batch), int(rotate),
+                                                  int(method), float(lam)))
+
+    def md_filter(self, d_md: int, d_tmp: int, weight: float = 1.0, passes: int = 1):
+        """meanFiltFiberMD (ir.cu:1304-1363), `passes` times, on device planes."""
+        self._check(lib().xr_md_filter(self._h, ctypes.c_void_p(d_md), ctypes.c_void_p(d_tmp), float(weight),
+                                       int(passes)))
+
+    def md_main_direction(self, d_vol: int, d_md: int, iteration: int = 0):
+        """calcMainDirection (ir.cu:624-710)."""
+        self._check(lib().xr_md_main_direction(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_md),
+                                               int(iteration)))
+
+    def md_with_estimate(self, d_vol: int, d_md: int, d_est: int):
+        """calcMDWithEst (ir.cu:712-789)."""
+        self._check(lib().xr_md_with_estimate(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_md),
+                                              ctypes.c_void_p(d_est)))
+
+    def md_update_estimation(self, d_vol: int, d_est: int, iteration: int):
+        """updateEstimation (ir.cu:791-844)."""
+        self._check(lib().xr_md_update_estimation(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_est),
+                                                  int(iteration)))
+
+    def dev_fill(self, d: int, n: int, value: float):
+        """fillVolume (ir.cu:846-854): n device floats <- value."""
+        self._check(lib().xr_dev_fill(self._h, ctypes.c_void_p(d), ctypes.c_size_t(n), float(value)))
 
     def dev_session_epoch(self, want_loss: bool = False):
         if not want_loss:

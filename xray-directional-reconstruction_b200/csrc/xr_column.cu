@@ -120,7 +120,8 @@ struct FwdColArgs {
     const void *vol;          /* storage type T                              */
     float *out;
     const BasisConst *basis;
-    const float *coef;        /* mode 3: per-voxel rotation planes (phi, cos) */
+    const float *coef;        /* mode 3: per-voxel rotation planes           */
+    int coef_kind;            /* 0: (phi, cos theta); 1: main direction      */
     int nbg, nba;             /* bricks along g and a                        */
 };
 
@@ -219,7 +220,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
         } else if (MODE == 2) {
             val[q] = 1.0f;
         } else if (MODE == 3) {   /* XTT with the voxel's rotated basis (forwardOrth, ir.cu:294-364) */
-            orth_moments<T>(a.basis, cond, g.K, __fmul_rn(g.vs, g.ratio), vol, a.coef, idx, N3, val[q], m[q]);
+            orth_moments<T>(a.basis, cond, g.K, a.coef_kind ? 1.0f : __fmul_rn(g.vs, g.ratio), vol, a.coef,
+                            a.coef_kind, idx, N3, val[q], m[q]);
         } else {
             const BasisConst *Bc = a.basis;
             const float sc = __fmul_rn(g.vs, g.ratio);
@@ -381,6 +383,7 @@ struct BackColArgs {
     float alpha;
     int sr;                   /* 16-bit volumes: stochastic rounding of updates */
     const float *coef;        /* non-null: per-voxel rotated basis (backwardOrth) */
+    int coef_kind;            /* 0: (phi, cos theta); 1: main direction            */
 };
 
 /* Shared-memory slot of brick voxel lv (x + 8y + 64z) in the per-voxel
@@ -517,11 +520,11 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
             xyz_of<G>(ca, cb, sg * 4 + q, lx, ly, lz);
             const int lv = sacc_slot(lx + 8 * ly + 64 * lz);
             const BasisConst *Bc = a.basis;
-            if (a.coef) {   /* backwardOrth (ir.cu:366-423): the voxel's rotated basis */
+            if (a.coef) {   /* backwardOrth(ByMD) (ir.cu:366-423, :233-292): the voxel's rotated basis */
                 int x, y, z;
                 xyz_of<G>(ia, ib, igb + q, x, y, z);
                 float R[9];
-                orth_rotation(a.coef, NN * N, (size_t)x + (size_t)N * y + NN * z, R);
+                src_rotation(a.coef, a.coef_kind, NN * N, (size_t)x + (size_t)N * y + NN * z, R);
                 const float G0 = Bc->G[3 * cond], G1 = Bc->G[3 * cond + 1], G2 = Bc->G[3 * cond + 2];
                 for (int k = 0; k < K; k++) {
                     float S[3];
@@ -626,10 +629,11 @@ cudaError_t check_exact_rdet(float det, float rdet, unsigned *d_flag, unsigned *
 cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, const int *d_conds, int n_cond, int G,
                                const float *d_magsig, const void *vol, float *out, int mode, int views_per_cta,
-                               int storage, cudaStream_t s, const float *coef) {
+                               int storage, cudaStream_t s, const float *coef, int coef_kind) {
     if (n_views <= 0 || n_cond <= 0) return cudaSuccess;
     if (coef && mode == 1) mode = 3;
     FwdColArgs a;
+    a.coef_kind = coef_kind;
     a.g = g;
     a.frames = frames;
     a.view_list = view_list;
@@ -689,9 +693,11 @@ cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, co
 cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                             const int *view_list, int n_views, const int *d_conds, int n_cond, const int *d_axis_g,
                             const float *d_magsig, const float *proj, void *vol, const float *fac_in, float *fac_out,
-                            int mode, int art, float alpha, int storage, cudaStream_t s, const float *coef) {
+                            int mode, int art, float alpha, int storage, cudaStream_t s, const float *coef,
+                            int coef_kind) {
     BackColArgs a;
     a.coef = coef;
+    a.coef_kind = coef_kind;
     a.sr = (storage & kStoreStochastic) != 0;
     storage &= ~kStoreStochastic;
     a.g = g;

@@ -285,7 +285,7 @@ static const ColInfo *dcol(xr_ctx *c) { return (const ColInfo *)c->colinfo.p; }
  * vol is the channel base (plain: the axis's own volume when one axis). */
 static cudaError_t forward_dispatch(xr_ctx *c, const int *vl, int n_views, const std::vector<int> &conds,
                                     const void *vol, float *out, int mode, int storage,
-                                    const float *coef = nullptr) {
+                                    const float *coef = nullptr, int coef_kind = 0) {
     const ViewFrame *fr = (const ViewFrame *)c->frames.p;
     const ColInfo *ci = dcol(c);
     std::vector<int> grp[3];
@@ -293,7 +293,7 @@ static cudaError_t forward_dispatch(xr_ctx *c, const int *vl, int n_views, const
         const int g = c->axis_g[cond];
         if (g < 0) {
             cudaError_t e = launch_forward(c->gc, dbasis(c), fr, vl, n_views, cond, 1, vol, out, mode,
-                                           c->views_per_cta, storage, c->stream, coef);
+                                           c->views_per_cta, storage, c->stream, coef, coef_kind);
             if (e != cudaSuccess) return e;
         } else {
             grp[g].push_back(cond);
@@ -311,14 +311,14 @@ static cudaError_t forward_dispatch(xr_ctx *c, const int *vl, int n_views, const
                 for (int cond : grp[g]) {
                     cudaError_t e = launch_forward_col(c->gc, dbasis(c), fr, vl, n_views, &ci->all[cond], 1, g,
                                                        ci->magsig, vol, out, mode, c->views_per_cta, storage,
-                                                       c->stream, coef);
+                                                       c->stream, coef, coef_kind);
                     if (e != cudaSuccess) return e;
                 }
                 continue;
             }
         }
         cudaError_t e = launch_forward_col(c->gc, dbasis(c), fr, vl, n_views, dl, (int)grp[g].size(), g, ci->magsig,
-                                           vol, out, mode, c->views_per_cta, storage, c->stream, coef);
+                                           vol, out, mode, c->views_per_cta, storage, c->stream, coef, coef_kind);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -456,7 +456,7 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
             {
                 Timed t(c, XR_T_FORWARD);
                 if ((st = cuda_check(c, forward_dispatch(c, vl, s.subset_size, all_conds(c), s.d_vol, proj, 1,
-                                                         s.storage, s.coef), "XTT forward")))
+                                                         s.storage, s.coef, s.coef_kind), "XTT forward")))
                     return st;
             }
             {
@@ -466,9 +466,11 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                         return st;
                     s.sino_ready = nullptr;
                 }
-                /* the orientation-parametrised forward is not chord-normalised
-                 * (forwardOrth -> projRatio, reconstruct.cu:1086-1099) */
-                if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, s.coef ? nullptr : norm,
+                /* the (phi, cos theta) forward is not chord-normalised (forwardOrth ->
+                 * projRatio, reconstruct.cu:1086-1099); the main-direction one is
+                 * (forwardOrthByMD -> correlationProjByLength, reconstruct.cu:1501-1509) */
+                const float *nrm = (s.coef && s.coef_kind == 0) ? nullptr : norm;
+                if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, nrm,
                                                      s.d_sino, s.art, dl, s.sino_storage, str), "ratio")))
                     return st;
             }
@@ -481,10 +483,10 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                         s.art ? nullptr : (const float *)c->sens.p + (size_t)orders[b] * c->K * N3;
                     e = launch_back_col(c->gc, dbasis(c), fr, vl, s.subset_size, ci->all, c->C, ci->axis_g,
                                         ci->magsig, proj, s.d_vol, sens, nullptr, 1, s.art, alpha, s.update_storage,
-                                        str, s.coef);
+                                        str, s.coef, s.coef_kind);
                 } else {
                     e = launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, 0, c->C, proj, s.d_vol, 1, s.art,
-                                           alpha, s.update_storage, str, s.coef);
+                                           alpha, s.update_storage, str, s.coef, s.coef_kind);
                 }
                 if ((st = cuda_check(c, e, "XTT back"))) return st;
             }
@@ -829,7 +831,8 @@ xr_status xr_reset_timings(xr_ctx *c) {
 /* ------------------------------------------------------------- sessions */
 
 static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, int xtt, int epochs, int batch,
-                                    xr_rotate dir, xr_method method, float lambda, const float *coef) {
+                                    xr_rotate dir, xr_method method, float lambda, const float *coef,
+                                    int coef_kind = 0) {
     if (!c || !d_sino || !d_vol) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
     if (batch < 1 || batch > c->V) return fail(c, XR_ERR_ARG, "batch must be in [1, num_proj]");
     if (method != XR_METHOD_MLEM && method != XR_METHOD_ART && method != XR_METHOD_XTT)
@@ -857,6 +860,7 @@ static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, 
     s.sino_storage = sino_st(c);
     s.update_storage = s.storage | ((c->stochastic && s.storage != 0) ? kStoreStochastic : 0);
     s.coef = coef;
+    s.coef_kind = coef_kind;
     std::vector<int> lists((size_t)batch * s.subset_size);
     for (int sub = 0; sub < batch; sub++)
         for (int j = 0; j < s.subset_size; j++)   /* n = (sub + batch*j) % nProj, reconstruct.cu:89 */
@@ -892,7 +896,7 @@ static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, 
                                                (const int *)c->subsets.p + (size_t)sub * s.subset_size, s.subset_size,
                                                ci->all, c->C, ci->axis_g, ci->magsig, nullptr, nullptr, nullptr,
                                                (float *)c->sens.p + (size_t)sub * c->K * N3, 2, 0, 0.f, 0, c->stream,
-                                               coef),
+                                               coef, coef_kind),
                             "sensitivity");
             if (st) return st;
         }
@@ -912,6 +916,12 @@ xr_status xr_dev_session_begin_orth(xr_ctx *c, const void *d_sino, void *d_vol, 
                                     int batch, xr_rotate dir, xr_method method, float lambda) {
     if (!c || !d_coef) return c ? fail(c, XR_ERR_ARG, "null coefficient planes") : XR_ERR_ARG;
     return session_begin_impl(c, d_sino, d_vol, 1, epochs, batch, dir, method, lambda, d_coef);
+}
+
+xr_status xr_dev_session_begin_md(xr_ctx *c, const void *d_sino, void *d_vol, const float *d_md, int epochs,
+                                  int batch, xr_rotate dir, xr_method method, float lambda) {
+    if (!c || !d_md) return c ? fail(c, XR_ERR_ARG, "null main-direction planes") : XR_ERR_ARG;
+    return session_begin_impl(c, d_sino, d_vol, 1, epochs, batch, dir, method, lambda, d_md, 1);
 }
 
 xr_status xr_dev_session_epoch(xr_ctx *c, double *loss) {
@@ -996,7 +1006,7 @@ xr_status xr_dev_session_proj(xr_ctx *c, const float **d_proj) {
 /* ---------------------------------------------------- device-buffer calls */
 
 static xr_status forward_into(xr_ctx *c, const void *d_vol, float *d_out, int rotation, int mode, bool normalise,
-                              int storage, const float *coef = nullptr) {
+                              int storage, const float *coef = nullptr, int coef_kind = 0) {
     xr_status st;
     if ((st = ensure_frames(c, rotation))) return st;
     const size_t npx = (size_t)c->C * c->V * c->Nd * c->Nd;
@@ -1009,7 +1019,7 @@ static xr_status forward_into(xr_ctx *c, const void *d_vol, float *d_out, int ro
     {
         Timed t(c, XR_T_FORWARD);
         st = cuda_check(c, forward_dispatch(c, (const int *)lst.p, c->V, all_conds(c), d_vol, d_out, mode, storage,
-                                            coef),
+                                            coef, coef_kind),
                         "forward");
     }
     if (!st && normalise) {
@@ -1027,6 +1037,67 @@ xr_status xr_dev_forward_orth(xr_ctx *c, const void *d_vol, const float *d_coef,
     if ((st = check_xtt_k(c))) return st;
     if ((st = ensure_device(c))) return st;
     return forward_into(c, d_vol, d_sino, dir == XR_ROTATE_CCW ? -1 : 1, 1, false, c->storage, d_coef);
+}
+
+xr_status xr_dev_forward_md(xr_ctx *c, const void *d_vol, const float *d_md, float *d_sino, xr_rotate dir) {
+    if (!c || !d_vol || !d_md || !d_sino) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = check_xtt_k(c))) return st;
+    if ((st = ensure_device(c))) return st;
+    return forward_into(c, d_vol, d_sino, dir == XR_ROTATE_CCW ? -1 : 1, 1, true, c->storage, d_md, 1);
+}
+
+static xr_status md_need3(xr_ctx *c) {
+    if (c->K < 3) return fail(c, XR_ERR_CONFIG, "the main-direction steps need three basis vectors");
+    return ensure_device(c);
+}
+
+xr_status xr_md_filter(xr_ctx *c, float *d_md, float *d_tmp, float weight, int passes) {
+    if (!c || !d_md || !d_tmp || passes < 0) return c ? fail(c, XR_ERR_ARG, "bad argument") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    const size_t bytes = 3 * (size_t)c->N * c->N * c->N * sizeof(float);
+    Timed t(c, XR_T_ORIENT);
+    for (int p = 0; p < passes; p++) {
+        if ((st = cuda_check(c, cudaMemcpyAsync(d_tmp, d_md, bytes, cudaMemcpyDeviceToDevice, c->stream), "md copy")))
+            return st;
+        if ((st = cuda_check(c, launch_md_filter(c->N, d_md, d_tmp, weight, c->stream), "md filter"))) return st;
+        if ((st = cuda_check(c, cudaMemcpyAsync(d_md, d_tmp, bytes, cudaMemcpyDeviceToDevice, c->stream), "md copy")))
+            return st;
+    }
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "md filter");
+}
+
+xr_status xr_md_main_direction(xr_ctx *c, const float *d_vol, float *d_md, int iter) {
+    if (!c || !d_vol || !d_md || iter < 0 || iter > 3) return c ? fail(c, XR_ERR_ARG, "bad argument") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = md_need3(c))) return st;
+    st = cuda_check(c, launch_main_direction(c->N, d_vol, d_md, nullptr, iter, c->stream), "main direction");
+    return st ? st : cuda_check(c, cudaStreamSynchronize(c->stream), "main direction");
+}
+
+xr_status xr_md_with_estimate(xr_ctx *c, const float *d_vol, float *d_md, const float *d_est) {
+    if (!c || !d_vol || !d_md || !d_est) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = md_need3(c))) return st;
+    st = cuda_check(c, launch_main_direction(c->N, d_vol, d_md, d_est, 0, c->stream), "main direction");
+    return st ? st : cuda_check(c, cudaStreamSynchronize(c->stream), "main direction");
+}
+
+xr_status xr_md_update_estimation(xr_ctx *c, const float *d_vol, float *d_est, int iter) {
+    if (!c || !d_vol || !d_est) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = md_need3(c))) return st;
+    st = cuda_check(c, launch_update_estimation(c->N, d_vol, d_est, iter, c->stream), "estimation");
+    return st ? st : cuda_check(c, cudaStreamSynchronize(c->stream), "estimation");
+}
+
+xr_status xr_dev_fill(xr_ctx *c, float *d, size_t n, float value) {
+    if (!c || (!d && n)) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    st = cuda_check(c, launch_fill((long)n, d, value, c->stream), "fill");
+    return st ? st : cuda_check(c, cudaStreamSynchronize(c->stream), "fill");
 }
 
 xr_status xr_orth_normal_update(xr_ctx *c, const float *d_vol, float *d_coef, float *d_loss, int rot) {

@@ -92,7 +92,8 @@ struct Session {
     int storage = 0;                  /* volume                      */
     int sino_storage = 0;             /* measured sinogram           */
     int update_storage = 0;           /* volume, | kStoreStochastic  */
-    const float *coef = nullptr;      /* orientation-parametrised XTT: (phi, cos) planes */
+    const float *coef = nullptr;      /* orientation-parametrised XTT: rotation planes */
+    int coef_kind = 0;                /* 0: (phi, cos theta); 1: main direction (3 planes) */
     cudaEvent_t sino_ready = nullptr; /* set: the first ratio launch waits for it (sinogram upload) */
     std::vector<int> order;            /* persistent subset order (XTT)     */
     std::vector<int> ir_orders;        /* C*epochs rows (IR)                */
@@ -164,8 +165,10 @@ void timing_end(xr_ctx *c, int cls, cudaEvent_t ev);
 
 /* ---- kernel launchers (xr_kernels.cu) ---- */
 /* coef (the forward / back launchers): non-null selects the orientation-
- * parametrised XTT of the reference's forwardOrth / backwardOrth (ir.cu:
- * 294-423), every voxel's basis rotated by its (phi, cos theta) planes. */
+ * parametrised XTT, every voxel's basis rotated: coef_kind 0 by its
+ * (phi, cos theta) planes (forwardOrth / backwardOrth, ir.cu:294-423), 1 by
+ * its main-direction planes (forwardOrthByMD / backwardOrthByMD, ir.cu:
+ * 154-292; that forward carries no vs * ratio factor). */
 /* Forward splat of one set of views (all listed views of every listed axis).
  * mode 0: plain, value = ratio * vol[0]; mode 1: XTT K channels; mode 2:
  * weights only (value 1, the reference's devProjFactor).  out: C blocks of
@@ -173,7 +176,7 @@ void timing_end(xr_ctx *c, int cls, cudaEvent_t ev);
 cudaError_t launch_forward(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                            const int *view_list, int n_views, int cond0, int n_cond, const void *vol,
                            float *out, int mode, int views_per_cta, int storage, cudaStream_t s,
-                           const float *coef = nullptr);
+                           const float *coef = nullptr, int coef_kind = 0);
 /* Chord-length normaliser: norm = L / (norm + 1e-5) in place, every view. */
 cudaError_t launch_chord(const GeomConst &g, const ViewFrame *frames, float *norm, int n_cond, cudaStream_t s);
 /* Normalise (skipped when norm is null) + ratio (MLEM) or subtract (ART) on
@@ -186,7 +189,7 @@ cudaError_t launch_normalize(const GeomConst &g, int n_cond, float *proj, const 
 cudaError_t launch_back_update(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, int cond0, int n_cond, const float *proj,
                                void *vol, int xtt, int art, float alpha, int storage, cudaStream_t s,
-                               const float *coef = nullptr);
+                               const float *coef = nullptr, int coef_kind = 0);
 /* FP64 sums: out[0] += sum (p-b)^2, out[1] += sum b^2, out[2] += sum |p-b|. */
 cudaError_t launch_residual(long n, const float *p, const void *b, double *out, int storage, cudaStream_t s);
 /* mu = sqrt|mu| over n values. */
@@ -199,18 +202,26 @@ cudaError_t check_exact_rdet(float det, float rdet, unsigned *d_flag, unsigned *
 cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, const int *d_conds, int n_cond, int G,
                                const float *d_magsig, const void *vol, float *out, int mode, int views_per_cta,
-                               int storage, cudaStream_t s, const float *coef = nullptr);
+                               int storage, cudaStream_t s, const float *coef = nullptr, int coef_kind = 0);
 /* mode 0: plain (one axis, update in place); 1: XTT (fac_in = sensitivity);
  * 2: sensitivity of the listed views into fac_out. */
 cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                             const int *view_list, int n_views, const int *d_conds, int n_cond, const int *d_axis_g,
                             const float *d_magsig, const float *proj, void *vol, const float *fac_in, float *fac_out,
                             int mode, int art, float alpha, int storage, cudaStream_t s,
-                            const float *coef = nullptr);
+                            const float *coef = nullptr, int coef_kind = 0);
 
 /* ---- xr_orient.cu ---- */
 /* calcNormalVectorThreeDirec (ir.cu:856-974) on every voxel: vol holds the
  * three coefficients (FP32), coef (phi, cos theta) is updated, loss |(R e_z) x n|. */
+/* Main-direction kernels of circleEstReconstruct (ir.cu:624-844, 1304-1363),
+ * FP32 planes of N^3: meanFiltFiberMD over 2 <= x, y, z < N-2 into out;
+ * calcMainDirection (est null, sign pattern iter) or calcMDWithEst (est
+ * planes (loss, pattern)); updateEstimation. */
+cudaError_t launch_md_filter(int N, const float *md, float *out, float coef, cudaStream_t s);
+cudaError_t launch_main_direction(int N, const float *vol, float *md, const float *est, int iter, cudaStream_t s);
+cudaError_t launch_update_estimation(int N, const float *vol, float *est, int iter, cudaStream_t s);
+cudaError_t launch_fill(long n, float *p, float value, cudaStream_t s);
 cudaError_t launch_normal_three(long nvox, const BasisConst *d_basis, const float *vol, float *coef, float *loss,
                                 int rot, cudaStream_t s);
 cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, const void *mu, float *md,

@@ -116,6 +116,7 @@ struct FwdArgs {
     float *out;               /* C blocks of V*Nd*Nd         */
     const BasisConst *basis;  /* device                      */
     const float *coef;        /* mode 3: rotation planes     */
+    int coef_kind;            /* 0: (phi, cos); 1: md        */
     int nbx, nby;             /* bricks along x, y           */
 };
 
@@ -209,7 +210,8 @@ __global__ void __launch_bounds__(kFwdThreads, 3) k_forward(FwdArgs a) {
         } else if (MODE == 2) {
             val[q] = 1.0f;
         } else if (MODE == 3) {   /* forwardOrth (ir.cu:294-364) */
-            orth_moments<T>(a.basis, cond, g.K, __fmul_rn(g.vs, g.ratio), vol, a.coef, idx, N3, val[q], m[q]);
+            orth_moments<T>(a.basis, cond, g.K, a.coef_kind ? 1.0f : __fmul_rn(g.vs, g.ratio), vol, a.coef,
+                            a.coef_kind, idx, N3, val[q], m[q]);
         } else {
             const BasisConst *B = a.basis;
             const float sc = __fmul_rn(g.vs, g.ratio);
@@ -454,6 +456,7 @@ struct BackArgs {
     float alpha;
     int sr;                   /* 16-bit volumes: stochastic rounding of updates */
     const float *coef;        /* non-null: per-voxel rotated basis (backwardOrth) */
+    int coef_kind;            /* 0: (phi, cos theta); 1: main direction            */
 };
 
 template <bool XTT, typename T>
@@ -520,10 +523,10 @@ __global__ void __launch_bounds__(kBackThreads) k_back_update(BackArgs a) {
                 }
             }
         }
-        if (XTT && ok && a.coef) {   /* backwardOrth (ir.cu:366-423): the voxel's rotated basis */
+        if (XTT && ok && a.coef) {   /* backwardOrth(ByMD) (ir.cu:366-423, :233-292): the voxel's rotated basis */
             const BasisConst *B = a.basis;
             float R[9];
-            orth_rotation(a.coef, (size_t)N * N * N, (size_t)x + (size_t)N * y + (size_t)N * N * z, R);
+            src_rotation(a.coef, a.coef_kind, (size_t)N * N * N, (size_t)x + (size_t)N * y + (size_t)N * N * z, R);
             const float G0 = B->G[3 * cond], G1 = B->G[3 * cond + 1], G2 = B->G[3 * cond + 2];
 #pragma unroll
             for (int k = 0; k < 16; k++) {
@@ -624,11 +627,13 @@ int grid_for(size_t n, int threads) {
 
 cudaError_t launch_forward(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                            const int *view_list, int n_views, int cond0, int n_cond, const void *vol, float *out,
-                           int mode, int views_per_cta, int storage, cudaStream_t s, const float *coef) {
+                           int mode, int views_per_cta, int storage, cudaStream_t s, const float *coef,
+                           int coef_kind) {
     if (n_views <= 0 || n_cond <= 0) return cudaSuccess;
     if (coef && mode == 1) mode = 3;
     FwdArgs a;
     a.coef = coef;
+    a.coef_kind = coef_kind;
     a.g = g;
     a.frames = frames;
     a.view_list = view_list;
@@ -703,9 +708,10 @@ cudaError_t launch_normalize(const GeomConst &g, int n_cond, float *proj, const 
 cudaError_t launch_back_update(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, int cond0, int n_cond, const float *proj,
                                void *vol, int xtt, int art, float alpha, int storage, cudaStream_t s,
-                               const float *coef) {
+                               const float *coef, int coef_kind) {
     BackArgs a;
     a.coef = coef;
+    a.coef_kind = coef_kind;
     a.sr = (storage & kStoreStochastic) != 0;
     storage &= ~kStoreStochastic;
     a.g = g;

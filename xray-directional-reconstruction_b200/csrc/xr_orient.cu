@@ -134,6 +134,104 @@ __global__ void k_normal_three(long nvox, const BasisConst *B, const float *vol,
     }
 }
 
+/* meanFiltFiberMD, ir.cu:1304-1363, for 2 <= x, y, z < N-2: the 27
+ * neighbours of the centre c signed by their agreement with it (c.o > 0
+ * added, < 0 subtracted, weight w), normalised (zero -> e_z), scaled to |c|. */
+__global__ void k_md_filter(int N, const float *md, float *out, float w) {
+    const long n3 = (long)N * N * N, M = N - 4;
+    const long nint = M > 0 ? M * M * M : 0;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += (long)gridDim.x * blockDim.x) {
+        const long x = 2 + t % M, y = 2 + (t / M) % M, z = 2 + t / (M * M);
+        const long c = x + N * (y + (long)N * z);
+        const float c0 = md[c], c1 = md[n3 + c], c2 = md[2 * n3 + c];
+        const float len = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
+        float v[3] = {0.f, 0.f, 0.f};
+        for (int i = -1; i < 2; i++)
+            for (int j = -1; j < 2; j++)
+                for (int k = -1; k < 2; k++) {
+                    const long o = (x - i) + N * ((y - j) + (long)N * (z - k));
+                    const float o0 = md[o], o1 = md[n3 + o], o2 = md[2 * n3 + o];
+                    /* products and sums rounded one by one, as the reference's FP32
+                     * code: the sign of d decides between adding and subtracting */
+                    const float d = __fadd_rn(__fadd_rn(__fmul_rn(c0, o0), __fmul_rn(c1, o1)), __fmul_rn(c2, o2));
+                    if (d > 0.f) {
+                        v[0] = __fadd_rn(v[0], __fmul_rn(w, o0));
+                        v[1] = __fadd_rn(v[1], __fmul_rn(w, o1));
+                        v[2] = __fadd_rn(v[2], __fmul_rn(w, o2));
+                    } else if (d < -0.f) {
+                        v[0] = __fsub_rn(v[0], __fmul_rn(w, o0));
+                        v[1] = __fsub_rn(v[1], __fmul_rn(w, o1));
+                        v[2] = __fsub_rn(v[2], __fmul_rn(w, o2));
+                    }
+                }
+        normalize3(v);
+        if (sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) < 1e-8f) { v[0] = 0.f; v[1] = 0.f; v[2] = 1.f; }
+        out[c] = len * v[0];
+        out[n3 + c] = len * v[1];
+        out[2 * n3 + c] = len * v[2];
+    }
+}
+
+/* calcMainDirection (ir.cu:624-710; sign pattern iter) or calcMDWithEst
+ * (:712-789; pattern from estimate plane 1): the in-plane magnitudes of mu
+ * (planes 0..2) after removing its (+-1, +-1, +-1) component, signed, times
+ * half the sum of mu, rotated by the voxel's previous main direction, z >= 0. */
+__global__ void k_main_direction(int N, const float *vol, float *md, const float *est, int iter) {
+    const long n3 = (long)N * N * N;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (long)gridDim.x * blockDim.x) {
+        const float mu0 = vol[i], mu1 = vol[n3 + i], mu2 = vol[2 * n3 + i];
+        float n0 = 0.f, n1 = 0.f, n2 = 0.f;
+        if (mu2 + mu1 - mu0 < 0.f) { n0 = -1.f; n1 = 1.f; n2 = 1.f; }
+        else if (mu0 + mu2 - mu1 < 0.f) { n0 = 1.f; n1 = -1.f; n2 = 1.f; }
+        else if (mu1 + mu0 - mu2 < 0.f) { n0 = 1.f; n1 = 1.f; n2 = -1.f; }
+        /* rounded one by one: the square roots below amplify any difference
+         * in these near-cancelling sums */
+        const float co = __fdiv_rn(__fadd_rn(__fadd_rn(__fmul_rn(mu0, n0), __fmul_rn(mu1, n1)), __fmul_rn(mu2, n2)), 3.f);
+        const float v0 = __fsub_rn(mu0, __fmul_rn(co, n0)), v1 = __fsub_rn(mu1, __fmul_rn(co, n1));
+        const float v2 = __fsub_rn(mu2, __fmul_rn(co, n2));
+        float fx = sqrtf(0.5f * fabsf(v2 + v1 - v0)), fy = sqrtf(0.5f * fabsf(v0 + v2 - v1));
+        const float fz = sqrtf(0.5f * fabsf(v1 + v0 - v2));
+        int sgn = iter;
+        if (est) {
+            const float r = est[n3 + i];
+            sgn = r < 0.5f ? 0 : (r < 1.5f ? 1 : (r < 2.5f ? 2 : 3));
+        }
+        if (sgn == 1) fx = -fx;
+        else if (sgn == 2) { fx = -fx; fy = -fy; }
+        else if (sgn == 3) fy = -fy;
+        const float mean = (mu0 + mu1 + mu2) / 2.0f;
+        const float m[3] = {mean * fx, mean * fy, mean * fz};
+        float R[9];
+        md_rotation(md, (size_t)n3, (size_t)i, R);
+        float r[3] = {R[0] * m[0] + R[1] * m[1] + R[2] * m[2], R[3] * m[0] + R[4] * m[1] + R[5] * m[2],
+                      R[6] * m[0] + R[7] * m[1] + R[8] * m[2]};
+        if (r[2] < 0.f) { r[0] = -r[0]; r[1] = -r[1]; r[2] = -r[2]; }
+        md[i] = r[0];
+        md[n3 + i] = r[1];
+        md[2 * n3 + i] = r[2];
+    }
+}
+
+/* updateEstimation, ir.cu:791-844: loss = mu2^2 + (1 - lo/hi)^2 of the first
+ * two channels; where it beats estimate plane 0, planes 0/1 <- (loss, iter). */
+__global__ void k_update_estimation(int N, const float *vol, float *est, int iter) {
+    const long n3 = (long)N * N * N;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (long)gridDim.x * blockDim.x) {
+        const float mu0 = vol[i], mu1 = vol[n3 + i], mu2 = vol[2 * n3 + i];
+        const float lo = mu0 < mu1 ? mu0 : mu1, hi = mu0 < mu1 ? mu1 : mu0;
+        const float q = __fsub_rn(1.0f, __fdiv_rn(lo, hi));
+        const float loss = __fadd_rn(__fmul_rn(mu2, mu2), __fmul_rn(q, q));
+        if (loss < est[i]) {
+            est[i] = loss;
+            est[n3 + i] = (float)iter;
+        }
+    }
+}
+
+__global__ void k_fill(long n, float *p, float value) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) p[i] = value;
+}
+
 int grid_for(long n, int threads) {
     long b = (n + threads - 1) / threads;
     if (b > 148 * 16) b = 148 * 16;
@@ -148,6 +246,28 @@ cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, cons
     if (storage == kBF16) k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const __nv_bfloat16 *)mu, md, ev);
     else if (storage == kF16) k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const __half *)mu, md, ev);
     else k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const float *)mu, md, ev);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_md_filter(int N, const float *md, float *out, float coef, cudaStream_t s) {
+    const long M = N - 4;
+    if (M <= 0) return cudaSuccess;
+    k_md_filter<<<grid_for(M * M * M, 256), 256, 0, s>>>(N, md, out, coef);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_main_direction(int N, const float *vol, float *md, const float *est, int iter, cudaStream_t s) {
+    k_main_direction<<<grid_for((long)N * N * N, 256), 256, 0, s>>>(N, vol, md, est, iter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update_estimation(int N, const float *vol, float *est, int iter, cudaStream_t s) {
+    k_update_estimation<<<grid_for((long)N * N * N, 256), 256, 0, s>>>(N, vol, est, iter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill(long n, float *p, float value, cudaStream_t s) {
+    k_fill<<<grid_for(n, 256), 256, 0, s>>>(n, p, value);
     return cudaGetLastError();
 }
 

@@ -1,9 +1,10 @@
 /*
  * Orientation-parametrised XTT (the reference's forwardOrth / backwardOrth,
- * reconstruct/src/ir.cu:294-423): every voxel's scattering basis is rotated
- * by its own Rodrigues rotation, built from two coefficient planes
- * (phi, cos theta) as rodriguesRotation(cos phi, sin phi, 0, cos theta,
- * sqrt(1 - cos^2 theta)) (ir.cu:597-623).  With S' = R S_k the weight of
+ * reconstruct/src/ir.cu:294-423, and forwardOrthByMD / backwardOrthByMD,
+ * :154-292): every voxel's scattering basis is rotated by its own Rodrigues
+ * rotation, built from two coefficient planes (phi, cos theta) as
+ * rodriguesRotation(cos phi, sin phi, 0, cos theta, sqrt(1 - cos^2 theta)), or
+ * from the voxel's main direction m (ir.cu:597-623).  With S' = R S_k the weight of
  * channel k stays (|B x S'| |S' . G|)^2 = (S' . G)^2 (|S'|^2 - (B . S')^2),
  * so the projectors keep their quadratic-form structure with per-voxel
  * g_k = (S' . G)^2, |S'|^2 and S' S'^T.
@@ -16,10 +17,9 @@
 
 namespace xr {
 
-/* R (row-major) of voxel idx; coef holds the phi plane then the cos plane. */
-__device__ __forceinline__ void orth_rotation(const float *coef, size_t n3, size_t idx, float R[9]) {
-    const float phi = __ldg(coef + idx), ct = __ldg(coef + n3 + idx);
-    const float x = cosf(phi), y = sinf(phi), sn = sqrtf(1.0f - ct * ct);
+/* rodriguesRotation (ir.cu:597-623) about (x, y, 0) normalised, by the angle
+ * of cosine ct / sine sn; identity when |(x, y)| < 1e-8. */
+__device__ __forceinline__ void rodrigues_xy(float x, float y, float ct, float sn, float R[9]) {
     const float l = sqrtf(x * x + y * y);
     if (l < 1e-8f) {
 #pragma unroll
@@ -30,6 +30,28 @@ __device__ __forceinline__ void orth_rotation(const float *coef, size_t n3, size
     R[0] = oc * nx * nx + ct;      R[1] = oc * nx * ny - nz * sn; R[2] = oc * nx * nz + ny * sn;
     R[3] = oc * nx * ny + nz * sn; R[4] = oc * ny * ny + ct;      R[5] = oc * ny * nz - nx * sn;
     R[6] = oc * nx * nz - ny * sn; R[7] = oc * ny * nz + nx * sn; R[8] = oc * nz * nz + ct;
+}
+
+/* R (row-major) of voxel idx; coef holds the phi plane then the cos plane. */
+__device__ __forceinline__ void orth_rotation(const float *coef, size_t n3, size_t idx, float R[9]) {
+    const float phi = __ldg(coef + idx), ct = __ldg(coef + n3 + idx);
+    rodrigues_xy(cosf(phi), sinf(phi), ct, sqrtf(1.0f - ct * ct), R);
+}
+
+/* R of voxel idx from its main direction m (three planes), as
+ * forwardOrthByMD / backwardOrthByMD (ir.cu:183-189, :262-268): about
+ * (-m1, m0, 0) by the angle of cosine m2 / |m|. */
+__device__ __forceinline__ void md_rotation(const float *md, size_t n3, size_t idx, float R[9]) {
+    const float m0 = __ldg(md + idx), m1 = __ldg(md + n3 + idx), m2 = __ldg(md + 2 * n3 + idx);
+    const float l3 = sqrtf(m0 * m0 + m1 * m1 + m2 * m2);
+    rodrigues_xy(-m1, m0, m2 / l3, sqrtf(m0 * m0 + m1 * m1) / l3, R);
+}
+
+/* The rotation source of the orientation-parametrised projectors:
+ * kind 0 (phi, cos theta) planes, kind 1 main-direction planes. */
+__device__ __forceinline__ void src_rotation(const float *coef, int kind, size_t n3, size_t idx, float R[9]) {
+    if (kind) md_rotation(coef, n3, idx, R);
+    else orth_rotation(coef, n3, idx, R);
 }
 
 /* S' = R S_k */
@@ -45,9 +67,10 @@ __device__ __forceinline__ void orth_basis(const BasisConst *B, int k, const flo
  * (xx, yy, zz, 2xy, 2xz, 2yz). */
 template <typename T>
 __device__ __forceinline__ void orth_moments(const BasisConst *B, int cond, int K, float sc, const T *vol,
-                                             const float *coef, size_t idx, size_t n3, float &a0, float mm[6]) {
+                                             const float *coef, int kind, size_t idx, size_t n3, float &a0,
+                                             float mm[6]) {
     float R[9];
-    orth_rotation(coef, n3, idx, R);
+    src_rotation(coef, kind, n3, idx, R);
     const float G0 = B->G[3 * cond], G1 = B->G[3 * cond + 1], G2 = B->G[3 * cond + 2];
     a0 = 0.f;
 #pragma unroll
