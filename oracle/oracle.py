@@ -143,6 +143,22 @@ class Oracle:
         """updateEstimation (ir.cu:791-844): est (2 planes) updated in place."""
         self._fn("update_estimation", dt)(ctypes.byref(self._scan(s)), _p(vol, dt), _p(est, dt), int(iteration))
 
+    def normal_three_est(self, s, vol, coef, loss, est, dt=np.float32):
+        """calcNormalVectorThreeDirecWithEst (ir.cu:976-1071): coef and loss updated in place."""
+        self._fn("normal_three_est", dt)(ctypes.byref(self._scan(s)), _p(vol, dt), _p(coef, dt), _p(loss, dt),
+                                         _p(est, dt))
+
+    def coef_filter_slab(self, s, y, coef, vol, out, w, dt=np.float32):
+        """meanFiltFiber (ir.cu:1231-1302) of slab y into out."""
+        c = ctypes.c_float(w) if dt == np.float32 else ctypes.c_double(w)
+        self._fn("coef_filter_slab", dt)(ctypes.byref(self._scan(s)), int(y), _p(coef, dt), _p(vol, dt),
+                                         _p(out, dt), c)
+
+    def update_estimation_coef(self, s, vol, est, iteration, dt=np.float32):
+        """updateEstimationByCoef (ir.cu:1073-1120): est updated in place."""
+        self._fn("update_estimation_coef", dt)(ctypes.byref(self._scan(s)), _p(vol, dt), _p(est, dt),
+                                               int(iteration))
+
     def correlation(self, s, cond, n, proj, factor, dt=np.float32):
         self._fn("correlation", dt)(ctypes.byref(self._scan(s)), cond, n, _p(proj, dt), _p(factor, dt))
 
@@ -276,6 +292,16 @@ class RefHost:
 
     def backward_md(self, cond, y, n, proj, md, tmp, factor):
         self.lib.xr_ref_backward_md(cond, y, n, _p(proj), _p(md), _p(tmp), _p(factor))
+
+    def normal_three_est(self, vol, coef, loss, est):
+        self.lib.xr_ref_normal_three_est(_p(vol), _p(coef), _p(loss), _p(est))
+
+    def coef_filter(self, y, coef, out, vol, w):
+        self.lib.xr_ref_coef_filter(int(y), _p(coef), _p(out), _p(vol), ctypes.c_float(w))
+
+    def update_estimation_coef(self, vol, est, iteration):
+        loss = np.zeros(self.s.N ** 3, np.float32)
+        self.lib.xr_ref_update_estimation_coef(_p(vol), _p(loss), _p(est), int(iteration))
 
     def md_filter(self, y, md, out, coef):
         self.lib.xr_ref_md_filter(int(y), _p(md), _p(out), ctypes.c_float(coef))

@@ -171,6 +171,24 @@ void xr_ref_update_estimation(const float *vol, float *md, float *loss, float *e
         launch2d(g.gridV, g.blockV, updateEstimation, vol, md, y, (const Geometry *)&g.geom, loss, est, iter);
 }
 
+/* calcNormalVectorThreeDirecWithEst (ir.cu:976-1071), every y slab. */
+void xr_ref_normal_three_est(float *vol, float *coef, float *loss, const float *est) {
+    for (int y = 0; y < g.geom.voxel; y++)
+        launch2d(g.gridV, g.blockV, calcNormalVectorThreeDirecWithEst, vol, coef, y, (const Geometry *)&g.geom, loss,
+                 est);
+}
+
+/* meanFiltFiber (ir.cu:1231-1302), slab y: coef -> out. */
+void xr_ref_coef_filter(int y, const float *coef, float *out, const float *vol, float w) {
+    launch2d(g.gridV, g.blockV, meanFiltFiber, coef, out, vol, (const Geometry *)&g.geom, y, w);
+}
+
+/* updateEstimationByCoef (ir.cu:1073-1120), every y slab. */
+void xr_ref_update_estimation_coef(const float *vol, float *loss, float *est, int iter) {
+    for (int y = 0; y < g.geom.voxel; y++)
+        launch2d(g.gridV, g.blockV, updateEstimationByCoef, vol, y, (const Geometry *)&g.geom, loss, est, iter);
+}
+
 void xr_ref_correlation(int cond, int n, float *proj, const float *factor) {
     launch2d(g.gridD, g.blockD, correlationProjByLength, proj, factor, &g.geom, cond, n);
 }

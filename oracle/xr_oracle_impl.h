@@ -394,9 +394,27 @@ static void RV(normalize3)(real *v) {
  * coefficients mu (planes 0..2) and the sign pattern rot, the plane normal
  * (mu0 S0 - mu1' S1) x (mu0 S0 - mu2' S2), rotated by the voxel's current R,
  * z >= 0, gives the new (phi, cos theta); loss = |(R e_z) x norm|. */
+static void RV(normal_three_voxel)(const or_scan *s, const real *vol, real *coef, real *loss, long N3, long i,
+                                   int rot);
+
 void RV(normal_three)(const or_scan *s, const real *vol, real *coef, real *loss, int rot) {
     const long N3 = (long)s->N * s->N * s->N;
+    for (long i = 0; i < N3; i++) RV(normal_three_voxel)(s, vol, coef, loss, N3, i, rot);
+}
+
+/* calcNormalVectorThreeDirecWithEst, ir.cu:976-1071: the sign pattern of each
+ * voxel from its estimate plane 1 (< 0.5, < 1.5, < 2.5, else). */
+void RV(normal_three_est)(const or_scan *s, const real *vol, real *coef, real *loss, const real *est) {
+    const long N3 = (long)s->N * s->N * s->N;
     for (long i = 0; i < N3; i++) {
+        const real r = est[N3 + i];
+        RV(normal_three_voxel)(s, vol, coef, loss, N3, i, r < (real)0.5f ? 0 : (r < (real)1.50f ? 1 : (r < (real)2.50f ? 2 : 3)));
+    }
+}
+
+static void RV(normal_three_voxel)(const or_scan *s, const real *vol, real *coef, real *loss, long N3, long i,
+                                   int rot) {
+    {
         real R[9];
         RV(orth_rotation)(coef, N3, i, R);
         const real mu0 = vol[i], m1 = vol[N3 + i], m2 = vol[2 * N3 + i];
@@ -605,6 +623,79 @@ void RV(update_estimation)(const or_scan *s, const real *vol, real *est, int ite
         const real loss = mu2 * mu2 + ((real)1.0f - lo / hi) * ((real)1.0f - lo / hi);
         if (loss < est[i]) {
             est[i] = loss;
+            est[N3 + i] = (real)iter;
+        }
+    }
+}
+
+/* meanFiltFiber, ir.cu:1231-1302, on slab y (1 <= y < N-1, as the driver
+ * reconstruct.cu:534-537 calls it) for 1 <= x, z < N-1: each neighbour's
+ * direction from its (phi, cos theta) planes as mu (sin t cos(phi - pi/2),
+ * sin t sin(phi - pi/2), cos t), mu the sum of its three coefficients; pairs
+ * (i, 26 - i) within 60 degrees of the centre (|dot| > 0.5) added signed to
+ * it, normalised, z >= 0, back to (phi, cos theta).  -pi/2 + phi is
+ * evaluated in double (M_PI) and rounded to float. */
+void RV(coef_filter_slab)(const or_scan *s, int y, const real *coef, const real *vol, real *out, real w) {
+    const long N = s->N, N3 = N * N * N;
+    for (long z = 1; z < N - 1; z++)
+        for (long x = 1; x < N - 1; x++) {
+            real nv[27][3];
+            int cnt = 0;
+            for (int i = -1; i < 2; i++)
+                for (int j = -1; j < 2; j++)
+                    for (int k = -1; k < 2; k++) {
+                        const long o = (x - i) + N * (y - j) + N * N * (z - k);
+                        const real ct = coef[N3 + o];
+                        const real st = RSQRT((real)1.f - ct * ct);
+                        const real phi = (real)(-M_PI / 2.0f + (double)coef[o]);
+                        const real mu = vol[o] + vol[N3 + o] + vol[2 * N3 + o];
+                        nv[cnt][0] = mu * (st * RCOS(phi));
+                        nv[cnt][1] = mu * (st * RSIN(phi));
+                        nv[cnt][2] = mu * ct;
+                        cnt++;
+                    }
+            real c[3] = {nv[13][0], nv[13][1], nv[13][2]};
+            for (int i = 0; i < 13; i++) {
+                const real *a = nv[i], *b = nv[26 - i];
+                const real da = a[0] * nv[13][0] + a[1] * nv[13][1] + a[2] * nv[13][2];
+                if (da > (real)0.5f) { c[0] = c[0] + w * a[0]; c[1] = c[1] + w * a[1]; c[2] = c[2] + w * a[2]; }
+                else if (da < -(real)0.5f) { c[0] = c[0] - w * a[0]; c[1] = c[1] - w * a[1]; c[2] = c[2] - w * a[2]; }
+                const real db = b[0] * nv[13][0] + b[1] * nv[13][1] + b[2] * nv[13][2];
+                if (db > (real)0.5f) { c[0] = c[0] + w * b[0]; c[1] = c[1] + w * b[1]; c[2] = c[2] + w * b[2]; }
+                else if (db < -(real)0.5f) { c[0] = c[0] - w * b[0]; c[1] = c[1] - w * b[1]; c[2] = c[2] - w * b[2]; }
+            }
+            RV(normalize3)(c);
+            if (c[2] < (real)0) { c[0] = -c[0]; c[1] = -c[1]; c[2] = -c[2]; }
+            /* rotAxis = e_z x c, cos = e_z . c */
+            const real ax = (real)0 * c[2] - (real)1 * c[1], ay = (real)1 * c[0] - (real)0 * c[2];
+            const long ci = x + N * y + N * N * z;
+            out[ci] = RATAN2(ay, ax);
+            out[N3 + ci] = (real)0 * c[0] + (real)0 * c[1] + (real)1 * c[2];
+        }
+}
+
+/* updateEstimationByCoef, ir.cu:1073-1120: the plane normal of the three
+ * coefficients (no signs), z >= 0; where its cosine to e_z exceeds estimate
+ * plane 0, planes 0/1 <- (cosine, iter). */
+void RV(update_estimation_coef)(const or_scan *s, const real *vol, real *est, int iter) {
+    const long N3 = (long)s->N * s->N * s->N;
+    const float *b = s->basis;
+    for (long i = 0; i < N3; i++) {
+        const real mu0 = vol[i], mu1 = vol[N3 + i], mu2 = vol[2 * N3 + i];
+        real v1[3], v2[3], n[3];
+        for (int j = 0; j < 3; j++) {
+            v1[j] = mu0 * (real)b[j] - mu1 * (real)b[3 + j];
+            v2[j] = mu0 * (real)b[j] - mu2 * (real)b[6 + j];
+        }
+        n[0] = v1[1] * v2[2] - v1[2] * v2[1];
+        n[1] = v1[2] * v2[0] - v1[0] * v2[2];
+        n[2] = v1[0] * v2[1] - v1[1] * v2[0];
+        RV(normalize3)(n);
+        if (n[2] < (real)0) { n[0] = -n[0]; n[1] = -n[1]; n[2] = -n[2]; }
+        RV(normalize3)(n);
+        const real c = (real)0 * n[0] + (real)0 * n[1] + (real)1 * n[2];
+        if (c > est[i]) {
+            est[i] = c;
             est[N3 + i] = (real)iter;
         }
     }

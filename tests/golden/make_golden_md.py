@@ -1,6 +1,8 @@
 """Golden vectors of the reference's main-direction (circle-estimate) kernels
 (forwardOrthByMD, backwardOrthByMD, meanFiltFiberMD, calcMainDirection,
-calcMDWithEst, updateEstimation; reconstruct/src/ir.cu) from its host build
+calcMDWithEst, updateEstimation) and of the coefficient-plane steps of its
+orth drivers (meanFiltFiber, calcNormalVectorThreeDirecWithEst,
+updateEstimationByCoef; reconstruct/src/ir.cu) from its host build
 (oracle/_ref/libxrref.so, serial launch order).
 
     python tests/golden/make_golden_md.py
@@ -36,7 +38,8 @@ def md_inputs(s: Scan):
     md[:2, 6, 6, 6] = 0.0                     # along z
     ratio = rng.uniform(0.0, 2.0, (V, Nd, Nd)).astype(np.float32)
     est = np.stack([rng.uniform(0.0, 2.0, (N, N, N)), rng.uniform(0.0, 3.5, (N, N, N))]).astype(np.float32)
-    return vol, md, ratio, est
+    coef = np.stack([rng.uniform(-3.1, 3.1, (N, N, N)), rng.uniform(-0.99, 0.99, (N, N, N))]).astype(np.float32)
+    return vol, md, ratio, est, coef
 
 
 def main() -> None:
@@ -45,9 +48,9 @@ def main() -> None:
     s = md_scan()
     R.setup(s)
     N, Nd, V = s.N, s.Nd, s.V
-    vol, md, ratio, est = md_inputs(s)
+    vol, md, ratio, est, coef = md_inputs(s)
     out = {"geom": np.array([s.sdd, s.sod, s.det, N, Nd, V], np.float64), "rot": s.rot, "trans": s.trans,
-           "offset": s.offset, "basis": s.basis, "vol": vol, "md": md, "ratio": ratio, "est": est}
+           "offset": s.offset, "basis": s.basis, "vol": vol, "md": md, "ratio": ratio, "est": est, "coef": coef}
     for cond in range(3):
         n = 1 + 3 * cond
         p = np.zeros(V * Nd * Nd, np.float32)
@@ -74,6 +77,18 @@ def main() -> None:
     e = est.ravel().copy()
     R.update_estimation(vol.ravel().copy(), md.ravel().copy(), e, 2)
     out["update_est"] = e
+    c = coef.ravel().copy()
+    loss = np.zeros(N ** 3, np.float32)
+    R.normal_three_est(vol.ravel().copy(), c, loss, est.ravel().copy())
+    out["nrm_est_coef"] = c
+    out["nrm_est_loss"] = loss
+    cf = coef.ravel().copy()
+    for y in range(1, N - 1):
+        R.coef_filter(y, coef.ravel().copy(), cf, vol.ravel().copy(), 1.0)
+    out["coef_filter"] = cf
+    e = est.ravel().copy()
+    R.update_estimation_coef(vol.ravel().copy(), e, 3)
+    out["update_est_coef"] = e
     path = os.path.join(HERE, "ref_md_small.npz")
     np.savez_compressed(path, **out)
     print(path, len(out), "arrays")

@@ -1,6 +1,7 @@
 """Pin the oracle's main-direction restatements (forwardOrthByMD,
 backwardOrthByMD, meanFiltFiberMD, calcMainDirection, calcMDWithEst,
-updateEstimation) bit for bit against golden vectors from the reference's own
+updateEstimation) and coefficient-plane steps (meanFiltFiber,
+calcNormalVectorThreeDirecWithEst, updateEstimationByCoef) bit for bit against golden vectors from the reference's own
 ir.cu built for the host (tests/golden/make_golden_md.py).  CPU only."""
 from __future__ import annotations
 
@@ -69,3 +70,19 @@ def test_md_with_estimate_and_update_bit_exact(oracle, g):
     e = g["est"].ravel().copy()
     oracle.update_estimation(s, g["vol"].ravel().copy(), e, 2)
     assert same(e, g["update_est"])
+
+
+def test_coefficient_steps_bit_exact(oracle, g):
+    s = _scan(g)
+    c = g["coef"].ravel().copy()
+    loss = np.zeros(s.N ** 3, np.float32)
+    oracle.normal_three_est(s, g["vol"].ravel().copy(), c, loss, g["est"].ravel().copy())
+    assert same(c, g["nrm_est_coef"])
+    assert same(loss, g["nrm_est_loss"])
+    cf = g["coef"].ravel().copy()
+    for y in range(1, s.N - 1):
+        oracle.coef_filter_slab(s, y, g["coef"].ravel().copy(), g["vol"].ravel().copy(), cf, 1.0)
+    assert same(cf, g["coef_filter"])
+    e = g["est"].ravel().copy()
+    oracle.update_estimation_coef(s, g["vol"].ravel().copy(), e, 3)
+    assert same(e, g["update_est_coef"])
