@@ -244,6 +244,23 @@ xr_status xr_dev_session_begin_orth(xr_ctx *ctx, const void *d_sino, void *d_vol
  * place, d_loss (N^3) receives |(R e_z) x n|; rot in 0..3 picks the signs. */
 xr_status xr_orth_normal_update(xr_ctx *ctx, const float *d_vol, float *d_coef, float *d_loss, int rot);
 
+/* calcNormalVectorThreeDirecWithEst (ir.cu:976-1071): as xr_orth_normal_update
+ * with each voxel's sign pattern from plane 1 of d_est (2 N^3 floats). */
+xr_status xr_orth_normal_update_est(xr_ctx *ctx, const float *d_vol, float *d_coef, float *d_loss,
+                                    const float *d_est);
+/* meanFiltFiber (ir.cu:1231-1302), `passes` times: each voxel with
+ * 1 <= x, y, z < N-1 gets the direction of its neighbours (weight `weight`,
+ * from their (phi, cos theta) planes in d_coef scaled by the sum of their
+ * three coefficients in d_vol) that lie within 60 degrees of its own, signed
+ * and summed; d_tmp (2 N^3 floats) is scratch; the outer one-voxel border
+ * keeps its values (the reference copies its uninitialised scratch there,
+ * reconstruct.cu:538). */
+xr_status xr_orth_filter(xr_ctx *ctx, float *d_coef, float *d_tmp, const float *d_vol, float weight, int passes);
+/* updateEstimationByCoef (ir.cu:1073-1120): where the cosine between e_z and
+ * the plane normal of the three coefficients exceeds d_est plane 0, planes
+ * 0 / 1 <- (that cosine, iter). */
+xr_status xr_orth_update_estimation(xr_ctx *ctx, const float *d_vol, float *d_est, int iter);
+
 /* ---- main-direction XTT (circleEstReconstruct, reconstruct.cu:1373-1649) -- */
 /* The XTT operators with every voxel's basis rotated by its main direction
  * m (d_md: three planes m_x, m_y, m_z of N^3 floats, FP32): about (-m_y, m_x, 0)

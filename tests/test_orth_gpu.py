@@ -134,3 +134,43 @@ def test_orth_normal_update(oracle, rot):
     unit = lambda c: np.stack([np.cos(c[:n3]), np.sin(c[:n3]), c[n3:]])
     assert np.abs(unit(c_got) - unit(c_ref)).max() <= 1e-4
     assert np.abs(dl.cpu().numpy() - l_ref).max() <= 1e-5
+
+
+def test_orth_coefficient_steps(oracle):
+    """calcNormalVectorThreeDirecWithEst, meanFiltFiber (two passes, border
+    kept) and updateEstimationByCoef against the oracle."""
+    s, ctx, coef = _case(three_axes(), 12, 20, 8, 3, 58)
+    N = s.N
+    rng = np.random.default_rng(59)
+    vol = rng.uniform(0.1, 1.0, (3, N, N, N)).astype(np.float32)
+    est = np.stack([rng.uniform(-1, 1, (N, N, N)), rng.uniform(0, 3.5, (N, N, N))]).astype(np.float32)
+    dv, de = torch.from_numpy(vol).cuda(), torch.from_numpy(est).cuda()
+    n3 = N ** 3
+    unit = lambda c: np.stack([np.cos(c[:n3]), np.sin(c[:n3]), c[n3:]])
+    # WithEst
+    c_ref = coef.ravel().copy()
+    l_ref = np.zeros(n3, np.float32)
+    oracle.normal_three_est(s, vol.ravel().copy(), c_ref, l_ref, est.ravel().copy())
+    dc = torch.from_numpy(coef).cuda()
+    dl = torch.zeros(n3, dtype=torch.float32, device="cuda")
+    ctx.orth_normal_update_est(dv.data_ptr(), dc.data_ptr(), dl.data_ptr(), de.data_ptr())
+    assert np.abs(unit(dc.cpu().numpy().ravel()) - unit(c_ref)).max() <= 1e-4
+    assert np.abs(dl.cpu().numpy() - l_ref).max() <= 1e-5
+    # meanFiltFiber, two passes
+    ref = coef.ravel().copy()
+    for _ in range(2):
+        out = ref.copy()
+        for y in range(1, N - 1):
+            oracle.coef_filter_slab(s, y, ref, vol.ravel().copy(), out, 1.0)
+        ref = out
+    dc = torch.from_numpy(coef).cuda()
+    tmp = torch.empty_like(dc)
+    ctx.orth_filter(dc.data_ptr(), tmp.data_ptr(), dv.data_ptr(), 1.0, 2)
+    assert np.abs(unit(dc.cpu().numpy().ravel()) - unit(ref)).max() <= 1e-4
+    # updateEstimationByCoef
+    ref = est.ravel().copy()
+    oracle.update_estimation_coef(s, vol.ravel().copy(), ref, 3)
+    ctx.orth_update_estimation(dv.data_ptr(), de.data_ptr(), 3)
+    got = de.cpu().numpy().ravel()
+    assert np.array_equal(got[n3:], ref[n3:])
+    assert np.abs(got[:n3] - ref[:n3]).max() <= 1e-6

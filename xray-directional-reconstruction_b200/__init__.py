@@ -149,6 +149,11 @@ _SIGS = {
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float], ctypes.c_int),
     "xr_orth_normal_update": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int],
                               ctypes.c_int),
+    "xr_orth_normal_update_est": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_void_p], ctypes.c_int),
+    "xr_orth_filter": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float,
+                        ctypes.c_int], ctypes.c_int),
+    "xr_orth_update_estimation": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "xr_dev_forward_md": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int],
                           ctypes.c_int),
     "xr_dev_session_begin_md": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
@@ -493,6 +498,21 @@ class Context:
         """calcNormalVectorThreeDirec (ir.cu:856-974) on device buffers."""
         self._check(lib().xr_orth_normal_update(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_coef),
                                                 ctypes.c_void_p(d_loss), int(rot)))
+
+    def orth_normal_update_est(self, d_vol: int, d_coef: int, d_loss: int, d_est: int):
+        """calcNormalVectorThreeDirecWithEst (ir.cu:976-1071) on device buffers."""
+        self._check(lib().xr_orth_normal_update_est(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_coef),
+                                                    ctypes.c_void_p(d_loss), ctypes.c_void_p(d_est)))
+
+    def orth_filter(self, d_coef: int, d_tmp: int, d_vol: int, weight: float = 1.0, passes: int = 1):
+        """meanFiltFiber (ir.cu:1231-1302), `passes` times, on device planes."""
+        self._check(lib().xr_orth_filter(self._h, ctypes.c_void_p(d_coef), ctypes.c_void_p(d_tmp),
+                                         ctypes.c_void_p(d_vol), float(weight), int(passes)))
+
+    def orth_update_estimation(self, d_vol: int, d_est: int, iteration: int):
+        """updateEstimationByCoef (ir.cu:1073-1120)."""
+        self._check(lib().xr_orth_update_estimation(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_est),
+                                                    int(iteration)))
 
     def dev_forward_md(self, d_vol: int, d_md: int, d_sino: int, rotate=Rotate.CW):
         """forwardOrthByMD + chord normalisation over every axis and view (ir.cu:154-231)."""

@@ -1111,6 +1111,45 @@ xr_status xr_orth_normal_update(xr_ctx *c, const float *d_vol, float *d_coef, fl
     return st;
 }
 
+xr_status xr_orth_normal_update_est(xr_ctx *c, const float *d_vol, float *d_coef, float *d_loss, const float *d_est) {
+    if (!c || !d_vol || !d_coef || !d_loss || !d_est) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    if (c->K < 3) return fail(c, XR_ERR_CONFIG, "the normal update needs three basis vectors");
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    st = cuda_check(c, launch_normal_three((long)c->N * c->N * c->N, dbasis(c), d_vol, d_coef, d_loss, 0, c->stream,
+                                           d_est),
+                    "normal update");
+    return st ? st : cuda_check(c, cudaStreamSynchronize(c->stream), "normal update");
+}
+
+xr_status xr_orth_filter(xr_ctx *c, float *d_coef, float *d_tmp, const float *d_vol, float weight, int passes) {
+    if (!c || !d_coef || !d_tmp || !d_vol || passes < 0) return c ? fail(c, XR_ERR_ARG, "bad argument") : XR_ERR_ARG;
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    const size_t bytes = 2 * (size_t)c->N * c->N * c->N * sizeof(float);
+    Timed t(c, XR_T_ORIENT);
+    for (int p = 0; p < passes; p++) {
+        if ((st = cuda_check(c, cudaMemcpyAsync(d_tmp, d_coef, bytes, cudaMemcpyDeviceToDevice, c->stream), "copy")))
+            return st;
+        if ((st = cuda_check(c, launch_coef_filter(c->N, d_coef, d_vol, d_tmp, weight, c->stream), "fiber filter")))
+            return st;
+        if ((st = cuda_check(c, cudaMemcpyAsync(d_coef, d_tmp, bytes, cudaMemcpyDeviceToDevice, c->stream), "copy")))
+            return st;
+    }
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "fiber filter");
+}
+
+xr_status xr_orth_update_estimation(xr_ctx *c, const float *d_vol, float *d_est, int iter) {
+    if (!c || !d_vol || !d_est) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    if (c->K < 3) return fail(c, XR_ERR_CONFIG, "the estimation needs three basis vectors");
+    xr_status st;
+    if ((st = ensure_device(c))) return st;
+    st = cuda_check(c, launch_update_estimation_coef((long)c->N * c->N * c->N, dbasis(c), d_vol, d_est, iter,
+                                                     c->stream),
+                    "estimation");
+    return st ? st : cuda_check(c, cudaStreamSynchronize(c->stream), "estimation");
+}
+
 xr_status xr_dev_forward(xr_ctx *c, const void *d_vol, float *d_sino, xr_rotate dir, int xtt) {
     if (!c || !d_vol || !d_sino) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
     xr_status st;

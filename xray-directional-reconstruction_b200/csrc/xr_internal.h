@@ -213,7 +213,9 @@ cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const
 
 /* ---- xr_orient.cu ---- */
 /* calcNormalVectorThreeDirec (ir.cu:856-974) on every voxel: vol holds the
- * three coefficients (FP32), coef (phi, cos theta) is updated, loss |(R e_z) x n|. */
+ * three coefficients (FP32), coef (phi, cos theta) is updated, loss |(R e_z) x n|;
+ * with est, the sign pattern of each voxel from est plane 1
+ * (calcNormalVectorThreeDirecWithEst, ir.cu:976-1071). */
 /* Main-direction kernels of circleEstReconstruct (ir.cu:624-844, 1304-1363),
  * FP32 planes of N^3: meanFiltFiberMD over 2 <= x, y, z < N-2 into out;
  * calcMainDirection (est null, sign pattern iter) or calcMDWithEst (est
@@ -223,7 +225,12 @@ cudaError_t launch_main_direction(int N, const float *vol, float *md, const floa
 cudaError_t launch_update_estimation(int N, const float *vol, float *est, int iter, cudaStream_t s);
 cudaError_t launch_fill(long n, float *p, float value, cudaStream_t s);
 cudaError_t launch_normal_three(long nvox, const BasisConst *d_basis, const float *vol, float *coef, float *loss,
-                                int rot, cudaStream_t s);
+                                int rot, cudaStream_t s, const float *est = nullptr);
+/* meanFiltFiber (ir.cu:1231-1302) over 1 <= x, y, z < N-1 into out;
+ * updateEstimationByCoef (ir.cu:1073-1120). */
+cudaError_t launch_coef_filter(int N, const float *coef, const float *vol, float *out, float w, cudaStream_t s);
+cudaError_t launch_update_estimation_coef(long nvox, const BasisConst *d_basis, const float *vol, float *est, int iter,
+                                          cudaStream_t s);
 cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, const void *mu, float *md,
                                float *ev, int storage, cudaStream_t s);
 cudaError_t launch_angle_from_md(long nvox, const float *md, float *angle, cudaStream_t s);

@@ -103,8 +103,14 @@ __device__ __forceinline__ void normalize3(float v[3]) {
  * (mu0 S0 - mu1' S1) x (mu0 S0 - mu2' S2) (signs of mu1, mu2 by rot), turned
  * by the voxel's current rotation, z >= 0, becomes the new (phi, cos theta);
  * loss = |(R e_z) x normal|. */
-__global__ void k_normal_three(long nvox, const BasisConst *B, const float *vol, float *coef, float *loss, int rot) {
+__global__ void k_normal_three(long nvox, const BasisConst *B, const float *vol, float *coef, float *loss, int rot_all,
+                               const float *est) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nvox; i += (long)gridDim.x * blockDim.x) {
+        int rot = rot_all;
+        if (est) {   /* calcNormalVectorThreeDirecWithEst (ir.cu:976-1071): pattern from estimate plane 1 */
+            const float r = est[nvox + i];
+            rot = r < 0.5f ? 0 : (r < 1.5f ? 1 : (r < 2.5f ? 2 : 3));
+        }
         float R[9];
         orth_rotation(coef, (size_t)nvox, (size_t)i, R);
         const float mu0 = vol[i], m1 = vol[nvox + i], m2 = vol[2 * nvox + i];
@@ -228,6 +234,80 @@ __global__ void k_update_estimation(int N, const float *vol, float *est, int ite
     }
 }
 
+/* meanFiltFiber, ir.cu:1231-1302, for 1 <= x, y, z < N-1: each neighbour's
+ * direction from its (phi, cos theta) planes as mu (sin t cos(phi - pi/2),
+ * sin t sin(phi - pi/2), cos t), mu the sum of its three coefficients; the
+ * pairs (i, 26 - i) within 60 degrees of the centre (|dot| > 0.5) added
+ * signed to it (weight w), normalised, z >= 0, back to (phi, cos theta). */
+__global__ void k_coef_filter(int N, const float *coef, const float *vol, float *out, float w) {
+    const long n3 = (long)N * N * N, M = N - 2;
+    const long nint = M > 0 ? M * M * M : 0;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += (long)gridDim.x * blockDim.x) {
+        const long x = 1 + t % M, y = 1 + (t / M) % M, z = 1 + t / (M * M);
+        float nv[27][3];
+        int cnt = 0;
+        for (int i = -1; i < 2; i++)
+            for (int j = -1; j < 2; j++)
+                for (int k = -1; k < 2; k++) {
+                    const long o = (x - i) + N * ((y - j) + (long)N * (z - k));
+                    const float ct = coef[n3 + o];
+                    const float st = sqrtf(1.f - ct * ct);
+                    const float phi = __double2float_rn(-1.5707963267948966 + (double)coef[o]);
+                    const float mu = __fadd_rn(__fadd_rn(vol[o], vol[n3 + o]), vol[2 * n3 + o]);
+                    nv[cnt][0] = mu * (st * cosf(phi));
+                    nv[cnt][1] = mu * (st * sinf(phi));
+                    nv[cnt][2] = mu * ct;
+                    cnt++;
+                }
+        float c[3] = {nv[13][0], nv[13][1], nv[13][2]};
+        for (int i = 0; i < 13; i++) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const float *a = nv[h ? 26 - i : i];
+                const float d = __fadd_rn(__fadd_rn(__fmul_rn(a[0], nv[13][0]), __fmul_rn(a[1], nv[13][1])),
+                                          __fmul_rn(a[2], nv[13][2]));
+                if (d > 0.5f) {
+                    c[0] = __fadd_rn(c[0], __fmul_rn(w, a[0]));
+                    c[1] = __fadd_rn(c[1], __fmul_rn(w, a[1]));
+                    c[2] = __fadd_rn(c[2], __fmul_rn(w, a[2]));
+                } else if (d < -0.5f) {
+                    c[0] = __fsub_rn(c[0], __fmul_rn(w, a[0]));
+                    c[1] = __fsub_rn(c[1], __fmul_rn(w, a[1]));
+                    c[2] = __fsub_rn(c[2], __fmul_rn(w, a[2]));
+                }
+            }
+        }
+        normalize3(c);
+        if (c[2] < 0.f) { c[0] = -c[0]; c[1] = -c[1]; c[2] = -c[2]; }
+        const long ci = x + N * (y + (long)N * z);
+        out[ci] = atan2f(c[0], -c[1]);   /* e_z x c = (-c1, c0, 0) */
+        out[n3 + ci] = c[2];
+    }
+}
+
+/* updateEstimationByCoef, ir.cu:1073-1120: the plane normal of the three
+ * coefficients (no signs), z >= 0; where its cosine to e_z exceeds estimate
+ * plane 0, planes 0/1 <- (cosine, iter). */
+__global__ void k_update_estimation_coef(long nvox, const BasisConst *B, const float *vol, float *est, int iter) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nvox; i += (long)gridDim.x * blockDim.x) {
+        const float mu0 = vol[i], mu1 = vol[nvox + i], mu2 = vol[2 * nvox + i];
+        float v1[3], v2[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            v1[j] = mu0 * B->S[j] - mu1 * B->S[3 + j];
+            v2[j] = mu0 * B->S[j] - mu2 * B->S[6 + j];
+        }
+        float n[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2], v1[0] * v2[1] - v1[1] * v2[0]};
+        normalize3(n);
+        if (n[2] < 0.f) { n[0] = -n[0]; n[1] = -n[1]; n[2] = -n[2]; }
+        normalize3(n);
+        if (n[2] > est[i]) {
+            est[i] = n[2];
+            est[nvox + i] = (float)iter;
+        }
+    }
+}
+
 __global__ void k_fill(long n, float *p, float value) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) p[i] = value;
 }
@@ -271,9 +351,22 @@ cudaError_t launch_fill(long n, float *p, float value, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+cudaError_t launch_coef_filter(int N, const float *coef, const float *vol, float *out, float w, cudaStream_t s) {
+    const long M = N - 2;
+    if (M <= 0) return cudaSuccess;
+    k_coef_filter<<<grid_for(M * M * M, 128), 128, 0, s>>>(N, coef, vol, out, w);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update_estimation_coef(long nvox, const BasisConst *d_basis, const float *vol, float *est, int iter,
+                                          cudaStream_t s) {
+    k_update_estimation_coef<<<grid_for(nvox, 256), 256, 0, s>>>(nvox, d_basis, vol, est, iter);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_normal_three(long nvox, const BasisConst *d_basis, const float *vol, float *coef, float *loss,
-                                int rot, cudaStream_t s) {
-    k_normal_three<<<grid_for(nvox, 256), 256, 0, s>>>(nvox, d_basis, vol, coef, loss, rot);
+                                int rot, cudaStream_t s, const float *est) {
+    k_normal_three<<<grid_for(nvox, 256), 256, 0, s>>>(nvox, d_basis, vol, coef, loss, rot, est);
     return cudaGetLastError();
 }
 
