@@ -579,20 +579,32 @@ __global__ void __launch_bounds__(kBackThreads, 4) k_back_col(BackColArgs a) {
         const int x = bx0 + (lv & 7), y = by0 + ((lv >> 3) & 7), z = bz0 + (lv >> 6);
         if (x >= N || y >= N || z >= N) continue;
         const size_t idx = (size_t)x + (size_t)N * y + NN * z;
-        for (int k = 0; k < K; k++) {
-            const float t = sacc[k * 512 + sacc_slot(lv)];
-            if (MODE == B_SENS) {
-                a.fac_out[idx + (size_t)k * N3] = t;
-            } else {
-                T *vp = reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3;
-                const float mu = ldf<T>(vp);
-                const uint32_t key = (uint32_t)(idx + (size_t)k * N3);
-                if (a.art) {
-                    stu<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, t)), key, a.sr);
-                } else {
-                    const float f = a.fac_in[idx + (size_t)k * N3];
-                    stu<T>(vp, (f == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, t), f), key, a.sr);
+        if (MODE == B_SENS) {
+            for (int k = 0; k < K; k++) a.fac_out[idx + (size_t)k * N3] = sacc[k * 512 + sacc_slot(lv)];
+            continue;
+        }
+        /* eight channels at a time: their loads are all in flight before the
+         * first store (a load-update-store chain per channel would wait for
+         * each load in turn) */
+        for (int k0 = 0; k0 < K; k0 += 8) {
+            float mu[8], f[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int k = k0 + j;
+                if (k < K) {
+                    mu[j] = ldf<T>(reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3);
+                    f[j] = a.art ? 0.f : __ldg(a.fac_in + idx + (size_t)k * N3);
                 }
+            }
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int k = k0 + j;
+                if (k >= K) break;
+                const float t = sacc[k * 512 + sacc_slot(lv)];
+                T *vp = reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3;
+                const uint32_t key = (uint32_t)(idx + (size_t)k * N3);
+                if (a.art) stu<T>(vp, __fadd_rn(mu[j], __fmul_rn(a.alpha, t)), key, a.sr);
+                else stu<T>(vp, (f[j] == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu[j], t), f[j]), key, a.sr);
             }
         }
     }
