@@ -567,14 +567,23 @@ __global__ void __launch_bounds__(kBackThreads) k_back_update(BackArgs a) {
         if (a.art) stu<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmp)), (uint32_t)idx, a.sr);
         else stu<T>(vp, (fac == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmp), fac), (uint32_t)idx, a.sr);
     } else {
+        /* four channels' loads in flight before their first store */
 #pragma unroll
-        for (int k = 0; k < 16; k++) {
-            if (k >= g.K) break;
-            T *vp = reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3;
-            const float mu = ldf<T>(vp);
-            const uint32_t key = (uint32_t)(idx + (size_t)k * N3);
-            if (a.art) stu<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmpk[k])), key, a.sr);
-            else stu<T>(vp, (fack[k] == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmpk[k]), fack[k]), key, a.sr);
+        for (int k0 = 0; k0 < 16; k0 += 4) {
+            if (k0 >= g.K) break;
+            float mu[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (k0 + j < g.K) mu[j] = ldf<T>(reinterpret_cast<T *>(a.vol) + idx + (size_t)(k0 + j) * N3);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int k = k0 + j;
+                if (k >= g.K) break;
+                T *vp = reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3;
+                const uint32_t key = (uint32_t)(idx + (size_t)k * N3);
+                if (a.art) stu<T>(vp, __fadd_rn(mu[j], __fmul_rn(a.alpha, tmpk[k])), key, a.sr);
+                else stu<T>(vp, (fack[k] == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu[j], tmpk[k]), fack[k]), key, a.sr);
+            }
         }
     }
 }
