@@ -451,6 +451,14 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
         /* XTT::reconstruct epoch, reconstruct.cu:857-917: the ratio images of
          * every axis are cleared once per epoch. */
         cudaMemsetAsync(proj, 0, (size_t)c->C * blk * sizeof(float), str);
+        /* ratio_dst: a view's ratio image is final after the last subset of the
+         * epoch that holds it (views recur when V % batch != 0) */
+        std::vector<int> last;
+        if (s.ratio_dst) {
+            last.assign(c->V, -1);
+            for (int b = 0; b < s.batch; b++)
+                for (int j = 0; j < s.subset_size; j++) last[((long)orders[b] + (long)s.batch * j) % c->V] = b;
+        }
         for (int b = 0; b < s.batch; b++) {
             const int *vl = (const int *)c->subsets.p + (size_t)orders[b] * s.subset_size;
             {
@@ -473,6 +481,22 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                 if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, nrm,
                                                      s.d_sino, s.art, dl, s.sino_storage, str), "ratio")))
                     return st;
+            }
+            if (s.ratio_dst) {
+                cudaStream_t cs = c->copy_stream;
+                if ((st = cuda_check(c, cudaEventRecord(c->copy_ev[0], str), "cudaEventRecord"))) return st;
+                if ((st = cuda_check(c, cudaStreamWaitEvent(cs, c->copy_ev[0], 0), "cudaStreamWaitEvent"))) return st;
+                for (int j = 0; j < s.subset_size; j++) {
+                    const int n = (int)(((long)orders[b] + (long)s.batch * j) % c->V);
+                    if (last[n] != b) continue;
+                    for (int cond = 0; cond < c->C; cond++) {
+                        const size_t off = (size_t)n * NdNd;
+                        if ((st = cuda_check(c, cudaMemcpyAsync(s.ratio_dst[cond] + off, proj + cond * blk + off,
+                                                                NdNd * sizeof(float), cudaMemcpyDeviceToHost, cs),
+                                             "ratio images")))
+                            return st;
+                    }
+                }
             }
             {
                 Timed t(c, XR_T_BACK);
@@ -1378,9 +1402,15 @@ xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
         xr_dev_session_end(c, nullptr, nullptr);
         return st;
     }
+    /* the last epoch hands each view's final ratio image to the copy stream
+     * as soon as its subset is done (not inside a captured epoch graph) */
+    const bool early = !c->use_graphs && epoch > 0;
     for (int ep = 0; ep < epoch; ep++) {
         double l = 0;
-        if ((st = xr_dev_session_epoch(c, losses ? &l : nullptr))) return st;
+        if (early && ep == epoch - 1) c->sess.ratio_dst = sino;
+        st = xr_dev_session_epoch(c, losses ? &l : nullptr);
+        c->sess.ratio_dst = nullptr;
+        if (st) return st;
         if (losses) losses[ep] = (float)l;
     }
     float *d_md = nullptr, *d_ev = nullptr;
@@ -1389,9 +1419,11 @@ xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
         d_md = (float *)c->scratch_md.p;
         d_ev = evalue ? d_md + 3 * N3 : nullptr;
     }
-    /* the ratio images are final after the last epoch */
-    if ((st = stream_after(c, cs, c->stream, c->copy_ev[0]))) return st;
-    if ((st = download_planes_async(c, (const float *)c->proj.p, sino, c->C, blk, "ratio images", cs))) return st;
+    if (!early) {   /* the ratio images are final after the last epoch */
+        if ((st = stream_after(c, cs, c->stream, c->copy_ev[0]))) return st;
+        if ((st = download_planes_async(c, (const float *)c->proj.p, sino, c->C, blk, "ratio images", cs)))
+            return st;
+    }
     const void *d_vol = c->scratch_vol.p;
     auto after = [&](int phase) -> xr_status {
         xr_status s2 = stream_after(c, cs, c->stream, c->copy_ev[1 + phase]);

@@ -95,6 +95,7 @@ struct Session {
     const float *coef = nullptr;      /* orientation-parametrised XTT: rotation planes */
     int coef_kind = 0;                /* 0: (phi, cos theta); 1: main direction (3 planes) */
     cudaEvent_t sino_ready = nullptr; /* set: the first ratio launch waits for it (sinogram upload) */
+    float *const *ratio_dst = nullptr; /* set: each view's final ratio image to these host planes */
     std::vector<int> order;            /* persistent subset order (XTT)     */
     std::vector<int> ir_orders;        /* C*epochs rows (IR)                */
     std::map<std::vector<int>, cudaGraphExec_t> graphs;  /* per subset order */
