@@ -3,7 +3,7 @@
  * compiled for the CPU through the CUDA shim in this folder.
  *
  * TEST INFRASTRUCTURE ONLY (the checker and the timed CPU baseline).  The
- * kernels are the reference's, compiled from /root/reference in place; the
+ * kernels are the reference's, compiled from its source tree in place; the
  * host loops below restate the reference's schedulers:
  *   ref_ir_reconstruct   <- IR::reconstruct   reconstruct/src/reconstruct.cu:23-156
  *   ref_xtt_reconstruct  <- XTT::reconstruct  reconstruct/src/reconstruct.cu:799-927
