@@ -191,3 +191,30 @@ def test_raw_volume_io(tmp_path):
     assert np.array_equal(w.get(), v.get())
     with pytest.raises(IOError):
         w.load(name, 8, 8, 8)
+
+
+def test_orientation_step_arguments_rejected():
+    """The orientation-parametrised and main-direction entry points reject
+    null buffers, out-of-range sign patterns and too few basis vectors with
+    XR_ERR_ARG (1) / XR_ERR_CONFIG (6) before touching a device."""
+    xr = load_xr()
+    rot = np.eye(3, dtype=np.float32).ravel()
+    basis = np.eye(3, dtype=np.float32)
+    ctx = xr.Context.create(1000, 500, 2, 8, 12, 4, rot, basis=basis)
+    calls = [lambda: ctx.md_filter(0, 0), lambda: ctx.md_main_direction(0, 0, 0),
+             lambda: ctx.md_with_estimate(0, 0, 0), lambda: ctx.md_update_estimation(0, 0, 1),
+             lambda: ctx.orth_filter(0, 0, 0), lambda: ctx.orth_update_estimation(0, 0, 1),
+             lambda: ctx.orth_normal_update_est(0, 0, 0, 0), lambda: ctx.dev_forward_md(0, 0, 0),
+             lambda: ctx.dev_session_begin_md(0, 0, 0, 1, 1), lambda: ctx.md_main_direction(8, 8, 4),
+             lambda: ctx.md_filter(8, 8, 1.0, -1)]
+    for call in calls:
+        with pytest.raises(xr.XRError) as e:
+            call()
+        assert e.value.status == 1
+    ctx.close()
+    one = xr.Context.create(1000, 500, 2, 8, 12, 4, rot)            # K = 1
+    for call in [lambda: one.md_main_direction(8, 8, 0), lambda: one.orth_update_estimation(8, 8, 0)]:
+        with pytest.raises(xr.XRError) as e:
+            call()
+        assert e.value.status == 6
+    one.close()
