@@ -159,6 +159,15 @@ class Oracle:
         self._fn("update_estimation_coef", dt)(ctypes.byref(self._scan(s)), _p(vol, dt), _p(est, dt),
                                                int(iteration))
 
+    def fiber_forward_view(self, s, cond, n, vol, proj, dt=np.float32):
+        """forwardProjFiber (fiber.cu:13-153) of one view into proj (axis block, all views)."""
+        self._fn("fiber_forward_view", dt)(ctypes.byref(self._scan(s)), cond, n, _p(vol, dt), _p(proj, dt))
+
+    def fiber_backward_slab(self, s, cond, y, n, proj, vol, tmp, factor, dt=np.float32):
+        """backwardProjFiber (fiber.cu:155-226) of slab y, view n."""
+        self._fn("fiber_backward_slab", dt)(ctypes.byref(self._scan(s)), cond, y, n, _p(proj, dt), _p(vol, dt),
+                                            _p(tmp, dt), _p(factor, dt))
+
     def correlation(self, s, cond, n, proj, factor, dt=np.float32):
         self._fn("correlation", dt)(ctypes.byref(self._scan(s)), cond, n, _p(proj, dt), _p(factor, dt))
 
@@ -302,6 +311,12 @@ class RefHost:
     def update_estimation_coef(self, vol, est, iteration):
         loss = np.zeros(self.s.N ** 3, np.float32)
         self.lib.xr_ref_update_estimation_coef(_p(vol), _p(loss), _p(est), int(iteration))
+
+    def fiber_forward(self, cond, n, vol, proj):
+        self.lib.xr_ref_fiber_forward(cond, n, _p(vol), _p(proj))
+
+    def fiber_backward(self, cond, y, n, proj, vol, tmp, factor):
+        self.lib.xr_ref_fiber_backward(cond, y, n, _p(proj), _p(vol), _p(tmp), _p(factor))
 
     def md_filter(self, y, md, out, coef):
         self.lib.xr_ref_md_filter(int(y), _p(md), _p(out), ctypes.c_float(coef))

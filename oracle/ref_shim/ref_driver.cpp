@@ -19,6 +19,7 @@
 #include "params.h"
 #include <geometry.h>
 #include <ir.cuh>
+#include <fiber.cuh>
 
 #include <algorithm>
 #include <random>
@@ -187,6 +188,17 @@ void xr_ref_coef_filter(int y, const float *coef, float *out, const float *vol, 
 void xr_ref_update_estimation_coef(const float *vol, float *loss, float *est, int iter) {
     for (int y = 0; y < g.geom.voxel; y++)
         launch2d(g.gridV, g.blockV, updateEstimationByCoef, vol, y, (const Geometry *)&g.geom, loss, est, iter);
+}
+
+/* forwardProjFiber (fiber.cu:80-153): one view, every y slab. */
+void xr_ref_fiber_forward(int cond, int n, float *vol, float *proj) {
+    for (int y = 0; y < g.geom.voxel; y++)
+        launch2d(g.gridV, g.blockV, forwardProjFiber, proj, vol, &g.geom, cond, y, n);
+}
+
+/* backwardProjFiber (fiber.cu:217-226): slab y, view n. */
+void xr_ref_fiber_backward(int cond, int y, int n, float *proj, float *vol, float *tmp, float *factor) {
+    launch2d(g.gridV, g.blockV, backwardProjFiber, proj, vol, tmp, factor, &g.geom, cond, y, n);
 }
 
 void xr_ref_correlation(int cond, int n, float *proj, const float *factor) {

@@ -701,6 +701,100 @@ void RV(update_estimation_coef)(const or_scan *s, const real *vol, real *est, in
     }
 }
 
+/* rayCastingFiber, fiber.cu:228-278: rayCasting's source and rotation, but
+ * voxel centres at (2i - N + 1)/2 and the detector v axis along -R e_z. */
+static void RV(raycast_fiber)(const or_scan *s, const RV(frame) * f, int x, int y, int z, real *u, real *v,
+                              real *B) {
+    const real vs = RV(vox_size)(s);
+    const real N = (real)s->N;
+    const int xyz[3] = {x, y, z};
+    real org[3], d[3], p[3];
+    for (int i = 0; i < 3; i++)
+        org[i] = ((real)2.0 * (real)xyz[i] - N + (real)1.0) * (real)0.5 * vs - f->off[i] - f->t[i];
+    for (int i = 0; i < 3; i++) d[i] = org[i] + (-f->src[i]);
+    const real coeff = -(f->ss) / RV(dot3)(f->src, d);
+    for (int i = 0; i < 3; i++) p[i] = f->src[i] + coeff * d[i];
+    const real mag = (real)s->sdd / (real)s->sod;
+    const real evn[3] = {-f->ev[0], -f->ev[1], -f->ev[2]};
+    *u = RV(dot3)(p, f->eu) * mag / (real)s->det + (real)0.5 * (real)s->Nd;
+    *v = RV(dot3)(p, evn) * mag / (real)s->det + (real)0.5 * (real)s->Nd;
+    const real val = RSQRT(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    for (int i = 0; i < 3; i++) B[i] = (val > (real)1e-8f) ? d[i] / val : (real)0;
+}
+
+/* The fiber model's signed projection of voxel idx: ps = (B x G).(f0, f1, f2)
+ * + f3 (fiber.cu:53-58, channels beyond the fourth are not read); the weight
+ * used is |ps|, its sign s. */
+static real RV(fiber_signed)(const or_scan *s, const real *B, const real *G, const real *vol, long idx, long N3,
+                             real *bxg) {
+    bxg[0] = B[1] * G[2] - B[2] * G[1];
+    bxg[1] = B[2] * G[0] - B[0] * G[2];
+    bxg[2] = B[0] * G[1] - B[1] * G[0];
+    real ps = (real)0;
+    const int K = s->K < 4 ? s->K : 4;
+    for (int i = 0; i < K; i++) ps += (i >= 3 ? (real)1.0f : bxg[i]) * vol[idx + (long)i * N3];
+    return ps;
+}
+
+/* forwardProjFiber / forwardFiberModel, fiber.cu:13-78 and 80-153: one view
+ * over every y slab, proj[tap] += c * vs * ratio * |ps|; no weight image. */
+void RV(fiber_forward_view)(const or_scan *s, int cond, int n, const real *vol, real *proj) {
+    RV(frame) f;
+    RV(view_frame)(s, cond, n, 0, &f);
+    const long N = s->N, Nd = s->Nd, N3 = N * N * N;
+    const long nn = n < 0 ? -n : n;
+    const real vs = RV(vox_size)(s);
+    const real ratio = (vs * vs) / ((real)s->det * ((real)s->sod / (real)s->sdd) * (real)s->det *
+                                    ((real)s->sod / (real)s->sdd));
+    for (long y = 0; y < N; y++)
+        for (long z = 0; z < N; z++)
+            for (long x = 0; x < N; x++) {
+                real u, v, B[3], c[4], bxg[3];
+                long iu, iv;
+                RV(raycast_fiber)(s, &f, (int)x, (int)y, (int)z, &u, &v, B);
+                if (!RV(taps)(s, u, v, &iu, &iv, c)) continue;
+                const long idx = x + N * y + N * N * z;
+                const real ps = RV(fiber_signed)(s, B, f.ev, vol, idx, N3, bxg);
+                const real pr = ps * (ps >= (real)0 ? (real)1.0f : -(real)1.0f);
+                const long base = Nd * Nd * nn;
+                proj[iu + Nd * (iv + 1) + base] += c[0] * vs * ratio * pr;
+                proj[(iu + 1) + Nd * (iv + 1) + base] += c[1] * vs * ratio * pr;
+                proj[(iu + 1) + Nd * iv + base] += c[2] * vs * ratio * pr;
+                proj[iu + Nd * iv + base] += c[3] * vs * ratio * pr;
+            }
+}
+
+/* backwardProjFiber / backwardFiberModel, fiber.cu:155-226, slab y, view n:
+ * channel i gets w_i = |(B x G)_i s| (i < 3) or 1, tmp_i += w_i sum c r,
+ * factor_i += w_i (K planes of N*N). */
+void RV(fiber_backward_slab)(const or_scan *s, int cond, int y, int n, const real *proj, const real *vol, real *tmp,
+                             real *factor) {
+    RV(frame) f;
+    RV(view_frame)(s, cond, n, 0, &f);
+    const long N = s->N, Nd = s->Nd, N3 = N * N * N;
+    const long nn = n < 0 ? -n : n;
+    const int K = s->K < 4 ? s->K : 4;
+    for (long z = 0; z < N; z++)
+        for (long x = 0; x < N; x++) {
+            real u, v, B[3], c[4], bxg[3];
+            long iu, iv;
+            RV(raycast_fiber)(s, &f, (int)x, y, (int)z, &u, &v, B);
+            if (!RV(taps)(s, u, v, &iu, &iv, c)) continue;
+            const real ps = RV(fiber_signed)(s, B, f.ev, vol, x + N * y + N * N * z, N3, bxg);
+            const real sg = ps >= (real)0 ? (real)1.0f : -(real)1.0f;
+            const long base = Nd * Nd * nn;
+            const real p0 = proj[iu + Nd * (iv + 1) + base], p1 = proj[(iu + 1) + Nd * (iv + 1) + base];
+            const real p2 = proj[(iu + 1) + Nd * iv + base], p3 = proj[iu + Nd * iv + base];
+            for (int i = 0; i < K; i++) {
+                const real w = (i >= 3) ? (real)1.0f : RFABS(bxg[i] * sg);
+                const real bf = w * c[0] * p0 + w * c[1] * p1 + w * c[2] * p2 + w * c[3] * p3;
+                const long idx = x + N * z + (long)i * N * N;
+                factor[idx] += w;
+                tmp[idx] += bf;
+            }
+        }
+}
+
 /* voxelProduct (ir.cu:1637-1654, MLEM) or voxelPlus (ir.cu:1682-1693, ART)
  * on slab y of one channel. */
 void RV(voxel_update)(const or_scan *s, int y, real *vol, const real *tmp, const real *factor, int art,

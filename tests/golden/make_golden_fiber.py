@@ -1,0 +1,59 @@
+"""Golden vectors of the reference's fiber-model projectors (forwardProjFiber,
+backwardProjFiber; reconstruct/src/fiber.cu) from its host build
+(oracle/_ref/libxrref.so, serial launch order), for K = 3 and K = 4.
+
+    python tests/golden/make_golden_fiber.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+from oracle import RefHost, Scan, build  # noqa: E402
+from scans import basis13, three_axes  # noqa: E402
+
+
+def fiber_scan(K: int) -> Scan:
+    rng = np.random.default_rng(90 + K)
+    return Scan(sdd=1000.0, sod=500.0, det=2.0, N=12, Nd=20, V=10, rot=three_axes(),
+                trans=rng.normal(0, 0.3, (3, 3)), offset=rng.normal(0, 0.2, (3, 3)), basis=basis13()[:K])
+
+
+def main() -> None:
+    build(ref=True)
+    out = {}
+    for K in (3, 4):
+        R = RefHost(parallel=False)
+        s = fiber_scan(K)
+        R.setup(s)
+        rng = np.random.default_rng(95 + K)
+        N, Nd, V = s.N, s.Nd, s.V
+        vol = rng.normal(0, 1, (K, N, N, N)).astype(np.float32)
+        ratio = rng.uniform(0.0, 2.0, (V, Nd, Nd)).astype(np.float32)
+        out[f"k{K}_geom"] = np.array([s.sdd, s.sod, s.det, N, Nd, V], np.float64)
+        out.update({f"k{K}_rot": s.rot, f"k{K}_trans": s.trans, f"k{K}_offset": s.offset, f"k{K}_basis": s.basis,
+                    f"k{K}_vol": vol, f"k{K}_ratio": ratio})
+        for cond in range(3):
+            n = 2 + 3 * cond
+            p = np.zeros(V * Nd * Nd, np.float32)
+            R.fiber_forward(cond, n, vol.ravel().copy(), p)
+            out[f"k{K}_fwd_c{cond}"] = p[n * Nd * Nd:(n + 1) * Nd * Nd].copy()
+            tmp = np.zeros(K * N * N, np.float32)
+            fac = np.zeros(K * N * N, np.float32)
+            R.fiber_backward(cond, 4, n, ratio.ravel().copy(), vol.ravel().copy(), tmp, fac)
+            out[f"k{K}_bwd_c{cond}_tmp"] = tmp
+            out[f"k{K}_bwd_c{cond}_fac"] = fac
+    path = os.path.join(HERE, "ref_fiber_small.npz")
+    np.savez_compressed(path, **out)
+    print(path, len(out), "arrays")
+
+
+if __name__ == "__main__":
+    main()

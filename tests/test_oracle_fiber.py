@@ -1,0 +1,41 @@
+"""Pin the oracle's fiber-model restatement (forwardProjFiber,
+backwardProjFiber with rayCastingFiber's frame) bit for bit against golden
+vectors from the reference's own fiber.cu built for the host
+(tests/golden/make_golden_fiber.py).  CPU only."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from oracle import Scan
+
+
+@pytest.fixture(scope="module")
+def g():
+    return np.load(os.path.join(ROOT, "tests", "golden", "ref_fiber_small.npz"))
+
+
+def _scan(g, K) -> Scan:
+    sdd, sod, det, N, Nd, V = g[f"k{K}_geom"]
+    return Scan(sdd=float(sdd), sod=float(sod), det=float(det), N=int(N), Nd=int(Nd), V=int(V), rot=g[f"k{K}_rot"],
+                trans=g[f"k{K}_trans"], offset=g[f"k{K}_offset"], basis=g[f"k{K}_basis"])
+
+
+@pytest.mark.parametrize("K", [3, 4])
+@pytest.mark.parametrize("cond", [0, 1, 2])
+def test_fiber_projectors_bit_exact(oracle, g, K, cond):
+    s = _scan(g, K)
+    N, Nd, V = s.N, s.Nd, s.V
+    n = 2 + 3 * cond
+    vol = g[f"k{K}_vol"].ravel()
+    p = np.zeros(V * Nd * Nd, np.float32)
+    oracle.fiber_forward_view(s, cond, n, vol.copy(), p)
+    assert np.array_equal(p[n * Nd * Nd:(n + 1) * Nd * Nd], g[f"k{K}_fwd_c{cond}"])
+    tmp = np.zeros(K * N * N, np.float32)
+    fac = np.zeros(K * N * N, np.float32)
+    oracle.fiber_backward_slab(s, cond, 4, n, g[f"k{K}_ratio"].ravel().copy(), vol.copy(), tmp, fac)
+    assert np.array_equal(tmp, g[f"k{K}_bwd_c{cond}_tmp"])
+    assert np.array_equal(fac, g[f"k{K}_bwd_c{cond}_fac"])
