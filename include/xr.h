@@ -293,6 +293,36 @@ xr_status xr_md_with_estimate(xr_ctx *ctx, const float *d_vol, float *d_md, cons
 /* updateEstimation (ir.cu:791-844): where mu_2^2 + (1 - lo/hi)^2 of the
  * coefficients is below d_est plane 0, planes 0 / 1 <- (that loss, iter). */
 xr_status xr_md_update_estimation(xr_ctx *ctx, const float *d_vol, float *d_est, int iter);
+/* ---- fiber model (reconstruct/src/fiber.cu; XTT::fiberModelReconstruct,
+ *      reconstruct.cuh:54-55, reconstruct.cu:1242-1371) ------------------ */
+/* Every voxel holds a fiber vector F = (mu_0, mu_1, mu_2) and, with K = 4, an
+ * isotropic term mu_3; a ray of unit direction B through the grating of
+ * direction G sees ps = (B x G) . F + mu_3 (fiber.cu:53-58).  The ray casting
+ * is rayCastingFiber's (fiber.cu:228-278): voxel centres at (2i - N + 1)/2
+ * and the detector v axis along -G.  These calls need K = 3 or 4 (the
+ * reference indexes exactly four planes, fiber.cu:19-24) and FP32 volumes.
+ *
+ * forwardProjFiber (fiber.cu:13-153) of every axis and view: d_sino
+ * (C*V*Nd^2, cleared first) receives c * vs * ratio * |ps| per bilinear tap;
+ * no chord-length normalisation, no weight image. */
+xr_status xr_dev_forward_fiber(xr_ctx *ctx, const float *d_vol, float *d_sino, xr_rotate dir);
+/* A session (xr_dev_session_epoch / _end as usual) of fiberModelReconstruct's
+ * epochs (reconstruct.cu:1286-1352): per subset forwardProjFiber ->
+ * projRatio / projSubtract over every axis, then backwardProjFiber
+ * (fiber.cu:155-226) over every axis and view with voxelProduct / voxelPlus of
+ * channel 0 alone (the reference updates the first N^3 of devVoxel,
+ * :1341-1345); the subset order is the XTT session's (a default
+ * std::mt19937_64 each epoch, :1296-1297).  The session end applies no
+ * voxelSqrt and no orientation (d_md and d_evalue are ignored). */
+xr_status xr_dev_session_begin_fiber(xr_ctx *ctx, const void *d_sino, float *d_vol, int epochs, int batch,
+                                     xr_rotate dir, xr_method method, float lambda);
+/* fiberModelReconstruct on host buffers: voxel[K] is set to 0.01 first
+ * (:1245-1247) and receives the result; sino[C] is overwritten with the last
+ * ratio images (:1355-1356; zeros when epoch = 0).  losses: NULL or epoch raw
+ * sums of |b - Ax|. */
+xr_status xr_fiber_reconstruct(xr_ctx *ctx, float *const *sino, float *const *voxel, int epoch, int batch,
+                               xr_rotate dir, xr_method method, float lambda, float *losses);
+
 /* fillVolume (ir.cu:846-854): n device floats <- value. */
 xr_status xr_dev_fill(xr_ctx *ctx, float *d, size_t n, float value);
 

@@ -242,6 +242,18 @@ inline void reconstruct(Volume<float> *sinogram, Volume<float> *voxel, Volume<fl
                                  xr::rotate_of(dir), xr::method_of(method), lambda, nullptr),
               "XTT::reconstruct");
 }
+
+/* reconstruct.cuh:54-55: the fiber model, channel 0 updated, every channel
+ * starting at 0.01; sinogram receives the last ratio images. */
+inline void fiberModelReconstruct(Volume<float> *sinogram, Volume<float> *voxel, const Geometry &geom, int epoch,
+                                  int batch, Rotate dir, Method method, float lambda = 1e-2) {
+    xr::check_geom(geom);
+    auto s = xr::ptrs(sinogram, NUM_PROJ_COND);
+    auto v = xr::ptrs(voxel, NUM_BASIS_VECTOR);
+    xr::check(xr_fiber_reconstruct(xr::need(), s.data(), v.data(), epoch, batch, xr::rotate_of(dir),
+                                   xr::method_of(method), lambda, nullptr),
+              "XTT::fiberModelReconstruct");
+}
 }  // namespace XTT
 
 /* reconstruct.cuh:33-39 */

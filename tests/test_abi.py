@@ -218,3 +218,30 @@ def test_orientation_step_arguments_rejected():
             call()
         assert e.value.status == 6
     one.close()
+
+
+def test_fiber_arguments_rejected():
+    """The fiber-model entry points reject null buffers and negative epoch
+    counts with XR_ERR_ARG (1), and K outside {3, 4} or 16-bit volume storage
+    with XR_ERR_CONFIG (6), before touching a device."""
+    xr = load_xr()
+    rot = np.eye(3, dtype=np.float32).ravel()
+    ctx = xr.Context.create(1000, 500, 2, 8, 12, 4, rot, basis=np.eye(3, dtype=np.float32))
+    for call in [lambda: ctx.dev_forward_fiber(0, 0), lambda: ctx.dev_session_begin_fiber(0, 0, 1, 1),
+                 lambda: ctx.fiber_reconstruct(np.zeros((1, 4, 12, 12), np.float32), -1, 1)]:
+        with pytest.raises(xr.XRError) as e:
+            call()
+        assert e.value.status == 1
+    ctx.set_option(xr.Option.STORAGE, 1)
+    with pytest.raises(xr.XRError) as e:
+        ctx.dev_forward_fiber(8, 8)
+    assert e.value.status == 6
+    ctx.close()
+    for K in (1, 13):
+        bad = xr.Context.create(1000, 500, 2, 8, 12, 4, rot, basis=np.eye(3, dtype=np.float32)[np.arange(K) % 3])
+        for call in [lambda: bad.dev_forward_fiber(8, 8), lambda: bad.dev_session_begin_fiber(8, 8, 1, 1),
+                     lambda: bad.fiber_reconstruct(np.zeros((1, 4, 12, 12), np.float32), 1, 1)]:
+            with pytest.raises(xr.XRError) as e:
+                call()
+            assert e.value.status == 6
+        bad.close()

@@ -126,6 +126,11 @@ _SIGS = {
                            ctypes.c_int),
     "xr_fdk_reconstruct": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
                            ctypes.c_int),
+    "xr_fiber_reconstruct": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                              ctypes.c_int, ctypes.c_int, ctypes.c_float, _F], ctypes.c_int),
+    "xr_dev_forward_fiber": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "xr_dev_session_begin_fiber": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_float], ctypes.c_int),
     "xr_orientation": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "xr_angle_from_md": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "xr_direction_normalization": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
@@ -430,6 +435,18 @@ class Context:
             int(epoch), int(batch), int(rotate), int(method), float(lam), losses.ctypes.data_as(_F)))
         return vols, sino, md, ev, losses[:epoch]
 
+    def fiber_reconstruct(self, sino, epoch, batch, rotate=Rotate.CW, method=Method.MLEM, lam=1e-2):
+        """XTT::fiberModelReconstruct (reconstruct.cu:1242-1371): every channel
+        starts at 0.01.  Returns (volume (K, N, N, N), last ratio images
+        (C, V, Nd, Nd), losses (epoch,))."""
+        sino = _f32(sino).reshape(self.C, self.V, self.Nd, self.Nd).copy()
+        vols = np.zeros((self.K, self.N, self.N, self.N), np.float32)
+        losses = np.zeros(max(epoch, 1), np.float32)
+        self._check(lib().xr_fiber_reconstruct(self._h, _ptrs([sino[c] for c in range(self.C)]),
+                                               _ptrs([vols[k] for k in range(self.K)]), int(epoch), int(batch),
+                                               int(rotate), int(method), float(lam), losses.ctypes.data_as(_F)))
+        return vols, sino, losses[:epoch]
+
     def fdk_reconstruct(self, sino, rotate=Rotate.CW, filt=Filter.REFERENCE):
         """Returns (volumes (C, N, N, N), filtered sinograms (C, V, Nd, Nd))."""
         sino = _f32(sino).reshape(self.C, self.V, self.Nd, self.Nd).copy()
@@ -513,6 +530,17 @@ class Context:
         """updateEstimationByCoef (ir.cu:1073-1120)."""
         self._check(lib().xr_orth_update_estimation(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_est),
                                                     int(iteration)))
+
+    def dev_forward_fiber(self, d_vol: int, d_sino: int, rotate=Rotate.CW):
+        """forwardProjFiber (fiber.cu:13-153) over every axis and view, device buffers."""
+        self._check(lib().xr_dev_forward_fiber(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_sino),
+                                               int(rotate)))
+
+    def dev_session_begin_fiber(self, d_sino: int, d_vol: int, epochs: int, batch: int, rotate=Rotate.CW,
+                                method=Method.MLEM, lam=1e-2):
+        """fiberModelReconstruct's epochs as a session (channel 0 updated)."""
+        self._check(lib().xr_dev_session_begin_fiber(self._h, ctypes.c_void_p(d_sino), ctypes.c_void_p(d_vol),
+                                                     int(epochs), int(batch), int(rotate), int(method), float(lam)))
 
     def dev_forward_md(self, d_vol: int, d_md: int, d_sino: int, rotate=Rotate.CW):
         """forwardOrthByMD + chord normalisation over every axis and view (ir.cu:154-231)."""

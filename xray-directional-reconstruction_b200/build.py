@@ -23,7 +23,8 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["xr_kernels.cu", "xr_column.cu", "xr_orient.cu", "xr_fdk.cu", "xr_static.cu", "xr_learn.cu", "xr_solver.cu"]
+CU_SOURCES = ["xr_kernels.cu", "xr_column.cu", "xr_orient.cu", "xr_fdk.cu", "xr_static.cu", "xr_learn.cu", "xr_solver.cu",
+              "xr_fiber.cu"]
 CXX_SOURCES = ["xr_host.cpp"]
 
 

@@ -402,6 +402,15 @@ static xr_status check_xtt_k(xr_ctx *c) {
     return XR_OK;
 }
 
+/* The fiber model reads the fiber vector (mu_0, mu_1, mu_2) and, with K = 4,
+ * the isotropic term mu_3 (fiber.cu:19-24 index exactly four planes), all
+ * FP32. */
+static xr_status check_fiber(xr_ctx *c) {
+    if (c->K < 3 || c->K > 4) return fail(c, XR_ERR_CONFIG, "the fiber model needs K = 3 or 4 channels");
+    if (c->storage != 0) return fail(c, XR_ERR_CONFIG, "the fiber model needs FP32 volume storage");
+    return XR_OK;
+}
+
 static xr_status validate_scan(xr_ctx *c) {
     if (!(c->sdd > 0 && c->sod > 0 && c->det > 0)) return fail(c, XR_ERR_ARG, "sdd, sod and det_size must be > 0");
     if (c->N < 1 || c->N > 4096) return fail(c, XR_ERR_ARG, "num_voxel out of range [1, 4096]");
@@ -463,9 +472,12 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
             const int *vl = (const int *)c->subsets.p + (size_t)orders[b] * s.subset_size;
             {
                 Timed t(c, XR_T_FORWARD);
-                if ((st = cuda_check(c, forward_dispatch(c, vl, s.subset_size, all_conds(c), s.d_vol, proj, 1,
-                                                         s.storage, s.coef, s.coef_kind), "XTT forward")))
-                    return st;
+                const cudaError_t e =
+                    s.fiber ? launch_fiber_forward(c->gc, fr, vl, s.subset_size, c->C, (const float *)s.d_vol, proj,
+                                                   str)
+                            : forward_dispatch(c, vl, s.subset_size, all_conds(c), s.d_vol, proj, 1, s.storage, s.coef,
+                                               s.coef_kind);
+                if ((st = cuda_check(c, e, "XTT forward"))) return st;
             }
             {
                 Timed t(c, XR_T_RATIO);
@@ -477,7 +489,7 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                 /* the (phi, cos theta) forward is not chord-normalised (forwardOrth ->
                  * projRatio, reconstruct.cu:1086-1099); the main-direction one is
                  * (forwardOrthByMD -> correlationProjByLength, reconstruct.cu:1501-1509) */
-                const float *nrm = (s.coef && s.coef_kind == 0) ? nullptr : norm;
+                const float *nrm = ((s.coef && s.coef_kind == 0) || s.fiber) ? nullptr : norm;
                 if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, nrm,
                                                      s.d_sino, s.art, dl, s.sino_storage, str), "ratio")))
                     return st;
@@ -501,7 +513,10 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
             {
                 Timed t(c, XR_T_BACK);
                 cudaError_t e;
-                if (c->all_aligned) {
+                if (s.fiber) {
+                    e = launch_fiber_back(c->gc, fr, vl, s.subset_size, c->C, proj, (float *)s.d_vol, s.art, alpha,
+                                          str);
+                } else if (c->all_aligned) {
                     const ColInfo *ci = dcol(c);
                     const float *sens =
                         s.art ? nullptr : (const float *)c->sens.p + (size_t)orders[b] * c->K * N3;
@@ -856,7 +871,7 @@ xr_status xr_reset_timings(xr_ctx *c) {
 
 static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, int xtt, int epochs, int batch,
                                     xr_rotate dir, xr_method method, float lambda, const float *coef,
-                                    int coef_kind = 0) {
+                                    int coef_kind = 0, bool fiber = false) {
     if (!c || !d_sino || !d_vol) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
     if (batch < 1 || batch > c->V) return fail(c, XR_ERR_ARG, "batch must be in [1, num_proj]");
     if (method != XR_METHOD_MLEM && method != XR_METHOD_ART && method != XR_METHOD_XTT)
@@ -864,7 +879,11 @@ static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, 
     if (dir != XR_ROTATE_CW && dir != XR_ROTATE_CCW) return fail(c, XR_ERR_ARG, "bad rotate");
     if (epochs < 0) return fail(c, XR_ERR_ARG, "epochs must be >= 0");
     xr_status st;
-    if (xtt && (st = check_xtt_k(c))) return st;
+    if (fiber) {
+        if ((st = check_fiber(c))) return st;
+    } else if (xtt && (st = check_xtt_k(c))) {
+        return st;
+    }
     if ((st = ensure_device(c))) return st;
     const int rotation = dir == XR_ROTATE_CW ? 1 : -1;
     if ((st = ensure_frames(c, rotation))) return st;
@@ -885,6 +904,7 @@ static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, 
     s.update_storage = s.storage | ((c->stochastic && s.storage != 0) ? kStoreStochastic : 0);
     s.coef = coef;
     s.coef_kind = coef_kind;
+    s.fiber = fiber;
     std::vector<int> lists((size_t)batch * s.subset_size);
     for (int sub = 0; sub < batch; sub++)
         for (int j = 0; j < s.subset_size; j++)   /* n = (sub + batch*j) % nProj, reconstruct.cu:89 */
@@ -908,7 +928,7 @@ static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, 
             std::copy(o.begin(), o.end(), s.ir_orders.begin() + r * batch);
         }
     }
-    if (s.xtt && c->all_aligned && !s.art) {
+    if (s.xtt && !s.fiber && c->all_aligned && !s.art) {
         /* factor_k of every subset (geometry only): sum over the subset's views
          * of (|B x S_k| |S_k . G|)^2 (ir.cu:1847), once per session. */
         const size_t N3 = (size_t)c->N * c->N * c->N;
@@ -946,6 +966,11 @@ xr_status xr_dev_session_begin_md(xr_ctx *c, const void *d_sino, void *d_vol, co
                                   int batch, xr_rotate dir, xr_method method, float lambda) {
     if (!c || !d_md) return c ? fail(c, XR_ERR_ARG, "null main-direction planes") : XR_ERR_ARG;
     return session_begin_impl(c, d_sino, d_vol, 1, epochs, batch, dir, method, lambda, d_md, 1);
+}
+
+xr_status xr_dev_session_begin_fiber(xr_ctx *c, const void *d_sino, float *d_vol, int epochs, int batch,
+                                     xr_rotate dir, xr_method method, float lambda) {
+    return session_begin_impl(c, d_sino, d_vol, 1, epochs, batch, dir, method, lambda, nullptr, 0, true);
 }
 
 xr_status xr_dev_session_epoch(xr_ctx *c, double *loss) {
@@ -997,7 +1022,7 @@ static xr_status session_end_impl(xr_ctx *c, float *d_md, float *d_ev,
     Session &s = c->sess;
     if (!s.active) return fail(c, XR_ERR_STATE, "no active session");
     xr_status st = XR_OK;
-    if (s.xtt) {
+    if (s.xtt && !s.fiber) {
         const long nvox = (long)c->N * c->N * c->N;
         if (c->xtt_sqrt) {
             Timed t(c, XR_T_ORIENT);
@@ -1029,6 +1054,9 @@ xr_status xr_dev_session_proj(xr_ctx *c, const float **d_proj) {
 
 /* ---------------------------------------------------- device-buffer calls */
 
+/* forward_into mode of the fiber model's forwardProjFiber */
+constexpr int kFiberMode = -1;
+
 static xr_status forward_into(xr_ctx *c, const void *d_vol, float *d_out, int rotation, int mode, bool normalise,
                               int storage, const float *coef = nullptr, int coef_kind = 0) {
     xr_status st;
@@ -1042,9 +1070,13 @@ static xr_status forward_into(xr_ctx *c, const void *d_vol, float *d_out, int ro
     cudaMemsetAsync(d_out, 0, npx * sizeof(float), c->stream);
     {
         Timed t(c, XR_T_FORWARD);
-        st = cuda_check(c, forward_dispatch(c, (const int *)lst.p, c->V, all_conds(c), d_vol, d_out, mode, storage,
-                                            coef, coef_kind),
-                        "forward");
+        const cudaError_t e =
+            mode == kFiberMode
+                ? launch_fiber_forward(c->gc, (const ViewFrame *)c->frames.p, (const int *)lst.p, c->V, c->C,
+                                       (const float *)d_vol, d_out, c->stream)
+                : forward_dispatch(c, (const int *)lst.p, c->V, all_conds(c), d_vol, d_out, mode, storage, coef,
+                                   coef_kind);
+        st = cuda_check(c, e, "forward");
     }
     if (!st && normalise) {
         Timed t(c, XR_T_OTHER);
@@ -1061,6 +1093,15 @@ xr_status xr_dev_forward_orth(xr_ctx *c, const void *d_vol, const float *d_coef,
     if ((st = check_xtt_k(c))) return st;
     if ((st = ensure_device(c))) return st;
     return forward_into(c, d_vol, d_sino, dir == XR_ROTATE_CCW ? -1 : 1, 1, false, c->storage, d_coef);
+}
+
+xr_status xr_dev_forward_fiber(xr_ctx *c, const float *d_vol, float *d_sino, xr_rotate dir) {
+    if (!c || !d_vol || !d_sino) return c ? fail(c, XR_ERR_ARG, "null buffer") : XR_ERR_ARG;
+    if (dir != XR_ROTATE_CW && dir != XR_ROTATE_CCW) return fail(c, XR_ERR_ARG, "bad rotate");
+    xr_status st;
+    if ((st = check_fiber(c))) return st;
+    if ((st = ensure_device(c))) return st;
+    return forward_into(c, d_vol, d_sino, dir == XR_ROTATE_CCW ? -1 : 1, kFiberMode, false, 0);
 }
 
 xr_status xr_dev_forward_md(xr_ctx *c, const void *d_vol, const float *d_md, float *d_sino, xr_rotate dir) {
@@ -1435,6 +1476,38 @@ xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
     };
     if ((st = session_end_impl(c, d_md, d_ev, after))) return st;
     return cuda_check(c, cudaStreamSynchronize(cs), "downloads");
+}
+
+xr_status xr_fiber_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel, int epoch, int batch,
+                               xr_rotate dir, xr_method method, float lambda, float *losses) {
+    if (!c || !sino || !voxel) return c ? fail(c, XR_ERR_ARG, "null argument") : XR_ERR_ARG;
+    if (epoch < 0) return fail(c, XR_ERR_ARG, "epoch must be >= 0");
+    xr_status st;
+    if ((st = check_fiber(c))) return st;
+    for (int i = 0; i < c->K; i++)
+        if (!voxel[i]) return fail(c, XR_ERR_ARG, "null host pointer: volume");
+    if ((st = ensure_device(c))) return st;
+    const size_t N3 = (size_t)c->N * c->N * c->N, blk = (size_t)c->V * c->Nd * c->Nd;
+    if ((st = upload_planes_s(c, c->scratch_sino, sino, c->C, blk, sino_st(c), "sinogram"))) return st;
+    if ((st = ensure(c, c->scratch_vol, (size_t)c->K * N3 * sizeof(float), "volume"))) return st;
+    /* every channel starts at 0.01 whatever the caller passed (reconstruct.cu:1245-1247) */
+    if ((st = cuda_check(c, launch_fill((long)(c->K * N3), (float *)c->scratch_vol.p, 0.01f, c->stream), "fill")))
+        return st;
+    if ((st = xr_dev_session_begin_fiber(c, c->scratch_sino.p, (float *)c->scratch_vol.p, epoch, batch, dir, method,
+                                         lambda)))
+        return st;
+    for (int ep = 0; ep < epoch; ep++) {
+        double l = 0;
+        if ((st = xr_dev_session_epoch(c, losses ? &l : nullptr))) return st;
+        if (losses) losses[ep] = (float)l;
+    }
+    if ((st = xr_dev_session_end(c, nullptr, nullptr))) return st;
+    /* with no epoch the reference hands back its never-written devProj; here that is zeros */
+    if (epoch == 0 && (st = cuda_check(c, cudaMemsetAsync(c->proj.p, 0, (size_t)c->C * blk * sizeof(float), c->stream),
+                                       "clear ratio images")))
+        return st;
+    if ((st = download_planes_async(c, (const float *)c->proj.p, sino, c->C, blk, "ratio images", c->stream))) return st;
+    return download_planes(c, (const float *)c->scratch_vol.p, voxel, c->K, N3, "volume");
 }
 
 xr_status xr_orientation(xr_ctx *c, const float *const *mu, float *const *md, float *const *evalue) {

@@ -94,6 +94,7 @@ struct Session {
     int update_storage = 0;           /* volume, | kStoreStochastic  */
     const float *coef = nullptr;      /* orientation-parametrised XTT: rotation planes */
     int coef_kind = 0;                /* 0: (phi, cos theta); 1: main direction (3 planes) */
+    bool fiber = false;               /* fiber model: fiber projectors, channel 0 updated   */
     cudaEvent_t sino_ready = nullptr; /* set: the first ratio launch waits for it (sinogram upload) */
     float *const *ratio_dst = nullptr; /* set: each view's final ratio image to these host planes */
     std::vector<int> order;            /* persistent subset order (XTT)     */
@@ -236,6 +237,17 @@ cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, cons
                                float *ev, int storage, cudaStream_t s);
 cudaError_t launch_angle_from_md(long nvox, const float *md, float *angle, cudaStream_t s);
 cudaError_t launch_direction_normalization(long nvox, float *md, cudaStream_t s);
+
+/* ---- xr_fiber.cu: the fiber model (reconstruct/src/fiber.cu) ---- */
+/* forwardProjFiber of the listed views of n_cond axes into out (C blocks of
+ * V*Nd*Nd, accumulated): c * vs * ratio * |(B x G).(mu_0, mu_1, mu_2) + mu_3|
+ * per tap, rayCastingFiber's frame; vol holds min(K, 4) FP32 planes of N^3. */
+cudaError_t launch_fiber_forward(const GeomConst &g, const ViewFrame *frames, const int *view_list, int n_views,
+                                 int n_cond, const float *vol, float *out, cudaStream_t s);
+/* backwardProjFiber of the listed views of n_cond axes fused with the update
+ * of channel 0 (voxelProduct, or voxelPlus with step alpha when art). */
+cudaError_t launch_fiber_back(const GeomConst &g, const ViewFrame *frames, const int *view_list, int n_views,
+                              int n_cond, const float *proj, float *vol, int art, float alpha, cudaStream_t s);
 
 /* ---- xr_fdk.cu ---- */
 cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_cond, const float *sino,
