@@ -40,16 +40,19 @@ def main() -> None:
         out[f"k{K}_geom"] = np.array([s.sdd, s.sod, s.det, N, Nd, V], np.float64)
         out.update({f"k{K}_rot": s.rot, f"k{K}_trans": s.trans, f"k{K}_offset": s.offset, f"k{K}_basis": s.basis,
                     f"k{K}_vol": vol, f"k{K}_ratio": ratio})
+        # views n > 0 (Rotate::CW) and n < 0 (Rotate::CCW, image |n|)
         for cond in range(3):
-            n = 2 + 3 * cond
-            p = np.zeros(V * Nd * Nd, np.float32)
-            R.fiber_forward(cond, n, vol.ravel().copy(), p)
-            out[f"k{K}_fwd_c{cond}"] = p[n * Nd * Nd:(n + 1) * Nd * Nd].copy()
-            tmp = np.zeros(K * N * N, np.float32)
-            fac = np.zeros(K * N * N, np.float32)
-            R.fiber_backward(cond, 4, n, ratio.ravel().copy(), vol.ravel().copy(), tmp, fac)
-            out[f"k{K}_bwd_c{cond}_tmp"] = tmp
-            out[f"k{K}_bwd_c{cond}_fac"] = fac
+            for sign, tag in ((1, ""), (-1, "_ccw")):
+                n = sign * (2 + 3 * cond)
+                m = abs(n)
+                p = np.zeros(V * Nd * Nd, np.float32)
+                R.fiber_forward(cond, n, vol.ravel().copy(), p)
+                out[f"k{K}_fwd_c{cond}{tag}"] = p[m * Nd * Nd:(m + 1) * Nd * Nd].copy()
+                tmp = np.zeros(K * N * N, np.float32)
+                fac = np.zeros(K * N * N, np.float32)
+                R.fiber_backward(cond, 4, n, ratio.ravel().copy(), vol.ravel().copy(), tmp, fac)
+                out[f"k{K}_bwd_c{cond}{tag}_tmp"] = tmp
+                out[f"k{K}_bwd_c{cond}{tag}_fac"] = fac
     path = os.path.join(HERE, "ref_fiber_small.npz")
     np.savez_compressed(path, **out)
     print(path, len(out), "arrays")

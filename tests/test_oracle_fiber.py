@@ -26,16 +26,21 @@ def _scan(g, K) -> Scan:
 
 @pytest.mark.parametrize("K", [3, 4])
 @pytest.mark.parametrize("cond", [0, 1, 2])
-def test_fiber_projectors_bit_exact(oracle, g, K, cond):
+@pytest.mark.parametrize("sign", [1, -1])
+def test_fiber_projectors_bit_exact(oracle, g, K, cond, sign):
+    """Views n > 0 (Rotate::CW) and n < 0 (Rotate::CCW, written to image |n|)."""
     s = _scan(g, K)
     N, Nd, V = s.N, s.Nd, s.V
-    n = 2 + 3 * cond
+    n = sign * (2 + 3 * cond)
+    m = abs(n)
+    tag = "" if sign > 0 else "_ccw"
     vol = g[f"k{K}_vol"].ravel()
     p = np.zeros(V * Nd * Nd, np.float32)
     oracle.fiber_forward_view(s, cond, n, vol.copy(), p)
-    assert np.array_equal(p[n * Nd * Nd:(n + 1) * Nd * Nd], g[f"k{K}_fwd_c{cond}"])
+    assert np.array_equal(p[m * Nd * Nd:(m + 1) * Nd * Nd], g[f"k{K}_fwd_c{cond}{tag}"])
+    assert not p[:m * Nd * Nd].any() and not p[(m + 1) * Nd * Nd:].any()
     tmp = np.zeros(K * N * N, np.float32)
     fac = np.zeros(K * N * N, np.float32)
     oracle.fiber_backward_slab(s, cond, 4, n, g[f"k{K}_ratio"].ravel().copy(), vol.copy(), tmp, fac)
-    assert np.array_equal(tmp, g[f"k{K}_bwd_c{cond}_tmp"])
-    assert np.array_equal(fac, g[f"k{K}_bwd_c{cond}_fac"])
+    assert np.array_equal(tmp, g[f"k{K}_bwd_c{cond}{tag}_tmp"])
+    assert np.array_equal(fac, g[f"k{K}_bwd_c{cond}{tag}_fac"])
