@@ -25,6 +25,7 @@ import argparse
 import ctypes
 import importlib.util
 import json
+import math
 import os
 import re
 import statistics
@@ -299,6 +300,35 @@ def load_warmstart():
     return mod
 
 
+def orientation_of(scan, mu):
+    """Per-voxel main direction (calcEigenVector, pca.cu:12-55, libxr's FP64
+    kernel) of sqrt|mu|, the voxelSqrt that XTT::reconstruct applies before it
+    (reconstruct.cu:919-942): (3, N, N, N) FP32 on the device."""
+    import torch
+    xr = load_pkg()
+    root = mu.float().abs().sqrt().contiguous()
+    md = torch.empty((3,) + tuple(mu.shape[1:]), dtype=torch.float32, device=mu.device)
+    scan.ctx.set_option(xr.Option.STORAGE, 0)
+    scan.ctx.dev_orientation(root.data_ptr(), md.data_ptr(), 0)
+    torch.cuda.synchronize()
+    return md
+
+
+def angle_stats(md_a, md_b, mask):
+    """Angle between the main directions md_a and md_b (unsigned axes) over
+    the voxels of `mask`: mean / median / 90th percentile in degrees."""
+    import torch
+    a, b = md_a[:, mask].double(), md_b[:, mask].double()
+    na, nb = a.norm(dim=0), b.norm(dim=0)
+    ok = (na > 0) & (nb > 0)
+    c = ((a * b).sum(0).abs()[ok] / (na[ok] * nb[ok])).clamp(max=1.0)
+    ang = torch.rad2deg(torch.acos(c))
+    if ang.numel() == 0:
+        return {"voxels": 0}
+    return {"voxels": int(ang.numel()), "mean_deg": float(ang.mean()), "median_deg": float(ang.median()),
+            "p90_deg": float(ang.kthvalue(max(1, int(math.ceil(0.9 * ang.numel()))))[0])}
+
+
 def run_ttr(args, local):
     """Time to a relative data residual ||A mu - b|| / ||b|| <= --target (FP64
     norms) on the XTT 256^3 x 13 workload, arms on the same data b = A mu_true
@@ -319,6 +349,13 @@ def run_ttr(args, local):
     torch.cuda.synchronize()
     K, N = scan.K, scan.N
     arms = {}
+    # orientation of the true volume, over the fiber voxels (not timed)
+    fiber_mask = mu_true.sum(0) > 0
+    md_arm = {}
+    try:
+        md_true, ori_err = orientation_of(scan, mu_true), None
+    except Exception as ex:      # an analysis failure is reported, it does not cost the timings
+        md_true, ori_err = None, f"{type(ex).__name__}: {ex}"
 
     def run_arm(name, storage, learned):
         dt = {0: torch.float32, 1: torch.bfloat16}[storage]
@@ -338,10 +375,18 @@ def run_ttr(args, local):
                                  target=args.target, max_epochs=args.max_epochs, final_sqrt=False)
         reached = bool(trace) and trace[-1][2] <= args.target
         err = float(torch.linalg.vector_norm(vol.float() - mu_true) / torch.linalg.vector_norm(mu_true))
+        ori = {"error": ori_err}
+        if md_true is not None:
+            try:
+                md_arm[name] = orientation_of(scan, vol)
+                ori = angle_stats(md_arm[name], md_true, fiber_mask)
+            except Exception as ex:
+                ori = {"error": f"{type(ex).__name__}: {ex}"}
         arms[name] = {"storage": {0: "f32", 1: "bf16"}[storage], "sinogram": "f32", "learned": learned,
                       "reached": reached, "epochs": e0 + e, "seconds": (ms0 + ms) / 1e3 if reached else None,
                       "seconds_run": (ms0 + ms) / 1e3, "residual_final": trace[-1][2] if trace else r0,
                       "residual_after_warm_start": r0, "volume_rel_error_final": err,
+                      "orientation_error_vs_truth": ori,
                       "history": [{"epoch": e0 + ep, "ms": ms0 + t, "rel_l2": r} for ep, t, r in trace]}
         del vol
 
@@ -353,6 +398,16 @@ def run_ttr(args, local):
     p, l = arms.get("plain_f32", {}), arms.get("learned_bf16", {})
     line["speedup_learned_bf16_vs_plain_f32"] = (p["seconds"] / l["seconds"]) if p.get("seconds") and \
         l.get("seconds") else None
+    cross = None
+    if "learned_bf16" in md_arm and "plain_f32" in md_arm:
+        try:
+            cross = angle_stats(md_arm["learned_bf16"], md_arm["plain_f32"], fiber_mask)
+        except Exception as ex:
+            cross = {"error": f"{type(ex).__name__}: {ex}"}
+    line["orientation_learned_bf16_vs_plain_f32"] = cross
+    line["orientation_note"] = ("angle between per-voxel main directions (calcEigenVector of sqrt|mu|) over the "
+                                "fiber voxels of the phantom; the truth is the orientation of the true volume")
+    del md_arm, md_true
     scan.ctx.close()
     return line
 
@@ -678,10 +733,12 @@ def main():
         t = run_ttr(args, local)
         ttr = {"target_rel_residual": t["target"], "speedup_learned_bf16_vs_plain_f32":
                t["speedup_learned_bf16_vs_plain_f32"], "note": "device time to the target, residual checked every "
-               f"{t['check_every']} epochs outside the timed work; same data b = A mu_true (held-out phantom)"}
+               f"{t['check_every']} epochs outside the timed work; same data b = A mu_true (held-out phantom)",
+               "orientation_learned_bf16_vs_plain_f32": t["orientation_learned_bf16_vs_plain_f32"],
+               "orientation_note": t["orientation_note"]}
         for k, a in t["arms"].items():
             ttr[k] = {x: a.get(x) for x in ("seconds", "epochs", "reached", "residual_final", "storage",
-                                            "unavailable") if x in a}
+                                            "orientation_error_vs_truth", "unavailable") if x in a}
     conv = None
     if world == 1 and args.size == "full":
         conv = conv_roofline(local)

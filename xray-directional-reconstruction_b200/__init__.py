@@ -487,6 +487,12 @@ class Context:
         self._check(lib().xr_dev_forward(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_sino), int(rotate),
                                          int(bool(xtt))))
 
+    def dev_orientation(self, d_mu: int, d_md: int, d_ev: int = 0):
+        """calcEigenVector (pca.cu:12-55) of every voxel: d_mu K planes of the
+        storage type, d_md three FP32 planes, d_ev three FP32 planes or 0."""
+        self._check(lib().xr_dev_orientation(self._h, ctypes.c_void_p(d_mu), ctypes.c_void_p(d_md),
+                                             ctypes.c_void_p(d_ev or None)))
+
     def dev_residual(self, d_vol: int, d_sino: int, xtt: bool, rotate=Rotate.CW):
         r, l1 = ctypes.c_double(), ctypes.c_double()
         self._check(lib().xr_dev_residual(self._h, ctypes.c_void_p(d_vol), ctypes.c_void_p(d_sino), int(rotate),
