@@ -511,6 +511,59 @@ def run_c4(args, local):
         sp["ctx"].close()
 
 
+def run_fiber(args, local):
+    """Fiber model (fiber.cu, fiberModelReconstruct): forwardProjFiber over
+    every (axis, view) pair, and OS-EM epochs (5 subsets) of forward, ratio and
+    back-projection with the update of channel 0, on a 128^3 x 4 volume of
+    signed fiber vectors plus an isotropic term, 3 axes x 120 views, 192^2
+    detector.  Device time by CUDA events on the library's stream, after
+    --warmup untimed repetitions."""
+    import torch
+    xr = load_pkg()
+    N, Nd, V, K, C = 128, 192, 120, 4, 3
+    rng = np.random.default_rng(11)
+    vol_h = rng.uniform(-1.0, 1.0, (K, N, N, N)).astype(np.float32)
+    vol_h[3] = np.abs(vol_h[3]) * 0.5
+    ctx = xr.Context.create(W["sdd"], W["sod"], W["det"], N, Nd, V, three_axes(), None, None,
+                            np.eye(4, 3, dtype=np.float32), device=local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    vol = torch.from_numpy(vol_h).cuda()
+    sino = torch.empty((C, V, Nd, Nd), dtype=torch.float32, device="cuda")
+    ctx.dev_forward_fiber(vol.data_ptr(), sino.data_ptr())
+    out = torch.empty_like(sino)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.warmup):
+        ctx.dev_forward_fiber(vol.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.dev_forward_fiber(vol.data_ptr(), out.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / args.steps
+    rec = torch.full_like(vol, 0.01)
+    ctx.dev_session_begin_fiber(sino.data_ptr(), rec.data_ptr(), args.warmup + args.steps, 5)
+    for _ in range(args.warmup):
+        ctx.dev_session_epoch()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.dev_session_epoch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ep_ms = e0.elapsed_time(e1) / args.steps
+    ctx.dev_session_end(0, 0)
+    bv = bytes_view(K, N, Nd)
+    line = {"mode": "fiber_model", "workload": f"fiber model {N}^3 x K{K}, {C} axes x {V} views, {Nd}^2 detector, "
+            "OS-EM 5 subsets, FP32", "forward_ms": fwd_ms, "epoch_ms": ep_ms,
+            "forward_effective_gbs": C * V * bv / (fwd_ms * 1e-3) / 1e9,
+            "epoch_effective_gbs": 2 * C * V * bv / (ep_ms * 1e-3) / 1e9, "steps": args.steps, "warmup": args.warmup}
+    ctx.close()
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -529,6 +582,7 @@ def main():
     ap.add_argument("--arms", default="plain_f32,learned_bf16", help="--ttr arms (also plain_bf16, learned_f32)")
     ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-residual comparison of the default run")
     ap.add_argument("--c4", action="store_true", help="uneven batch of 8 specimens (BF16), batched vs sequential")
+    ap.add_argument("--fiber", action="store_true", help="fiber-model forward and epoch timing (128^3 x 4)")
     ap.add_argument("--conv", type=int, default=0, metavar="N",
                     help="only the warm-start network's tensor-core roofline on an N^3 x 13 volume")
     args = ap.parse_args()
@@ -554,10 +608,12 @@ def main():
             torch.cuda.set_stream(torch.cuda.Stream())
             print(json.dumps(conv_roofline(local, args.conv)), flush=True)
         return
-    if args.ttr or args.c4:
+    if args.ttr or args.c4 or args.fiber:
         if rank == 0:          # one GPU: these comparisons run on rank 0 only
             if args.ttr:
                 print(json.dumps(run_ttr(args, local)), flush=True)
+            elif args.fiber:
+                print(json.dumps(run_fiber(args, local)), flush=True)
             else:
                 run_c4(args, local)
         return
