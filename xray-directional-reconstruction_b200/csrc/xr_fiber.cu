@@ -9,18 +9,24 @@
  * rayCastingFiber's (fiber.cu:228-278): rayCasting's source and rotation, but
  * voxel centres at (2i - N + 1)/2 and the detector v axis along -R e_z.
  *
- * Voxel-parallel kernels over all listed (axis, view) pairs with global
- * float atomics for the forward; the model is a research variant of the
- * reference, kept for completeness, not one of the tuned hot paths.
+ * Forward: a CTA owns a 16 x 8 x 8 brick and a chunk of views; per view it
+ * splats its voxels' taps into a shared detector tile (two-word fixed point,
+ * xr_tile.cuh) over the brick's footprint and flushes the tile with one float
+ * atomic per pixel.  Back: voxel-parallel over all listed (axis, view) pairs,
+ * gathers from the L2-resident ratio images, fused with the update.
  */
 #include <cuda_runtime.h>
 
 #include "xr_internal.h"
+#include "xr_tile.cuh"
 
 namespace xr {
 namespace {
 
-constexpr int kFiberThreads = 256;
+constexpr int kFiberThreads = 256;                 /* back kernel                    */
+constexpr int kFwdThreads = 256;                   /* forward: 16 x 8 x 8 brick      */
+constexpr int kBX = 16, kBY = 8, kBZ = 8;
+constexpr int kTileCap = 48 * 48;                  /* pixels per shared tile         */
 
 __device__ __forceinline__ float fdot_rn(float a0, float a1, float a2, float b0, float b1, float b2) {
     return __fadd_rn(__fadd_rn(__fmul_rn(a0, b0), __fmul_rn(a1, b1)), __fmul_rn(a2, b2));
@@ -74,46 +80,165 @@ __device__ __forceinline__ bool fiber_taps(const GeomConst &g, float u, float v,
     return true;
 }
 
-struct FiberArgs {
+struct FiberBackArgs {
     GeomConst g;
     const ViewFrame *frames;   /* [C][V] */
     const int *view_list;
     int n_views, n_cond;
-    const float *proj;         /* back: ratio images, C blocks */
-    float *out;                /* forward: C blocks            */
-    float *vol;                /* K (3 or 4) planes of N^3     */
+    const float *proj;         /* ratio images, C blocks          */
+    float *vol;                /* channel 0 updated in place       */
     int art;
     float alpha;
 };
 
-__global__ void k_fiber_forward(FiberArgs a) {
+struct FiberFwdArgs {
+    GeomConst g;
+    const ViewFrame *frames;   /* [C][V] */
+    const int *view_list;
+    int n_views, vpc;
+    const float *vol;          /* min(K, 4) planes of N^3 */
+    float *out;                /* C blocks of V*Nd*Nd, accumulated */
+    int nbx, nby;              /* bricks along x, y */
+};
+
+/* forwardProjFiber of a chunk of views of axis blockIdx.y over one brick. */
+__global__ void __launch_bounds__(kFwdThreads, 3) k_fiber_forward(FiberFwdArgs a) {
+    extern __shared__ int smem[];
+    __shared__ float s_red[kFwdThreads / 32];
+    int4 *bbox = reinterpret_cast<int4 *>(smem + 4 * kTileCap);   /* vpc entries */
+    ViewFrame *fr = reinterpret_cast<ViewFrame *>(bbox + a.vpc);
+
     const GeomConst &g = a.g;
-    const long N = g.N, N3 = N * N * N;
+    const int N = g.N, Nd = g.Nd;
     const int K = g.K < 4 ? g.K : 4;
-    const size_t NdNd = (size_t)g.Nd * g.Nd;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < N3; i += (long)gridDim.x * blockDim.x) {
-        const int x = (int)(i % N), y = (int)((i / N) % N), z = (int)(i / (N * N));
-        float mu[4];
-        for (int k = 0; k < K; k++) mu[k] = a.vol[i + k * N3];
-        for (int c = 0; c < a.n_cond; c++) {
-            for (int j = 0; j < a.n_views; j++) {
-                const ViewFrame &f = a.frames[(size_t)c * g.V + a.view_list[j]];
-                float u, v, B[3], w[4];
+    const int cond = blockIdx.y;
+    const int j0 = blockIdx.z * a.vpc;
+    const int nv = min(a.vpc, a.n_views - j0);
+    if (nv <= 0) return;
+
+    const int brick = blockIdx.x;
+    const int x0 = (brick % a.nbx) * kBX, y0 = ((brick / a.nbx) % a.nby) * kBY, z0 = (brick / (a.nbx * a.nby)) * kBZ;
+    const int x1 = min(x0 + kBX, N) - 1, y1 = min(y0 + kBY, N) - 1, z1 = min(z0 + kBZ, N) - 1;
+
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 4 * kTileCap; i += kFwdThreads) smem[i] = 0;
+    for (int i = tid; i < nv * 5; i += kFwdThreads) {
+        const int jj = i / 5, q = i % 5;
+        reinterpret_cast<float4 *>(&fr[jj])[q] =
+            reinterpret_cast<const float4 *>(&a.frames[(size_t)cond * g.V + a.view_list[j0 + jj]])[q];
+    }
+    __syncthreads();
+
+    /* footprint of the brick per view: hull of its 8 corner voxels' (u, v),
+     * widened by one pixel and clamped to the detector */
+    for (int i = tid; i < nv; i += kFwdThreads) {
+        const ViewFrame &f = fr[i];
+        float umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
+        bool ok = true;
+        for (int c = 0; c < 8; c++) {
+            float u, v, B[3];
+            fiber_ray(f, g, (c & 1) ? x1 : x0, (c & 2) ? y1 : y0, (c & 4) ? z1 : z0, u, v, B);
+            if (!(fabsf(u) < 1e7f && fabsf(v) < 1e7f)) ok = false;
+            umin = fminf(umin, u); umax = fmaxf(umax, u);
+            vmin = fminf(vmin, v); vmax = fmaxf(vmax, v);
+        }
+        int iu0 = (int)floorf(umin - 0.5f) - 1, iu1 = (int)floorf(umax - 0.5f) + 2;
+        int iv0 = (int)floorf(vmin - 0.5f) - 1, iv1 = (int)floorf(vmax - 0.5f) + 2;
+        iu0 = max(iu0, 0); iv0 = max(iv0, 0);
+        iu1 = min(iu1, Nd - 1); iv1 = min(iv1, Nd - 1);
+        int W = iu1 - iu0 + 1, H = iv1 - iv0 + 1;
+        if (!ok) { W = 1 << 20; H = 1; }              /* every tap to global memory */
+        if (iu1 < iu0 || iv1 < iv0) { W = 0; H = 0; } /* off the detector           */
+        bbox[i] = make_int4(iu0, iv0, W, H);
+    }
+
+    /* this thread's 4 voxels: a warp is 4 (x) x 4 (z) x 2 (y), so its taps
+     * spread over several pixels in any view */
+    const int lane = tid & 31, w = tid >> 5;
+    const int x = x0 + (w & 3) * 4 + (lane & 3);
+    const int z = z0 + ((w >> 2) & 1) * 4 + ((lane >> 2) & 3);
+    const int yb = y0 + (lane >> 4);
+    const long N3 = (long)N * N * N;
+    float mu[4][4];
+    bool okv[4];
+    float bound = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int y = yb + 2 * q;
+        okv[q] = x <= x1 && z <= z1 && y <= y1;
+        float sa = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            mu[q][k] = (okv[q] && k < K) ? __ldg(a.vol + (size_t)x + (size_t)N * y + (size_t)N * N * z + k * N3) : 0.f;
+            sa += fabsf(mu[q][k]);
+        }
+        /* |ps| <= |B x G| |F| + |mu_3| <= sum |mu_k| (B, G unit vectors); weights c <= 1 */
+        if (okv[q]) bound = fmaxf(bound, sa * g.vs * g.ratio * 1.001f);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bound = fmaxf(bound, __shfl_xor_sync(0xffffffffu, bound, o));
+    if (lane == 0) s_red[w] = bound;
+    __syncthreads();
+    float S = 0.f;
+#pragma unroll
+    for (int i = 0; i < kFwdThreads / 32; i++) S = fmaxf(S, s_red[i]);
+    if (!(S > 0.f) || !(S < 3e38f)) return;   /* nothing to splat (or non-finite input) */
+    const int sh = fix_shift(S);
+    const float fscale = ldexpf(1.0f, sh);
+    const float finv = ldexpf(1.0f, -sh);
+
+    const size_t NdNd = (size_t)Nd * Nd;
+    float *outc = a.out + (size_t)cond * g.V * NdNd;
+    for (int jj = 0; jj < nv; jj++) {
+        const ViewFrame f = fr[jj];
+        const int4 bb = bbox[jj];
+        int *T = smem + (jj & 1) * 2 * kTileCap;   /* hi words, lo words after */
+        float *P = outc + (size_t)f.view * NdNd;
+        const bool use_tile = (bb.z > 0) && (bb.z * bb.w <= kTileCap);
+        if (bb.z > 0) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (!okv[q]) continue;
+                float u, v, B[3], c[4];
                 int iu, iv;
-                fiber_ray(f, g, x, y, z, u, v, B);
-                if (!fiber_taps(g, u, v, iu, iv, w)) continue;
+                fiber_ray(f, g, x, yb + 2 * q, z, u, v, B);
+                if (!fiber_taps(g, u, v, iu, iv, c)) continue;
                 const float bxg[3] = {__fsub_rn(__fmul_rn(B[1], f.ev[2]), __fmul_rn(B[2], f.ev[1])),
                                       __fsub_rn(__fmul_rn(B[2], f.ev[0]), __fmul_rn(B[0], f.ev[2])),
                                       __fsub_rn(__fmul_rn(B[0], f.ev[1]), __fmul_rn(B[1], f.ev[0]))};
                 float ps = 0.f;
-                for (int k = 0; k < K; k++) ps = __fadd_rn(ps, __fmul_rn(k >= 3 ? 1.0f : bxg[k], mu[k]));
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (k < K) ps = __fadd_rn(ps, __fmul_rn(k >= 3 ? 1.0f : bxg[k], mu[q][k]));
                 const float pr = fabsf(ps);
-                float *P = a.out + (size_t)c * g.V * NdNd + (size_t)f.view * NdNd + iu + (size_t)g.Nd * iv;
-                /* c * vs * ratio * |ps|, left to right (fiber.cu:68-71) */
-                atomicAdd(P + g.Nd, __fmul_rn(__fmul_rn(__fmul_rn(w[0], g.vs), g.ratio), pr));
-                atomicAdd(P + g.Nd + 1, __fmul_rn(__fmul_rn(__fmul_rn(w[1], g.vs), g.ratio), pr));
-                atomicAdd(P + 1, __fmul_rn(__fmul_rn(__fmul_rn(w[2], g.vs), g.ratio), pr));
-                atomicAdd(P, __fmul_rn(__fmul_rn(__fmul_rn(w[3], g.vs), g.ratio), pr));
+                /* c * vs * ratio * |ps|, left to right (fiber.cu:68-75) */
+                float wv[4];
+#pragma unroll
+                for (int t = 0; t < 4; t++) wv[t] = __fmul_rn(__fmul_rn(__fmul_rn(c[t], g.vs), g.ratio), pr);
+                const int lu = iu - bb.x, lv = iv - bb.y;
+                if (use_tile && lu >= 0 && lu + 1 < bb.z && lv >= 0 && lv + 1 < bb.w) {
+                    int *t0 = T + lu + bb.z * lv;
+                    fix_add(t0 + bb.z, kTileCap, wv[0] * fscale);
+                    fix_add(t0 + bb.z + 1, kTileCap, wv[1] * fscale);
+                    fix_add(t0 + 1, kTileCap, wv[2] * fscale);
+                    fix_add(t0, kTileCap, wv[3] * fscale);
+                } else {
+                    float *p0 = P + iu + (size_t)Nd * iv;
+                    atomicAdd(p0 + Nd, wv[0]);
+                    atomicAdd(p0 + Nd + 1, wv[1]);
+                    atomicAdd(p0 + 1, wv[2]);
+                    atomicAdd(p0, wv[3]);
+                }
+            }
+        }
+        __syncthreads();
+        if (use_tile) {   /* one warp per tile row; the tile is cleared behind */
+            for (int r = w; r < bb.w; r += kFwdThreads / 32) {
+                for (int cc = lane; cc < bb.z; cc += 32) {
+                    float t;
+                    if (fix_take(T + cc + bb.z * r, kTileCap, finv, t))
+                        atomicAdd(P + (bb.x + cc) + (size_t)Nd * (bb.y + r), t);
+                }
             }
         }
     }
@@ -122,7 +247,7 @@ __global__ void k_fiber_forward(FiberArgs a) {
 /* Back-projection of the listed views of every axis fused with the update of
  * channel 0 (MLEM voxelProduct / ART voxelPlus); fiberModelReconstruct
  * (reconstruct.cu:1322-1347) updates that channel alone. */
-__global__ void k_fiber_back(FiberArgs a) {
+__global__ void k_fiber_back(FiberBackArgs a) {
     const GeomConst &g = a.g;
     const long N = g.N, N3 = N * N * N;
     const size_t NdNd = (size_t)g.Nd * g.Nd;
@@ -164,22 +289,35 @@ int fiber_grid(long n) {
 cudaError_t launch_fiber_forward(const GeomConst &g, const ViewFrame *frames, const int *view_list, int n_views,
                                  int n_cond, const float *vol, float *out, cudaStream_t s) {
     if (n_views <= 0 || n_cond <= 0) return cudaSuccess;
-    FiberArgs a{};
+    FiberFwdArgs a{};
     a.g = g;
     a.frames = frames;
     a.view_list = view_list;
     a.n_views = n_views;
-    a.n_cond = n_cond;
-    a.vol = const_cast<float *>(vol);
+    a.vol = vol;
     a.out = out;
-    k_fiber_forward<<<fiber_grid((long)g.N * g.N * g.N), kFiberThreads, 0, s>>>(a);
+    a.nbx = (g.N + kBX - 1) / kBX;
+    a.nby = (g.N + kBY - 1) / kBY;
+    const int nbz = (g.N + kBZ - 1) / kBZ;
+    const long bricks = (long)a.nbx * a.nby * nbz;
+    /* views per CTA: the whole list unless that leaves fewer than 2048 CTAs */
+    const long ctas = bricks * n_cond;
+    const long chunks = ctas >= 2048 ? 1 : (2048 + ctas - 1) / ctas;
+    int vpc = (int)((n_views + chunks - 1) / chunks);
+    vpc = vpc < 1 ? 1 : (vpc > 64 ? 64 : vpc);
+    a.vpc = vpc;
+    const dim3 grid((unsigned)bricks, (unsigned)n_cond, (unsigned)((n_views + vpc - 1) / vpc));
+    const size_t smem = 4 * kTileCap * sizeof(int) + (size_t)vpc * (sizeof(int4) + sizeof(ViewFrame));
+    cudaError_t e = cudaFuncSetAttribute(k_fiber_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_fiber_forward<<<grid, kFwdThreads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fiber_back(const GeomConst &g, const ViewFrame *frames, const int *view_list, int n_views,
                               int n_cond, const float *proj, float *vol, int art, float alpha, cudaStream_t s) {
     if (n_views <= 0 || n_cond <= 0) return cudaSuccess;
-    FiberArgs a{};
+    FiberBackArgs a{};
     a.g = g;
     a.frames = frames;
     a.view_list = view_list;
