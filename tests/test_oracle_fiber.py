@@ -44,3 +44,28 @@ def test_fiber_projectors_bit_exact(oracle, g, K, cond, sign):
     oracle.fiber_backward_slab(s, cond, 4, n, g[f"k{K}_ratio"].ravel().copy(), vol.copy(), tmp, fac)
     assert np.array_equal(tmp, g[f"k{K}_bwd_c{cond}{tag}_tmp"])
     assert np.array_equal(fac, g[f"k{K}_bwd_c{cond}{tag}_fac"])
+
+
+@pytest.mark.parametrize("K", [3, 4])
+def test_fiber_forward_fp64_and_symmetries(oracle, g, K):
+    """The FP32 restatement against the FP64 one (relative 1e-5 of the largest
+    pixel), and two exact properties of forwardProjFiber's |ps| weight: the
+    projection of -mu equals that of mu bit for bit, and scaling mu by a power
+    of two scales the projection by it exactly."""
+    s = _scan(g, K)
+    Nd, V = s.Nd, s.V
+    vol = g[f"k{K}_vol"].ravel()
+    for cond in range(3):
+        n = 1 + 2 * cond
+        p32 = np.zeros(V * Nd * Nd, np.float32)
+        oracle.fiber_forward_view(s, cond, n, vol.copy(), p32)
+        p64 = np.zeros(V * Nd * Nd, np.float64)
+        oracle.fiber_forward_view(s, cond, n, vol.astype(np.float64), p64, dt=np.float64)
+        assert np.abs(p64).max() > 0
+        assert np.abs(p32 - p64).max() <= 1e-5 * np.abs(p64).max()
+        neg = np.zeros_like(p32)
+        oracle.fiber_forward_view(s, cond, n, (-vol).copy(), neg)
+        assert np.array_equal(neg, p32)
+        dbl = np.zeros_like(p32)
+        oracle.fiber_forward_view(s, cond, n, (4.0 * vol).astype(np.float32), dbl)
+        assert np.array_equal(dbl, 4.0 * p32)
