@@ -29,6 +29,16 @@ def test_compat_header_compiles_and_links(tmp_path):
     assert os.path.exists(exe)
 
 
+def test_compat_signatures_match_the_reference():
+    """tests/compat/signatures.cpp static_asserts the type of every compat
+    entry point against the reference's declaration (reconstruct.cuh,
+    pca.cuh, tvmin.h, quadfilt.h, params.h); it must compile."""
+    src = os.path.join(ROOT, "tests", "compat", "signatures.cpp")
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), src],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 @pytest.mark.gpu
 def test_compat_driver_runs(tmp_path, oracle):
     from oracle import Scan
