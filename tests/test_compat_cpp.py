@@ -29,6 +29,21 @@ def test_compat_header_compiles_and_links(tmp_path):
     assert os.path.exists(exe)
 
 
+def test_c99_caller_builds_and_runs(tmp_path):
+    """The C ABI from plain C: tests/compat/c_caller.c compiles as pedantic
+    C99 with warnings as errors, links against libxr.so and passes its
+    device-free checks (context round trip, argument, state and
+    configuration errors)."""
+    load_xr().lib()
+    exe = str(tmp_path / "c_caller")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "compat", "c_caller.c"), "-o", exe, "-L", PKG_DIR, "-l:libxr.so",
+                    f"-Wl,-rpath,{PKG_DIR}"], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0, f"check {r.returncode} failed"
+    assert "sm_100a" in r.stdout
+
+
 def test_compat_signatures_match_the_reference():
     """tests/compat/signatures.cpp static_asserts the type of every compat
     entry point against the reference's declaration (reconstruct.cuh,
