@@ -13,7 +13,8 @@
  * splats its voxels' taps into a shared detector tile (two-word fixed point,
  * xr_tile.cuh) over the brick's footprint and flushes the tile with one float
  * atomic per pixel.  Back: voxel-parallel over all listed (axis, view) pairs,
- * gathers from the L2-resident ratio images, fused with the update.
+ * gathers from the L2-resident ratio images, fused with the update; since the
+ * reference's driver updates channel 0 alone, only channel 0's sums are formed.
  */
 #include <cuda_runtime.h>
 
