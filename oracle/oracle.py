@@ -168,6 +168,49 @@ class Oracle:
         self._fn("fiber_backward_slab", dt)(ctypes.byref(self._scan(s)), cond, y, n, _p(proj, dt), _p(vol, dt),
                                             _p(tmp, dt), _p(factor, dt))
 
+    def fiber_reconstruct(self, s, sino, vol, epoch, batch, rotate_ccw=0, art=False, lam=1e-2):
+        """XTT::fiberModelReconstruct (reconstruct.cu:1242-1371) from the volume
+        given (the reference starts every channel at 0.01, :1245-1247), FP32,
+        with the oracle's kernels: per subset forwardProjFiber + projRatio /
+        projSubtract over every axis (:1302-1326), then per slab
+        backwardProjFiber over every axis and view and voxelProduct / voxelPlus
+        (ir.cu:1637-1693) of channel 0 alone (:1328-1347).  Subset order: a
+        default std::mt19937_64 shuffles the persistent order every epoch
+        (:1296-1298).  sino: (C, V, Nd, Nd); vol: (K, N, N, N).  Returns
+        (volume, last ratio images (C, V, Nd, Nd), per-epoch sums of |b - p|)."""
+        N, Nd, V, K, C = s.N, s.Nd, s.V, s.K, s.C
+        rot = -1 if rotate_ccw else 1
+        sub_size = (V + batch - 1) // batch
+        alpha = np.float32(lam) / np.float32(sub_size)
+        vol = np.ascontiguousarray(vol, np.float32).reshape(K, -1).copy()
+        sino = np.ascontiguousarray(sino, np.float32).reshape(C, -1)
+        orders = self.subset_orders(batch, epoch, True)
+        proj = np.zeros((C, V * Nd * Nd), np.float32)
+        losses = np.zeros(epoch, np.float64)
+        v0 = vol[0].reshape(N, N, N)                       # [z][y][x], a view of vol
+        for e in range(epoch):
+            proj[:] = 0
+            for sub in orders[e]:
+                views = [rot * ((int(sub) + batch * j) % V) for j in range(sub_size)]
+                for c in range(C):
+                    for n in views:
+                        self.fiber_forward_view(s, c, n, vol.ravel(), proj[c])
+                        losses[e] += self.ratio(s, n, proj[c], sino[c], art)
+                for y in range(N):
+                    tmp = np.zeros(K * N * N, np.float32)
+                    fac = np.zeros(K * N * N, np.float32)
+                    for c in range(C):
+                        for n in views:
+                            self.fiber_backward_slab(s, c, y, n, proj[c], vol.ravel(), tmp, fac)
+                    t0, f0 = tmp[:N * N].reshape(N, N), fac[:N * N].reshape(N, N)   # [z][x]
+                    if art:
+                        v0[:, y, :] = v0[:, y, :] + alpha * t0
+                    else:
+                        with np.errstate(divide="ignore", invalid="ignore"):
+                            upd = (v0[:, y, :] * t0) / f0
+                        v0[:, y, :] = np.where(f0 == 0, np.float32(0), upd)
+        return vol.reshape(K, N, N, N), proj.reshape(C, V, Nd, Nd), losses
+
     def correlation(self, s, cond, n, proj, factor, dt=np.float32):
         self._fn("correlation", dt)(ctypes.byref(self._scan(s)), cond, n, _p(proj, dt), _p(factor, dt))
 
@@ -361,5 +404,17 @@ class RefHost:
         losses = np.zeros(epoch, np.float32)
         self.lib.xr_ref_xtt_reconstruct(_ptr_array(sino, np.float32), _ptr_array(vols, np.float32), epoch, batch,
                                         int(rotate_ccw), int(art), ctypes.c_float(lam), _p(losses))
+        return (np.stack(vols).reshape(s.K, s.N, s.N, s.N), np.stack(sino).reshape(s.C, s.V, s.Nd, s.Nd),
+                losses)
+
+    def fiber_reconstruct(self, sino, vol, epoch, batch, rotate_ccw=0, art=False, lam=1e-2):
+        """fiberModelReconstruct's epochs from the volume given; returns
+        (volume (K, N, N, N), last ratio images (C, V, Nd, Nd), float losses)."""
+        s = self.s
+        sino = [np.ascontiguousarray(x, np.float32).ravel().copy() for x in sino]
+        vols = [np.ascontiguousarray(x, np.float32).ravel().copy() for x in vol]
+        losses = np.zeros(epoch, np.float32)
+        self.lib.xr_ref_fiber_reconstruct(_ptr_array(sino, np.float32), _ptr_array(vols, np.float32), epoch, batch,
+                                          int(rotate_ccw), int(art), ctypes.c_float(lam), _p(losses))
         return (np.stack(vols).reshape(s.K, s.N, s.N, s.N), np.stack(sino).reshape(s.C, s.V, s.Nd, s.Nd),
                 losses)

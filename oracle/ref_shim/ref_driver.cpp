@@ -9,6 +9,10 @@
  *   ref_xtt_reconstruct  <- XTT::reconstruct  reconstruct/src/reconstruct.cu:799-927
  *                           (the Eigen orientation step :929-942 is not built:
  *                            Eigen is absent; the oracle's Jacobi replaces it)
+ *   ref_fiber_reconstruct <- XTT::fiberModelReconstruct  reconstruct.cu:1242-1371
+ *                           (its ratio launches pass a null loss pointer, :1318-1322,
+ *                            which projRatio's atomicAdd dereferences, ir.cu:1623:
+ *                            the restatement passes a local float instead)
  *   ref_forward_view     <- the forward half of one view of those loops
  *                           (reconstruct.cu:86-98 / :866-878)
  * A "launch" runs every (block, thread) of the grid as a plain call, serially in
@@ -381,6 +385,70 @@ void xr_ref_xtt_reconstruct(float **sino, float **vol, int epoch, int batch, int
     }
     for (int y = 0; y < N; y++)
         launch2d(g.gridV, g.blockV, voxelSqrt, devVoxel.data(), (const Geometry *)geom, y);
+    for (int i = 0; i < C; i++) std::memcpy(sino[i], &devProj[i * lenD], sizeof(float) * lenD);
+    for (int i = 0; i < K; i++) std::memcpy(vol[i], &devVoxel[i * lenV], sizeof(float) * lenV);
+}
+
+/* XTT::fiberModelReconstruct (reconstruct.cu:1242-1371): the caller's
+ * volume is the start (the reference sets every channel to 0.01 first,
+ * :1245-1247); per subset forwardProjFiber + projRatio / projSubtract over
+ * every axis, then per slab backwardProjFiber over every axis and view and
+ * voxelProduct / voxelPlus of channel 0 (the first N^3 of devVoxel,
+ * :1341-1345).  sino[C] receives devProj (:1355-1356). */
+void xr_ref_fiber_reconstruct(float **sino, float **vol, int epoch, int batch, int rotate_ccw, int art,
+                              float lambda, float *losses) {
+    Geometry *geom = &g.geom;
+    const int rotation = rotate_ccw ? -1 : 1;
+    const long N = geom->voxel, Nd = geom->detect;
+    const int nProj = geom->nProj;
+    const long lenV = N * N * N, lenD = Nd * Nd * (long)nProj, lenP = N * N;
+    const int C = g.C, K = g.K;
+    std::vector<float> devSino(lenD * C), devProj(lenD * C), devVoxel(lenV * K), devVoxelFactor(lenP * K),
+        devVoxelTmp(lenP * K);
+    for (int i = 0; i < C; i++) std::memcpy(&devSino[i * lenD], sino[i], sizeof(float) * lenD);
+    for (int i = 0; i < K; i++) std::memcpy(&devVoxel[i * lenV], vol[i], sizeof(float) * lenV);
+    const int subsetSize = (nProj + batch - 1) / batch;
+    std::vector<int> subsetOrder(batch);
+    for (int i = 0; i < batch; i++) subsetOrder[i] = i;
+    for (int ep = 0; ep < epoch; ep++) {
+        std::mt19937_64 get_rand_mt;
+        std::shuffle(subsetOrder.begin(), subsetOrder.end(), get_rand_mt);
+        float loss1 = 0.0f;
+        std::fill(devProj.begin(), devProj.end(), 0.0f);
+        for (int &sub : subsetOrder) {
+            for (int cond = 0; cond < C; cond++) {
+                for (int subOrder = 0; subOrder < subsetSize; subOrder++) {
+                    int n = rotation * ((sub + batch * subOrder) % nProj);
+                    for (int y = 0; y < N; y++)
+                        launch2d(g.gridV, g.blockV, forwardProjFiber, &devProj[lenD * cond], devVoxel.data(), geom,
+                                 cond, y, n);
+                    if (art)
+                        launch2d(g.gridD, g.blockD, projSubtract, &devProj[lenD * cond],
+                                 (const float *)&devSino[lenD * cond], (const Geometry *)geom, n, &loss1);
+                    else
+                        launch2d(g.gridD, g.blockD, projRatio, &devProj[lenD * cond],
+                                 (const float *)&devSino[lenD * cond], (const Geometry *)geom, n, &loss1);
+                }
+            }
+            for (int y = 0; y < N; y++) {
+                std::fill(devVoxelFactor.begin(), devVoxelFactor.end(), 0.0f);
+                std::fill(devVoxelTmp.begin(), devVoxelTmp.end(), 0.0f);
+                for (int cond = 0; cond < C; cond++)
+                    for (int subOrder = 0; subOrder < subsetSize; subOrder++) {
+                        int n = rotation * ((sub + batch * subOrder) % nProj);
+                        launch2d(g.gridV, g.blockV, backwardProjFiber, &devProj[lenD * cond], devVoxel.data(),
+                                 devVoxelTmp.data(), devVoxelFactor.data(), geom, cond, y, n);
+                    }
+                if (art)
+                    launch2d(g.gridV, g.blockV, voxelPlus, devVoxel.data(), (const float *)devVoxelTmp.data(),
+                             lambda / (float)subsetSize, (const Geometry *)geom, y);
+                else
+                    launch2d(g.gridV, g.blockV, voxelProduct, devVoxel.data(), (const float *)devVoxelTmp.data(),
+                             (const float *)devVoxelFactor.data(), (const Geometry *)geom, y);
+            }
+        }
+        if (losses) losses[ep] = loss1;
+    }
     for (int i = 0; i < C; i++) std::memcpy(sino[i], &devProj[i * lenD], sizeof(float) * lenD);
     for (int i = 0; i < K; i++) std::memcpy(vol[i], &devVoxel[i * lenV], sizeof(float) * lenV);
 }

@@ -1,6 +1,9 @@
 """Golden vectors of the reference's fiber-model projectors (forwardProjFiber,
 backwardProjFiber; reconstruct/src/fiber.cu) from its host build
-(oracle/_ref/libxrref.so, serial launch order), for K = 3 and K = 4.
+(oracle/_ref/libxrref.so, serial launch order), for K = 3 and K = 4, and of
+whole fiberModelReconstruct runs (reconstruct.cu:1242-1371, restated in
+oracle/ref_shim/ref_driver.cpp over the reference's kernels): MLEM and ART,
+CW and CCW, two epochs of three subsets.
 
     python tests/golden/make_golden_fiber.py
 """
@@ -53,6 +56,21 @@ def main() -> None:
                 R.fiber_backward(cond, 4, n, ratio.ravel().copy(), vol.ravel().copy(), tmp, fac)
                 out[f"k{K}_bwd_c{cond}{tag}_tmp"] = tmp
                 out[f"k{K}_bwd_c{cond}{tag}_fac"] = fac
+    # whole sessions: (K, art, ccw)
+    rng = np.random.default_rng(120)
+    for i, (K, art, ccw) in enumerate([(3, False, 0), (4, True, 1), (4, False, 1), (3, True, 0)]):
+        R = RefHost(parallel=False)
+        s = Scan(sdd=1000.0, sod=500.0, det=2.0, N=8, Nd=14, V=6, rot=three_axes(),
+                 trans=rng.normal(0, 0.3, (3, 3)), offset=rng.normal(0, 0.2, (3, 3)),
+                 basis=np.eye(4, 3, dtype=np.float32)[:K])
+        R.setup(s)
+        sino = rng.uniform(0.5, 1.5, (3, s.V, s.Nd, s.Nd)).astype(np.float32)
+        v0 = np.full((K, s.N, s.N, s.N), 0.01, np.float32)
+        vol, ratio, losses = R.fiber_reconstruct(sino, v0, 2, 3, ccw, art, 1e-2)
+        out.update({f"s{i}_case": np.array([K, int(art), ccw], np.int32), f"s{i}_geom":
+                    np.array([s.sdd, s.sod, s.det, s.N, s.Nd, s.V], np.float64), f"s{i}_rot": s.rot,
+                    f"s{i}_trans": s.trans, f"s{i}_offset": s.offset, f"s{i}_basis": s.basis, f"s{i}_sino": sino,
+                    f"s{i}_vol": vol, f"s{i}_ratio": ratio, f"s{i}_losses": losses})
     path = os.path.join(HERE, "ref_fiber_small.npz")
     np.savez_compressed(path, **out)
     print(path, len(out), "arrays")

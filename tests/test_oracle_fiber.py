@@ -69,3 +69,21 @@ def test_fiber_forward_fp64_and_symmetries(oracle, g, K):
         dbl = np.zeros_like(p32)
         oracle.fiber_forward_view(s, cond, n, (4.0 * vol).astype(np.float32), dbl)
         assert np.array_equal(dbl, 4.0 * p32)
+
+
+@pytest.mark.parametrize("i", [0, 1, 2, 3])
+def test_fiber_session_bit_exact(oracle, g, i):
+    """Whole fiberModelReconstruct runs (two epochs, three subsets; MLEM / ART,
+    CW / CCW, K = 3 / 4) from 0.01: the oracle's driver gives the reference's
+    volume (channel 0 updated, the others untouched) and last ratio images bit
+    for bit; the loss sums agree to float accumulation order."""
+    K, art, ccw = (int(v) for v in g[f"s{i}_case"])
+    sdd, sod, det, N, Nd, V = g[f"s{i}_geom"]
+    s = Scan(sdd=float(sdd), sod=float(sod), det=float(det), N=int(N), Nd=int(Nd), V=int(V), rot=g[f"s{i}_rot"],
+             trans=g[f"s{i}_trans"], offset=g[f"s{i}_offset"], basis=g[f"s{i}_basis"])
+    v0 = np.full((K, s.N, s.N, s.N), 0.01, np.float32)
+    vol, ratio, losses = oracle.fiber_reconstruct(s, g[f"s{i}_sino"], v0, 2, 3, ccw, bool(art), 1e-2)
+    assert np.array_equal(vol, g[f"s{i}_vol"])
+    assert np.array_equal(ratio, g[f"s{i}_ratio"])
+    assert np.array_equal(vol[1:], v0[1:]) and not np.array_equal(vol[0], v0[0])
+    assert np.allclose(losses, g[f"s{i}_losses"], rtol=1e-5)
