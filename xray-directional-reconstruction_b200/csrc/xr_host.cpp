@@ -477,7 +477,7 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                                                    str)
                             : forward_dispatch(c, vl, s.subset_size, all_conds(c), s.d_vol, proj, 1, s.storage, s.coef,
                                                s.coef_kind);
-                if ((st = cuda_check(c, e, "XTT forward"))) return st;
+                if ((st = cuda_check(c, e, s.fiber ? "fiber forward" : "XTT forward"))) return st;
             }
             {
                 Timed t(c, XR_T_RATIO);
@@ -527,7 +527,7 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                     e = launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, 0, c->C, proj, s.d_vol, 1, s.art,
                                            alpha, s.update_storage, str, s.coef, s.coef_kind);
                 }
-                if ((st = cuda_check(c, e, "XTT back"))) return st;
+                if ((st = cuda_check(c, e, s.fiber ? "fiber back" : "XTT back"))) return st;
             }
         }
     } else {
