@@ -297,7 +297,7 @@ xr_status xr_md_update_estimation(xr_ctx *ctx, const float *d_vol, float *d_est,
  *      reconstruct.cuh:54-55, reconstruct.cu:1242-1371) ------------------ */
 /* Every voxel holds a fiber vector F = (mu_0, mu_1, mu_2) and, with K = 4, an
  * isotropic term mu_3; a ray of unit direction B through the grating of
- * direction G sees ps = (B x G) . F + mu_3 (fiber.cu:53-58).  The ray casting
+ * direction G sees ps = (B x G) . F + mu_3 (fiber.cu:52-65).  The ray casting
  * is rayCastingFiber's (fiber.cu:228-278): voxel centres at (2i - N + 1)/2
  * and the detector v axis along -G.  These calls need K = 3 or 4 (the
  * reference indexes exactly four planes, fiber.cu:19-24) and FP32 volumes.

@@ -723,7 +723,7 @@ static void RV(raycast_fiber)(const or_scan *s, const RV(frame) * f, int x, int 
 }
 
 /* The fiber model's signed projection of voxel idx: ps = (B x G).(f0, f1, f2)
- * + f3 (fiber.cu:53-58, channels beyond the fourth are not read); the weight
+ * + f3 (fiber.cu:52-65, channels beyond the fourth are not read); the weight
  * used is |ps|, its sign s. */
 static real RV(fiber_signed)(const or_scan *s, const real *B, const real *G, const real *vol, long idx, long N3,
                              real *bxg) {

@@ -2,7 +2,7 @@
  * The fiber-model projectors (reconstruct/src/fiber.cu).  Every voxel holds a
  * fiber vector F = (mu_0, mu_1, mu_2) and, with K = 4, an isotropic term
  * mu_3; a ray with unit direction B through a grating along G sees the signed
- * projection ps = (B x G) . F + mu_3 (fiber.cu:53-58).  Forward:
+ * projection ps = (B x G) . F + mu_3 (fiber.cu:52-65).  Forward:
  * proj += c * vs * ratio * |ps| per tap (no weight image, no chord
  * normalisation).  Back: channel i gathers w_i = |(B x G)_i| (i < 3) or 1
  * times the 4-tap sum of the ratio image, and its own w_i.  The ray casting is
