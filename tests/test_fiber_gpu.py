@@ -5,7 +5,8 @@ reference's host build (tests/test_oracle_fiber.py), driven the way
 fiberModelReconstruct (reconstruct.cu:1242-1371) drives them.
 
 Tolerance 1e-5 of the largest value, as for the other projectors: the forward
-splat adds its taps with float atomics in another order."""
+splat sums its taps in another order (per-brick fixed-point tiles, then float
+atomics per pixel)."""
 from __future__ import annotations
 
 import numpy as np
