@@ -3,7 +3,7 @@ backwardProjFiber; reconstruct/src/fiber.cu) from its host build
 (oracle/_ref/libxrref.so, serial launch order), for K = 3 and K = 4, and of
 whole fiberModelReconstruct runs (reconstruct.cu:1242-1371, restated in
 oracle/ref_shim/ref_driver.cpp over the reference's kernels): MLEM and ART,
-CW and CCW, two epochs of three subsets.
+CW and CCW, two epochs of three subsets (one case with V % batch != 0).
 
     python tests/golden/make_golden_fiber.py
 """
@@ -58,9 +58,11 @@ def main() -> None:
                 out[f"k{K}_bwd_c{cond}{tag}_fac"] = fac
     # whole sessions: (K, art, ccw)
     rng = np.random.default_rng(120)
-    for i, (K, art, ccw) in enumerate([(3, False, 0), (4, True, 1), (4, False, 1), (3, True, 0)]):
+    # case 4: V % batch != 0, so the last subsets revisit views 0 and 1 (reconstruct.cu:1306)
+    for i, (K, art, ccw, V) in enumerate([(3, False, 0, 6), (4, True, 1, 6), (4, False, 1, 6), (3, True, 0, 6),
+                                          (4, False, 0, 7)]):
         R = RefHost(parallel=False)
-        s = Scan(sdd=1000.0, sod=500.0, det=2.0, N=8, Nd=14, V=6, rot=three_axes(),
+        s = Scan(sdd=1000.0, sod=500.0, det=2.0, N=8, Nd=14, V=V, rot=three_axes(),
                  trans=rng.normal(0, 0.3, (3, 3)), offset=rng.normal(0, 0.2, (3, 3)),
                  basis=np.eye(4, 3, dtype=np.float32)[:K])
         R.setup(s)

@@ -71,10 +71,12 @@ def test_fiber_forward_fp64_and_symmetries(oracle, g, K):
         assert np.array_equal(dbl, 4.0 * p32)
 
 
-@pytest.mark.parametrize("i", [0, 1, 2, 3])
+@pytest.mark.parametrize("i", [0, 1, 2, 3, 4])
 def test_fiber_session_bit_exact(oracle, g, i):
     """Whole fiberModelReconstruct runs (two epochs, three subsets; MLEM / ART,
-    CW / CCW, K = 3 / 4) from 0.01: the oracle's driver gives the reference's
+    CW / CCW, K = 3 / 4; case 4 with 7 views, so subsets revisit views and
+    their forwards add onto the earlier ratio images) from 0.01: the oracle's
+    driver gives the reference's
     volume (channel 0 updated, the others untouched) and last ratio images bit
     for bit; the loss sums agree to float accumulation order."""
     K, art, ccw = (int(v) for v in g[f"s{i}_case"])
