@@ -375,16 +375,22 @@ xr_status xr_batch_autotune(xr_batch *batch, int *chosen);
  * callers that cannot allocate device memory: code whose device memory is
  * all owned by another allocator (a framework's caching pool) or whose
  * steady-state loop must not allocate.  No counterpart in the reference.
- * Allocates nothing: its only scratch (the per-view geometry table and the
- * view list) is a fixed array inside libxr of num_cond * num_proj <= 4096
- * (axis, view) pairs, held by every GPU that loads the library until exit;
- * larger scans get XR_ERR_ARG.  d_vol: N^3 floats (channel 0); d_sino:
- * C*V*Nd^2 floats, cleared then accumulated.  Work is enqueued on `stream`
- * (a cudaStream_t, NULL = legacy default) without synchronizing.  All calls
- * share the scratch and it keeps the last call's contents, so calls that
- * overlap on the GPU race; serialise them.  The first call on a device
- * resolves the scratch address (cudaGetSymbolAddress): make it before any
- * stream capture. */
+ * Allocates nothing: its only scratch (the per-view geometry table, the
+ * view list and a flag word) is a fixed array inside libxr of
+ * num_cond * num_proj <= 4096 (axis, view) pairs, held by every GPU that
+ * loads the library until exit; larger scans get XR_ERR_ARG.  d_vol: N^3
+ * floats (channel 0); d_sino: C*V*Nd^2 floats, cleared then accumulated.
+ * Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default)
+ * without synchronizing; the caller's current device is restored on
+ * return.  Like the other entry points it returns XR_ERR_NODEV on a device
+ * that is not sm_100.  All calls share the scratch and it keeps the last
+ * call's contents, so calls that overlap on the GPU race; serialise them.
+ * The first call on a device resolves the scratch address
+ * (cudaGetSymbolAddress), and the first call on a context no other entry
+ * point has set up runs the detector-pitch division check (a kernel and a
+ * synchronize).  Every call copies the geometry table from host stack
+ * memory, so none may be captured into a CUDA graph: a call on a capturing
+ * stream returns XR_ERR_ARG and enqueues nothing. */
 xr_status xr_dev_forward_proj_only_static(xr_ctx *ctx, const float *d_vol, float *d_sino, xr_rotate dir,
                                           void *stream);
 

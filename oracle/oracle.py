@@ -24,6 +24,16 @@ _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
 
 
+def reference_root() -> str:
+    """The reference checkout oracle/Makefile builds from (XR_REFERENCE, else
+    the recipe's default); it may be absent (e.g. where only the prebuilt
+    checkers travel)."""
+    if os.environ.get("XR_REFERENCE"):
+        return os.environ["XR_REFERENCE"]
+    r = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True)
+    return r.stdout.strip() if r.returncode == 0 else ""
+
+
 def build(ref: bool = False) -> None:
     """Build liboracle.so (and, with ref=True, the reference host build)."""
     targets = ["all"] + (["ref"] if ref else [])
@@ -292,6 +302,21 @@ class Oracle:
         self.lib.or_orientation(ctypes.c_long(nv), K, _p(b), _p(mu), _p(md), _p(ev))
         return md.reshape((3,) + shp), ev.reshape((3,) + shp)
 
+    def angle_from_md(self, md):
+        """calcAngleFromMD (pca.cu:67-83): md (3, ...) -> angle (2, ...)."""
+        shp = md.shape[1:]
+        md = np.ascontiguousarray(md, np.float32).reshape(3, -1)
+        out = np.zeros((2, md.shape[1]), np.float32)
+        self.lib.or_angle_from_md(ctypes.c_long(md.shape[1]), _p(md), _p(out))
+        return out.reshape((2,) + shp)
+
+    def direction_normalization(self, md):
+        """directionNormalization (pca.cu:85-106) of a copy of md (3, ...)."""
+        shp = md.shape[1:]
+        out = np.ascontiguousarray(md, np.float32).reshape(3, -1).copy()
+        self.lib.or_direction_normalization(ctypes.c_long(out.shape[1]), _p(out))
+        return out.reshape((3,) + shp)
+
     def jacobi3(self, A):
         A = np.ascontiguousarray(A, np.float64).ravel()
         w = np.zeros(3)
@@ -377,6 +402,43 @@ class RefHost:
 
     def ratio(self, n, proj, sino, art):
         return float(self.lib.xr_ref_ratio(n, _p(proj), _p(sino), int(art)))
+
+    def fdk_weight(self):
+        """calcWeight (fdk.cu:13-26): (Nd, Nd)."""
+        w = np.zeros(self.s.Nd * self.s.Nd, np.float32)
+        self.lib.xr_ref_fdk_weight(_p(w))
+        return w.reshape(self.s.Nd, self.s.Nd)
+
+    def fdk_filter(self):
+        """The filter table of FDK::reconstruct (reconstruct.cu:1692-1698)."""
+        f = np.zeros(self.s.Nd, np.float32)
+        self.lib.xr_ref_fdk_filter(_p(f))
+        return f
+
+    def fdk_reconstruct(self, sino, rotate_ccw=0):
+        """FDK::reconstruct (reconstruct.cu:1651-1724) with the reference's
+        fdk.cu kernels: returns (volumes (C, N, N, N), filtered sinograms)."""
+        s = self.s
+        sino = np.ascontiguousarray(sino, np.float32).ravel()
+        vol = np.zeros(s.C * s.N ** 3, np.float32)
+        filt = np.zeros_like(sino)
+        self.lib.xr_ref_fdk_reconstruct(_p(sino), _p(vol), _p(filt), int(rotate_ccw))
+        return vol.reshape(s.C, s.N, s.N, s.N), filt.reshape(s.C, s.V, s.Nd, s.Nd)
+
+    def angle_from_md(self, md):
+        """calcAngleFromMD (pca.cu:67-83) on md (3, nz, ny, nx)."""
+        nz, ny, nx = md.shape[1:]
+        md = np.ascontiguousarray(md, np.float32)
+        out = np.zeros((2, nz, ny, nx), np.float32)
+        self.lib.xr_ref_angle_from_md(_p(md), _p(out), nx, ny, nz)
+        return out
+
+    def direction_normalization(self, md):
+        """directionNormalization (pca.cu:85-106) of a copy of md (3, nz, ny, nx)."""
+        nz, ny, nx = md.shape[1:]
+        out = np.ascontiguousarray(md, np.float32).copy()
+        self.lib.xr_ref_direction_normalization(_p(out), nx, ny, nz)
+        return out
 
     def backward_slab(self, cond, y, n, proj, tmp, factor, xtt):
         self.lib.xr_ref_backward_slab(cond, y, n, _p(proj), _p(tmp), _p(factor), int(xtt))

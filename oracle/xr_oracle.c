@@ -7,7 +7,8 @@
  * to check results.
  *
  * Exports or32_* (FP32, the reference's operation order) and or64_* (FP64),
- * plus or_orientation (FP64 Jacobi restatement of direction/src/pca.cu:12-55).
+ * plus or_orientation (FP64 Jacobi restatement of direction/src/pca.cu:12-55)
+ * and or_angle_from_md / or_direction_normalization (pca.cu:67-106).
  */
 #define _GNU_SOURCE
 #include <math.h>
@@ -133,6 +134,40 @@ void or_orientation(long nvox, int K, const float *basis, const float *mu, float
         for (int a = 0; a < 3; a++) {
             md[(long)a * nvox + i] = (float)(sg * mean * v0[a]);
             ev[(long)a * nvox + i] = (float)(w[a] / tr);
+        }
+    }
+}
+
+/* calcAngleFromMD, direction/src/pca.cu:67-83, elementwise over nvox voxels
+ * of three planes: the reference's std::atan2 and std::sqrt of floats are
+ * their float overloads (atan2f, sqrtf).  angle: phi plane, theta plane. */
+void or_angle_from_md(long nvox, const float *md, float *angle) {
+    for (long i = 0; i < nvox; i++) {
+        const float m0 = md[i], m1 = md[nvox + i], m2 = md[2 * nvox + i];
+        if (m1 < 0.f) {
+            angle[i] = atan2f(-m1, -m0);
+            angle[nvox + i] = atan2f(sqrtf(m1 * m1 + m0 * m0), -m2);
+        } else {
+            angle[i] = atan2f(m1, m0);
+            angle[nvox + i] = atan2f(sqrtf(m1 * m1 + m0 * m0), m2);
+        }
+    }
+}
+
+/* directionNormalization, direction/src/pca.cu:85-106, in place: unit
+ * vectors where the length exceeds 0.65, zero vectors elsewhere. */
+void or_direction_normalization(long nvox, float *md) {
+    for (long i = 0; i < nvox; i++) {
+        const float x = md[i], y = md[nvox + i], z = md[2 * nvox + i];
+        const float norm = sqrtf(x * x + y * y + z * z);
+        if (norm > 0.65f) {
+            md[i] = x / norm;
+            md[nvox + i] = y / norm;
+            md[2 * nvox + i] = z / norm;
+        } else {
+            md[i] = 0.f;
+            md[nvox + i] = 0.f;
+            md[2 * nvox + i] = 0.f;
         }
     }
 }

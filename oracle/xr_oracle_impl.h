@@ -11,10 +11,11 @@
  *
  * Pinned against: oracle/_ref/libxrref.so, the reference's own
  * reconstruct/src/ir.cu compiled through oracle/ref_shim, via the golden
- * vectors in tests/golden (tests/golden/make_golden.py).  The FDK part
- * (reconstruct/src/fdk.cu) cannot be compiled for the host (fdk.cu:330 holds a
- * kernel launch) and the orientation part needs Eigen, which is absent: those
- * two are restatements without a reference-run pin.
+ * vectors in tests/golden (tests/golden/make_golden.py).  The FDK part is
+ * pinned the same way against the reference's fdk.cu kernels (lines 1-170,
+ * built for the host from a slice: the file's later Hilbert variant holds a
+ * kernel launch) by tests/golden/make_golden_fdk.py.  The orientation step
+ * needs Eigen, which is absent: a restatement without a reference-run pin.
  *
  * Layouts follow the reference: volumes x-fastest (idx = x + N*y + N*N*z,
  * volume.h:65-71), K channels of N^3 back to back (ir.cu:1788-1790);
@@ -817,21 +818,52 @@ void RV(voxel_sqrt)(const or_scan *s, real *vol) {
 }
 
 /* The normalised forward operator A of the reconstruction loops: forward +
- * correlation for every axis and view (what the loops compare with b). */
+ * correlation for every axis and view (what the loops compare with b).  The
+ * (axis, view) pairs run in parallel (OpenMP): each writes only its own view
+ * image with a private weight image, so the result is the serial one bit for
+ * bit. */
 void RV(forward_all)(const or_scan *s, const real *vol, real *proj, int rotate_ccw, int xtt) {
     const long Nd = s->Nd, V = s->V;
     const long lenD = Nd * Nd * V;
     const int rotation = rotate_ccw ? -1 : 1;
-    real *factor = (real *)malloc(sizeof(real) * Nd * Nd);
     memset(proj, 0, sizeof(real) * lenD * s->C);
-    for (int cond = 0; cond < s->C; cond++)
-        for (long w = 0; w < V; w++) {
-            const int n = rotation * (int)w;
+#pragma omp parallel
+    {
+        real *factor = (real *)malloc(sizeof(real) * Nd * Nd);
+#pragma omp for schedule(dynamic, 1)
+        for (long i = 0; i < (long)s->C * V; i++) {
+            const int cond = (int)(i / V);
+            const int n = rotation * (int)(i % V);
             memset(factor, 0, sizeof(real) * Nd * Nd);
             RV(forward_view)(s, cond, n, vol, proj + lenD * cond, factor, xtt);
             RV(correlation)(s, cond, n, proj + lenD * cond, factor);
         }
-    free(factor);
+        free(factor);
+    }
+}
+
+/* The forward + correlation of one subset's views of every axis, in parallel:
+ * within a subset the views (sub + batch*j) % V are distinct (a wrapped index
+ * is congruent to sub - V modulo batch, never to sub), so every (axis, view)
+ * pair writes its own image; the serial loops' order of float sums inside each
+ * image is kept. */
+static void RV(forward_subset)(const or_scan *s, const real *vol, real *proj, int n_cond, int sub, int batch,
+                               int subsetSize, int rotation, int xtt) {
+    const long Nd = s->Nd, V = s->V;
+    const long lenD = Nd * Nd * V;
+#pragma omp parallel
+    {
+        real *pf = (real *)malloc(sizeof(real) * Nd * Nd);
+#pragma omp for schedule(dynamic, 1)
+        for (long i = 0; i < (long)n_cond * subsetSize; i++) {
+            const int cond = (int)(i / subsetSize), j = (int)(i % subsetSize);
+            const int n = rotation * (int)((sub + batch * j) % V);
+            memset(pf, 0, sizeof(real) * Nd * Nd);
+            RV(forward_view)(s, cond, n, vol, proj + lenD * cond, pf, xtt);
+            RV(correlation)(s, cond, n, proj + lenD * cond, pf);
+        }
+        free(pf);
+    }
 }
 
 /* IR::reconstruct, reconstruct.cu:23-156.  orders holds C*epoch rows of the
@@ -844,37 +876,49 @@ void RV(ir_reconstruct)(const or_scan *s, real **sino, real **vol, int epoch, in
     const int rotation = rotate_ccw ? -1 : 1;
     const int subsetSize = (int)((V + batch - 1) / batch);
     real *proj = (real *)malloc(sizeof(real) * lenD);
-    real *pf = (real *)malloc(sizeof(real) * Nd * Nd);
-    real *tmp = (real *)malloc(sizeof(real) * N * N);
-    real *fac = (real *)malloc(sizeof(real) * N * N);
     for (int cond = 0; cond < s->C; cond++) {
+        /* one axis at a time (the reference's outer loop, :64): a scan of
+         * this axis alone, so the subset helper sees one axis block */
+        or_scan one = *s;
+        one.C = 1;
+        one.rot = s->rot + 9 * cond;
+        one.trans = s->trans + 3 * cond;
+        one.offset = s->offset + 3 * cond;
         for (int ep = 0; ep < epoch; ep++) {
             const int *order = orders + ((long)cond * epoch + ep) * batch;
             real loss = (real)0;
             memset(proj, 0, sizeof(real) * lenD);
             for (int b = 0; b < batch; b++) {
                 const int sub = order[b];
+                /* forward + correlation in parallel, then the ratios in the
+                 * serial order of the single loss accumulator */
+                RV(forward_subset)(&one, vol[cond], proj, 1, sub, batch, subsetSize, rotation, 0);
                 for (int j = 0; j < subsetSize; j++) {
-                    memset(pf, 0, sizeof(real) * Nd * Nd);
                     const int n = rotation * (int)((sub + batch * j) % V);
-                    RV(forward_view)(s, cond, n, vol[cond], proj, pf, 0);
-                    RV(correlation)(s, cond, n, proj, pf);
                     RV(ratio)(s, n, proj, sino[cond], art, &loss);
                 }
-                for (int y = 0; y < N; y++) {
-                    memset(tmp, 0, sizeof(real) * N * N);
-                    memset(fac, 0, sizeof(real) * N * N);
-                    for (int j = 0; j < subsetSize; j++) {
-                        const int n = rotation * (int)((sub + batch * j) % V);
-                        RV(backward_slab)(s, cond, y, n, proj, tmp, fac, 0);
+#pragma omp parallel
+                {
+                    real *tmp = (real *)malloc(sizeof(real) * N * N);
+                    real *fac = (real *)malloc(sizeof(real) * N * N);
+#pragma omp for schedule(dynamic, 1)
+                    for (int y = 0; y < N; y++) {
+                        memset(tmp, 0, sizeof(real) * N * N);
+                        memset(fac, 0, sizeof(real) * N * N);
+                        for (int j = 0; j < subsetSize; j++) {
+                            const int n = rotation * (int)((sub + batch * j) % V);
+                            RV(backward_slab)(&one, 0, y, n, proj, tmp, fac, 0);
+                        }
+                        RV(voxel_update)(s, y, vol[cond], tmp, fac, art, lambda / (real)subsetSize);
                     }
-                    RV(voxel_update)(s, y, vol[cond], tmp, fac, art, lambda / (real)subsetSize);
+                    free(tmp);
+                    free(fac);
                 }
             }
             if (losses) losses[(long)cond * epoch + ep] = loss;
         }
     }
-    free(proj); free(pf); free(tmp); free(fac);
+    free(proj);
 }
 
 /* XTT::reconstruct, reconstruct.cu:799-927 (without the orientation step;
@@ -888,40 +932,46 @@ void RV(xtt_reconstruct)(const or_scan *s, const real *sino, real *vol, real *pr
     const long lenD = Nd * Nd * V, lenV = N * N * N, lenP = N * N;
     const int rotation = rotate_ccw ? -1 : 1;
     const int subsetSize = (int)((V + batch - 1) / batch);
-    real *pf = (real *)malloc(sizeof(real) * Nd * Nd);
-    real *tmp = (real *)malloc(sizeof(real) * lenP * K);
-    real *fac = (real *)malloc(sizeof(real) * lenP * K);
     for (int ep = 0; ep < epoch; ep++) {
         const int *order = orders + (long)ep * batch;
         real loss = (real)0;
         memset(proj, 0, sizeof(real) * lenD * s->C);
         for (int b = 0; b < batch; b++) {
             const int sub = order[b];
+            /* forward + correlation of the subset in parallel, then the
+             * ratios in the serial order of the single loss accumulator */
+            RV(forward_subset)(s, vol, proj, s->C, sub, batch, subsetSize, rotation, 1);
             for (int cond = 0; cond < s->C; cond++)
                 for (int j = 0; j < subsetSize; j++) {
-                    memset(pf, 0, sizeof(real) * Nd * Nd);
                     const int n = rotation * (int)((sub + batch * j) % V);
-                    RV(forward_view)(s, cond, n, vol, proj + lenD * cond, pf, 1);
-                    RV(correlation)(s, cond, n, proj + lenD * cond, pf);
                     RV(ratio)(s, n, proj + lenD * cond, sino + lenD * cond, art, &loss);
                 }
-            for (int y = 0; y < N; y++) {
-                memset(tmp, 0, sizeof(real) * lenP * K);
-                memset(fac, 0, sizeof(real) * lenP * K);
-                for (int cond = 0; cond < s->C; cond++)
-                    for (int j = 0; j < subsetSize; j++) {
-                        const int n = rotation * (int)((sub + batch * j) % V);
-                        RV(backward_slab)(s, cond, y, n, proj + lenD * cond, tmp, fac, 1);
-                    }
-                for (long k = 0; k < K; k++)
-                    RV(voxel_update)(s, y, vol + lenV * k, tmp + lenP * k, fac + lenP * k, art,
-                                     lambda / (real)subsetSize);
+            /* slabs in parallel: each reads the ratio images and updates its
+             * own y slab of every channel */
+#pragma omp parallel
+            {
+                real *tmp = (real *)malloc(sizeof(real) * lenP * K);
+                real *fac = (real *)malloc(sizeof(real) * lenP * K);
+#pragma omp for schedule(dynamic, 1)
+                for (int y = 0; y < N; y++) {
+                    memset(tmp, 0, sizeof(real) * lenP * K);
+                    memset(fac, 0, sizeof(real) * lenP * K);
+                    for (int cond = 0; cond < s->C; cond++)
+                        for (int j = 0; j < subsetSize; j++) {
+                            const int n = rotation * (int)((sub + batch * j) % V);
+                            RV(backward_slab)(s, cond, y, n, proj + lenD * cond, tmp, fac, 1);
+                        }
+                    for (long k = 0; k < K; k++)
+                        RV(voxel_update)(s, y, vol + lenV * k, tmp + lenP * k, fac + lenP * k, art,
+                                         lambda / (real)subsetSize);
+                }
+                free(tmp);
+                free(fac);
             }
         }
         if (losses) losses[ep] = loss;
     }
     RV(voxel_sqrt)(s, vol);
-    free(pf); free(tmp); free(fac);
 }
 
 /* ---------------------------------------------------------------- FDK ---- */

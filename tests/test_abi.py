@@ -13,9 +13,10 @@ import numpy as np
 import pytest
 
 from conftest import ROOT, gpu_available, load_xr
+from oracle import reference_root
 
 HEADERS = [os.path.join(ROOT, "include", "xr.h"), os.path.join(ROOT, "include", "xr_learn.h")]
-REF_SETTINGS = "/root/reference/utility/settings.json"
+REF_SETTINGS = os.path.join(reference_root() or "-", "utility", "settings.json")
 
 
 def declared_functions():

@@ -29,6 +29,20 @@ def rel_err(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
 
 
+class _DevFloats:
+    """A float32 device buffer owned by libxr, seen through the CUDA array
+    interface (read-only use: copied to the host at once)."""
+
+    def __init__(self, ptr, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def _device_array(ptr, shape):
+    torch.cuda.synchronize()
+    return torch.as_tensor(_DevFloats(ptr, shape), device="cuda").cpu().numpy()
+
+
 def _case(rot, N, Nd, V, K, seed):
     rng = np.random.default_rng(seed)
     C = rot.shape[0]
@@ -135,6 +149,30 @@ def test_fiber_session(oracle, method, K):
     assert not np.array_equal(ref[0], v0[0])
     assert np.array_equal(got[1:], v0[1:])             # only channel 0 is updated
     assert rel_err(got, ref) <= TOL
+
+
+@pytest.mark.parametrize("method", ["MLEM", "ART"])
+def test_fiber_session_views_revisited(oracle, method):
+    """V % batch != 0 (V = 7, batch = 3): the last view of some subsets wraps
+    around to a view an earlier subset of the same epoch already ratioed, and
+    its forward adds onto that ratio image (reconstruct.cu:1302-1326).  The
+    volume and the last ratio images are compared with the oracle."""
+    xr = load_xr()
+    s, ctx = _case(three_axes(), 12, 20, 7, 4, 80)
+    truth = np.abs(_fiber_volume(12, 4, 81))
+    sino = _oracle_forward(oracle, s, truth)
+    v0 = np.full((4, 12, 12, 12), 0.01, np.float32)
+    ref, ref_proj = _oracle_session(oracle, s, sino, v0, 2, 3, method == "ART", 1e-2)
+    db, dv = torch.from_numpy(sino).cuda(), torch.from_numpy(v0).cuda()
+    torch.cuda.synchronize()
+    ctx.dev_session_begin_fiber(db.data_ptr(), dv.data_ptr(), 2, 3, method=xr.Method[method], lam=1e-2)
+    for _ in range(2):
+        ctx.dev_session_epoch()
+    proj = _device_array(ctx.dev_session_proj(), (s.C, s.V, s.Nd, s.Nd))
+    ctx.dev_session_end(0, 0)
+    got = dv.cpu().numpy()
+    assert rel_err(got, ref) <= TOL
+    assert rel_err(proj, ref_proj) <= TOL
 
 
 def test_fiber_reconstruct_host(oracle):

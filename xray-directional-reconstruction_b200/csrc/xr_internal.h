@@ -145,6 +145,8 @@ struct xr_ctx {
     xr::DevBuf fdk_filt, fdk_weight, fdk_sf;
     bool dev_ready = false;
     double *h_loss = nullptr;          /* pinned, kLossSlots doubles                */
+    int static_rdet = -1;              /* xr_dev_forward_proj_only_static: its own
+                                          result of the division check (-1: not run) */
 
     /* column-aligned axes (grating direction = +-grid axis for every view) */
     int col_rotation = 0;              /* rotation the column info was built for   */

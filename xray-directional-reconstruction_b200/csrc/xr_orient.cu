@@ -65,7 +65,8 @@ __global__ void k_orientation(long nvox, int K, const BasisConst *B, const TS *m
 __global__ void k_angle_from_md(long nvox, const float *md, float *angle) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nvox; i += (long)gridDim.x * blockDim.x) {
         const float m0 = md[i], m1 = md[nvox + i], m2 = md[2 * nvox + i];
-        const float r = sqrtf(m1 * m1 + m0 * m0);
+        /* the reference's std::sqrt(m1 * m1 + m0 * m0), rounded op by op */
+        const float r = __fsqrt_rn(__fadd_rn(__fmul_rn(m1, m1), __fmul_rn(m0, m0)));
         if (m1 < 0.f) {
             angle[i] = atan2f(-m1, -m0);
             angle[nvox + i] = atan2f(r, -m2);
@@ -76,13 +77,15 @@ __global__ void k_angle_from_md(long nvox, const float *md, float *angle) {
     }
 }
 
-/* directionNormalization, direction/src/pca.cu:85-106 (threshold 0.65). */
+/* directionNormalization, direction/src/pca.cu:85-106 (threshold 0.65): the
+ * length and the quotients rounded op by op as the reference's host code, so
+ * the threshold decision and the results are its own bit for bit. */
 __global__ void k_direction_normalization(long nvox, float *md) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nvox; i += (long)gridDim.x * blockDim.x) {
         const float x = md[i], y = md[nvox + i], z = md[2 * nvox + i];
-        const float n = sqrtf(x * x + y * y + z * z);
+        const float n = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
         if (n > 0.65f) {
-            md[i] = x / n; md[nvox + i] = y / n; md[2 * nvox + i] = z / n;
+            md[i] = __fdiv_rn(x, n); md[nvox + i] = __fdiv_rn(y, n); md[2 * nvox + i] = __fdiv_rn(z, n);
         } else {
             md[i] = 0.f; md[nvox + i] = 0.f; md[2 * nvox + i] = 0.f;
         }
