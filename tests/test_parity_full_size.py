@@ -86,9 +86,13 @@ def test_c3_xtt_epoch(c3, oracle):
           f"loss {gl[0]:.6e} vs {rl[0]:.6e}")
     assert e_mu <= TOL
     assert e_ratio <= TOL
-    # the oracle adds 13.3 M terms into one float (as the reference's single
-    # loss accumulator does, ir.cu:1623); libxr sums in FP64
-    assert np.allclose(gl, rl, rtol=2e-3)
+    # The FP32 oracle adds the 13.3 M terms |b - p| into one float, as the
+    # reference's single loss accumulator does (ir.cu:1623): at ~5e7 that sum
+    # drops every term below half an ulp (2) and ends ~2 % low.  libxr sums
+    # in FP64, so its loss is compared with the FP64 oracle's.
+    _, _, rl64 = oracle.xtt_reconstruct(s, b.astype(np.float64), v0.astype(np.float64), 1, 5, dt=np.float64)
+    print(f"loss: libxr {gl[0]:.9e}, FP64 oracle {rl64[0]:.9e}, FP32 oracle {rl[0]:.9e}")
+    assert np.allclose(gl, rl64, rtol=1e-4)
 
 
 def test_xtt_tile_overflow_large_n(oracle):
