@@ -49,6 +49,9 @@ __device__ __forceinline__ float div_det(float a, const GeomConst &g) {
     return __fmaf_rn(r, g.rdet, q);
 }
 
+/* A pair with both lanes equal: the broadcast operand of packed FP32x2 ops. */
+__device__ __forceinline__ float2 bc2(float x) { return make_float2(x, x); }
+
 template <int G>
 struct Ax {
     static constexpr int A = (G == 0) ? 1 : 0;   /* the two other axes, ascending */
@@ -195,80 +198,106 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
     const int igb = g0 + seg * 4;
     const bool col_ok = ia < N && ib < N;
     const float ba = vox_base(ia, N, g.vs), bb = vox_base(ib, N, g.vs);
-    float bg[4];
+    /* o_g = (p_g - off_g) - t_g of each voxel (rayCasting's g component of
+     * the source-to-voxel vector): off_g and t_g are the same for every view
+     * of a column-aligned axis (checked on the host), so this is per voxel */
+    float2 dgp[2];
     bool okv[4];
+    {
+        const float offg = fr[0].off[G], tg = fr[0].t[G];
+        float dgq[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        bg[q] = vox_base(igb + q, N, g.vs);
-        okv[q] = col_ok && (igb + q <= g1);
+        for (int q = 0; q < 4; q++) {
+            dgq[q] = __fsub_rn(__fsub_rn(vox_base(igb + q, N, g.vs), offg), tg);
+            okv[q] = col_ok && (igb + q <= g1);
+        }
+        dgp[0] = make_float2(dgq[0], dgq[1]);
+        dgp[1] = make_float2(dgq[2], dgq[3]);
     }
 
-    /* per-voxel value: plain ratio*mu; XTT a0 and M of this axis (xyz order) */
-    float val[4], m[4][6];
+    /* per-voxel value: plain mu; XTT a0 and M of this axis; kept as pairs
+     * of voxels (q = 2p, 2p + 1) for the packed FP32x2 arithmetic below */
+    float2 valp[2], mp[2][6];
     const size_t NN = (size_t)N * N, N3 = NN * N;
+    {
+        float val[4], m[4][6];
+        /* the thread's voxels are consecutive along g: index idx0 + q * stride_g */
+        const size_t sgs = (G == 0) ? 1 : (G == 1 ? (size_t)N : NN);
+        size_t idx0;
+        {
+            int x, y, z;
+            xyz_of<G>(ia, ib, igb, x, y, z);
+            idx0 = (size_t)x + (size_t)N * y + NN * z;
+        }
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        val[q] = 0.f;
+        for (int q = 0; q < 4; q++) {
+            val[q] = 0.f;
 #pragma unroll
-        for (int e = 0; e < 6; e++) m[q][e] = 0.f;
-        if (!okv[q]) continue;
-        int x, y, z;
-        xyz_of<G>(ia, ib, igb + q, x, y, z);
-        const size_t idx = (size_t)x + (size_t)N * y + NN * z;
-        if (MODE == 0) {
-            val[q] = ldgf<T>(vol + idx);
-        } else if (MODE == 2) {
-            val[q] = 1.0f;
-        } else if (MODE == 3) {   /* XTT with the voxel's rotated basis (forwardOrth, ir.cu:294-364) */
-            orth_moments<T>(a.basis, cond, g.K, a.coef_kind ? 1.0f : __fmul_rn(g.vs, g.ratio), vol, a.coef,
-                            a.coef_kind, idx, N3, val[q], m[q]);
-        } else {
+            for (int e = 0; e < 6; e++) m[q][e] = 0.f;
+            if (!okv[q]) continue;
+            const size_t iq = idx0 + (size_t)q * sgs;
+            if (MODE == 0) {
+                val[q] = ldgf<T>(vol + iq);
+            } else if (MODE == 2) {
+                val[q] = 1.0f;
+            } else if (MODE == 3) {   /* XTT with the voxel's rotated basis (forwardOrth, ir.cu:294-364) */
+                orth_moments<T>(a.basis, cond, g.K, a.coef_kind ? 1.0f : __fmul_rn(g.vs, g.ratio), vol, a.coef,
+                                a.coef_kind, iq, N3, val[q], m[q]);
+            }
+        }
+        if (MODE == 1) {
+            /* a0 = sum_k g_kc |S_k|^2 mu_k and M = sum_k g_kc mu_k S_k S_k^T (scaled by
+             * vs * ratio), channel by channel for the thread's 4 voxels at once */
             const BasisConst *Bc = a.basis;
             const float sc = __fmul_rn(g.vs, g.ratio);
-            float s0m = 0.f, mm[6] = {0, 0, 0, 0, 0, 0};
             for (int k = 0; k < g.K; k++) {
                 const float gk = Bc->g[cond * g.K + k] * sc;
                 if (gk == 0.f) continue;
-                const float mu = ldgf<T>(vol + idx + (size_t)k * N3) * gk;
-                const float s0 = Bc->S[3 * k], s1 = Bc->S[3 * k + 1], s2 = Bc->S[3 * k + 2];
-                s0m = fmaf(Bc->S2[k], mu, s0m);
-                mm[0] = fmaf(mu * s0, s0, mm[0]);
-                mm[1] = fmaf(mu * s1, s1, mm[1]);
-                mm[2] = fmaf(mu * s2, s2, mm[2]);
-                mm[3] = fmaf(2.f * mu * s0, s1, mm[3]);
-                mm[4] = fmaf(2.f * mu * s0, s2, mm[4]);
-                mm[5] = fmaf(2.f * mu * s1, s2, mm[5]);
-            }
-            val[q] = s0m;
+                const float s0 = Bc->S[3 * k], s1 = Bc->S[3 * k + 1], s2 = Bc->S[3 * k + 2], s2k = Bc->S2[k];
+                const float e0 = s0 * s0, e1 = s1 * s1, e2 = s2 * s2;
+                const float e3 = 2.f * s0 * s1, e4 = 2.f * s0 * s2, e5 = 2.f * s1 * s2;
+                float mu[4];
 #pragma unroll
-            for (int e = 0; e < 6; e++) m[q][e] = mm[e];
+                const T *vk = vol + (size_t)k * N3 + idx0;
+#pragma unroll
+                for (int q = 0; q < 4; q++) mu[q] = okv[q] ? ldgf<T>(vk + (size_t)q * sgs) * gk : 0.f;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    val[q] = fmaf(s2k, mu[q], val[q]);
+                    m[q][0] = fmaf(mu[q], e0, m[q][0]);
+                    m[q][1] = fmaf(mu[q], e1, m[q][1]);
+                    m[q][2] = fmaf(mu[q], e2, m[q][2]);
+                    m[q][3] = fmaf(mu[q], e3, m[q][3]);
+                    m[q][4] = fmaf(mu[q], e4, m[q][4]);
+                    m[q][5] = fmaf(mu[q], e5, m[q][5]);
+                }
+            }
         }
-    }
-    if (MODE == 1 || MODE == 3) {
+        /* bound on |contribution| over the CTA's voxels (weights c <= 1) */
+        float bound = 0.f;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (!okv[q]) continue;
+            float bq = (MODE == 0) ? fabsf(val[q]) * g.ratio : (MODE == 2 ? 1.0f : fabsf(val[q]));
+            if (MODE == 1 || MODE == 3)
+#pragma unroll
+                for (int e = 0; e < 6; e++) bq += fabsf(m[q][e]);
+            bound = fmaxf(bound, bq * 1.001f);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) bound = fmaxf(bound, __shfl_xor_sync(0xffffffffu, bound, o));
+        if ((tid & 31) == 0) s_red[tid >> 5] = bound;
         /* M in the column frame: (aa, bb, ab, ag, bg, gg), so that per view
          * d^T M d = aa da^2 + bb db^2 + ab da db + dg (ag da + bg db + gg dg) */
         constexpr int AB = 3 + A + B - 1, AG = 3 + A + G - 1, BG = 3 + B + G - 1;
+        constexpr int perm[6] = {A, B, AB, AG, BG, G};
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const float t[6] = {m[q][A], m[q][B], m[q][AB], m[q][AG], m[q][BG], m[q][G]};
+        for (int p = 0; p < 2; p++) {
+            valp[p] = make_float2(val[2 * p], val[2 * p + 1]);
 #pragma unroll
-            for (int e = 0; e < 6; e++) m[q][e] = t[e];
+            for (int e = 0; e < 6; e++) mp[p][e] = make_float2(m[2 * p][perm[e]], m[2 * p + 1][perm[e]]);
         }
     }
-    /* bound on |contribution| over the CTA's voxels (weights c <= 1) */
-    float bound = 0.f;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        if (!okv[q]) continue;
-        float bq = (MODE == 0) ? fabsf(val[q]) * g.ratio : (MODE == 2 ? 1.0f : fabsf(val[q]));
-        if (MODE == 1 || MODE == 3)
-#pragma unroll
-            for (int e = 0; e < 6; e++) bq += fabsf(m[q][e]);
-        bound = fmaxf(bound, bq * 1.001f);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) bound = fmaxf(bound, __shfl_xor_sync(0xffffffffu, bound, o));
-    if ((tid & 31) == 0) s_red[tid >> 5] = bound;
     __syncthreads();
     float S = 0.f;
 #pragma unroll
@@ -277,11 +306,10 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
     const int sh = fix_shift(S);
     const float fscale = ldexpf(1.0f, sh);
     const float finv = ldexpf(1.0f, -sh);
-
     const size_t NdNd = (size_t)Nd * Nd;
     float *outc = a.out + (size_t)cond * g.V * NdNd;
     for (int jj = 0; jj < nv; jj++) {
-        const ViewFrame f = fr[jj];          /* registers: no reload after the shared atomics */
+        const ViewFrame &f = fr[jj];
         const int4 bb4 = bbox[jj];
         int *T = smem + (jj & 1) * 2 * kTileCap;   /* hi words, lo words after */
         float *P = outc + (size_t)f.view * NdNd;
@@ -292,49 +320,60 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
         if (bb4.z > 0 && col_ok) {
             col_ray<G>(f, g, ba, bb, u, coeff, da, db);
             if (tap1(g, u, iu, fu, gu)) {
-                const float dab2 = fmaf(da, da, db * db);
-                const float daa = da * da, dbb = db * db, dab = da * db;
+                const int lu = iu - bb4.x;
+                const bool col_tile = use_tile && lu >= 0 && lu + 1 < bb4.z;
+                const int W = bb4.z;
+                int *tcol = T + lu;
+                float *pcol = P + iu;
+                const float2 dab2 = bc2(fmaf(da, da, db * db));
+                const float2 daa = bc2(da * da), dbb = bc2(db * db), dab = bc2(da * db);
+                const float2 da2 = bc2(da), db2 = bc2(db);
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     if (!okv[q]) continue;
-                    float dg;
-                    const float v = col_v<G>(f, g, bg[q], coeff, magsig, dg);
+                    const float dgs = (q & 1) ? dgp[q >> 1].y : dgp[q >> 1].x;
+                    const float av = __fmul_rn(__fmul_rn(coeff, dgs), magsig);
+                    const float v = __fadd_rn(div_det(av, g), g.half);
                     int iv;
                     float fv, gv;
                     if (!tap1(g, v, iv, fv, gv)) continue;
+                    float pvs;
+                    if (MODE == 0) {
+                        pvs = (q & 1) ? valp[q >> 1].y : valp[q >> 1].x;
+                    } else if (MODE == 2) {
+                        pvs = fscale;
+                    } else {
+                        float m[6];
+#pragma unroll
+                        for (int e = 0; e < 6; e++) m[e] = (q & 1) ? mp[q >> 1][e].y : mp[q >> 1][e].x;
+                        const float dd = fmaf(dgs, dgs, dab2.x);
+                        const float al = fmaf(m[0], daa.x, fmaf(m[1], dbb.x, m[2] * dab.x));
+                        const float be = fmaf(m[3], da, fmaf(m[4], db, m[5] * dgs));
+                        const float q2 = fmaf(dgs, be, al);
+                        const float vq = (q & 1) ? valp[q >> 1].y : valp[q >> 1].x;
+                        pvs = fmaf(q2, __fdividef(-1.0f, dd), vq) * fscale;
+                    }
                     const float c1 = __fmul_rn(gu, fv), c2 = __fmul_rn(fu, fv);
                     const float c3 = __fmul_rn(fu, gv), c4 = __fmul_rn(gu, gv);
-                    float w1, w2, w3, w4;
-                    if (MODE == 0) {
-                        const float pv = val[q];
-                        w1 = __fmul_rn(__fmul_rn(c1, g.ratio), pv);
-                        w2 = __fmul_rn(__fmul_rn(c2, g.ratio), pv);
-                        w3 = __fmul_rn(__fmul_rn(c3, g.ratio), pv);
-                        w4 = __fmul_rn(__fmul_rn(c4, g.ratio), pv);
-                    } else if (MODE == 2) {
-                        w1 = c1; w2 = c2; w3 = c3; w4 = c4;
+                    const int lv = iv - bb4.y;
+                    if (col_tile && lv >= 0 && lv + 1 < bb4.w) {
+                        int *t0 = tcol + W * lv;
+                        auto tap = [&](float c, int *adr) {
+                            float xs;
+                            if (MODE == 0) xs = __fmul_rn(__fmul_rn(c, g.ratio), pvs) * fscale;
+                            else xs = c * pvs;
+                            fix_add(adr, kTileCap, xs);
+                        };
+                        tap(c1, t0 + W); tap(c2, t0 + W + 1); tap(c3, t0 + 1); tap(c4, t0);
                     } else {
-                        const float dd = fmaf(dg, dg, dab2);
-                        const float al = fmaf(m[q][0], daa, fmaf(m[q][1], dbb, m[q][2] * dab));
-                        const float be = fmaf(m[q][3], da, fmaf(m[q][4], db, m[q][5] * dg));
-                        const float q2 = fmaf(dg, be, al);
-                        const float pv = val[q] - __fdividef(q2, dd);
-                        w1 = __fmul_rn(c1, pv); w2 = __fmul_rn(c2, pv);
-                        w3 = __fmul_rn(c3, pv); w4 = __fmul_rn(c4, pv);
-                    }
-                    const int lu = iu - bb4.x, lv = iv - bb4.y;
-                    if (use_tile && lu >= 0 && lu + 1 < bb4.z && lv >= 0 && lv + 1 < bb4.w) {
-                        int *t0 = T + lu + bb4.z * lv;
-                        fix_add(t0 + bb4.z, kTileCap, w1 * fscale);
-                        fix_add(t0 + bb4.z + 1, kTileCap, w2 * fscale);
-                        fix_add(t0 + 1, kTileCap, w3 * fscale);
-                        fix_add(t0, kTileCap, w4 * fscale);
-                    } else {
-                        float *p0 = P + iu + (size_t)Nd * iv;
-                        atomicAdd(p0 + Nd, w1);
-                        atomicAdd(p0 + Nd + 1, w2);
-                        atomicAdd(p0 + 1, w3);
-                        atomicAdd(p0, w4);
+                        float *p0 = pcol + (size_t)Nd * iv;
+                        auto tapg = [&](float c, float *adr) {
+                            float xs;
+                            if (MODE == 0) xs = __fmul_rn(__fmul_rn(c, g.ratio), pvs);
+                            else xs = c * pvs * finv;
+                            atomicAdd(adr, xs);
+                        };
+                        tapg(c1, p0 + Nd); tapg(c2, p0 + Nd + 1); tapg(c3, p0 + 1); tapg(c4, p0);
                     }
                 }
             }
@@ -393,12 +432,14 @@ struct BackColArgs {
  * and the brick-linear final pass all hit 32 different banks. */
 __device__ __forceinline__ int sacc_slot(int lv) { return lv ^ ((lv >> 5) & 7) ^ (((lv >> 6) & 3) << 3); }
 
-/* One view of one axis for a thread's column segment of 4 voxels: the ray
- * set-up once, then per voxel v, the taps and the 4-tap gather from the
- * (L2-resident) ratio image. */
+/* One view of one axis for a thread's column segment of 4 voxels (two pairs
+ * in packed FP32x2 arithmetic, each lane rounded as the scalar form): the
+ * ray set-up once, then per voxel v, the taps and the 4-tap gather from the
+ * (L2-resident) ratio image, accumulated into the moments of the pair.
+ * dg: o_g of the voxels (per axis, view-independent); okq: voxel in range. */
 template <int MODE, int G>
 __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f, float magsig, float ba, float bb,
-                                          const float bg[4], int nq, const float *Pv, float acc[4][7]) {
+                                          const float2 dg[2], const bool okq[4], const float *Pv, float2 acc[2][7]) {
     constexpr int A = Ax<G>::A, B = Ax<G>::B;
     const int Nd = g.Nd;
     float u, coeff, da, db;
@@ -406,58 +447,76 @@ __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f
     int iu;
     float fu, gu;
     if (!tap1(g, u, iu, fu, gu)) return;
-    const float dab2 = fmaf(da, da, db * db);
+    const float2 dab2 = bc2(fmaf(da, da, db * db));
     const float *Pc = Pv + iu;
-    /* Two phases: first every voxel's taps and its 4 gathers (16 loads in
-     * flight; a voxel off the detector reads row 0 and is dropped), then the
-     * accumulation. */
-    float fv[4], gv[4], dg[4], pr[4][4];
+    /* the products of d = (d_A, d_B, d_G) that do not involve d_G */
+    const float2 daa = bc2(da * da), dbb = bc2(db * db), dab = bc2(da * db), da2 = bc2(da), db2 = bc2(db);
+    /* Two phases: first both pairs' taps and their 16 gathers (a voxel off
+     * the detector reads row 0 and is dropped), then the accumulation. */
+    float2 fv[2], gv[2], p0[2], p1[2], p2[2], p3[2];
     bool ok[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const float v = col_v<G>(f, g, bg[q], coeff, magsig, dg[q]);
-        int iv = 0;
-        ok[q] = (q < nq) && tap1(g, v, iv, fv[q], gv[q]);
+    for (int p = 0; p < 2; p++) {
+        const float2 av = __fmul2_rn(__fmul2_rn(bc2(coeff), dg[p]), bc2(magsig));
+        float2 v;
+        if (g.exact_rdet) {
+            const float2 qd = __fmul2_rn(av, bc2(g.rdet));
+            const float2 rd = __ffma2_rn(qd, bc2(-g.det), av);
+            v = __fadd2_rn(__ffma2_rn(rd, bc2(g.rdet), qd), bc2(g.half));
+        } else {
+            v = __fadd2_rn(make_float2(__fdiv_rn(av.x, g.det), __fdiv_rn(av.y, g.det)), bc2(g.half));
+        }
+        ok[2 * p] = okq[2 * p] && 0.55f < v.x && v.x < g.lim;
+        ok[2 * p + 1] = okq[2 * p + 1] && 0.55f < v.y && v.y < g.lim;
+        const float2 ut = __fadd2_rn(v, bc2(-0.5f));
+        const float2 fi = make_float2(floorf(ut.x), floorf(ut.y));
+        fv[p] = __ffma2_rn(fi, bc2(-1.0f), ut);
+        gv[p] = __ffma2_rn(fv[p], bc2(-1.0f), bc2(1.0f));
         if (MODE != B_SENS) {
-            const float *pp = Pc + (size_t)Nd * (ok[q] ? iv : 0);
-            pr[q][0] = __ldg(pp);
-            pr[q][1] = __ldg(pp + 1);
-            pr[q][2] = __ldg(pp + Nd);
-            pr[q][3] = __ldg(pp + Nd + 1);
+            const float *q0 = Pc + Nd * (ok[2 * p] ? (int)fi.x : 0);
+            const float *q1 = Pc + Nd * (ok[2 * p + 1] ? (int)fi.y : 0);
+            p0[p] = make_float2(__ldg(q0), __ldg(q1));
+            p1[p] = make_float2(__ldg(q0 + 1), __ldg(q1 + 1));
+            p2[p] = make_float2(__ldg(q0 + Nd), __ldg(q1 + Nd));
+            p3[p] = make_float2(__ldg(q0 + Nd + 1), __ldg(q1 + Nd + 1));
         }
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        if (!ok[q]) continue;
-        float nb = 0.f;
+    for (int p = 0; p < 2; p++) {
+        if (!(ok[2 * p] || ok[2 * p + 1])) continue;
+        /* a voxel off the detector contributes nothing: its lane is zeroed */
+        const float2 m = make_float2(ok[2 * p] ? 1.0f : 0.0f, ok[2 * p + 1] ? 1.0f : 0.0f);
+        float2 nb = bc2(0.0f);
         if (MODE != B_SENS) {
-            const float c1 = __fmul_rn(gu, fv[q]), c2 = __fmul_rn(fu, fv[q]);
-            const float c3 = __fmul_rn(fu, gv[q]), c4 = __fmul_rn(gu, gv[q]);
-            nb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(c1, pr[q][2]), __fmul_rn(c2, pr[q][3])),
-                                     __fmul_rn(c3, pr[q][1])),
-                           __fmul_rn(c4, pr[q][0]));
+            /* numBack in the reference's order (ir.cu:1744-1750) */
+            const float2 c1 = __fmul2_rn(bc2(gu), fv[p]), c2 = __fmul2_rn(bc2(fu), fv[p]);
+            const float2 c3 = __fmul2_rn(bc2(fu), gv[p]), c4 = __fmul2_rn(bc2(gu), gv[p]);
+            nb = __fadd2_rn(__fadd2_rn(__fadd2_rn(__fmul2_rn(c1, p2[p]), __fmul2_rn(c2, p3[p])),
+                                       __fmul2_rn(c3, p1[p])),
+                            __fmul2_rn(c4, p0[p]));
+            nb = __fmul2_rn(nb, m);
         }
         if (MODE == B_PLAIN) {
-            acc[q][0] = __fadd_rn(acc[q][0], nb);     /* tmp    (ir.cu:1750) */
-            acc[q][1] = __fadd_rn(acc[q][1], 1.0f);   /* factor (ir.cu:1749) */
+            acc[p][0] = __fadd2_rn(acc[p][0], nb);   /* tmp    (ir.cu:1750) */
+            acc[p][1] = __fadd2_rn(acc[p][1], m);    /* factor (ir.cu:1749) */
         } else {
-            float d[3];
-            d[A] = da; d[B] = db; d[G] = dg[q];
-            const float inv = __fdividef(1.0f, fmaf(dg[q], dg[q], dab2));   /* approximate reciprocal, ~2 ulp */
-            float wgt;
+            const float2 dd = __ffma2_rn(dg[p], dg[p], dab2);
+            const float2 inv = make_float2(__fdividef(1.0f, dd.x), __fdividef(1.0f, dd.y));  /* ~2 ulp */
+            float2 wgt;
             if (MODE == B_XTT) {
-                acc[q][6] += nb;
-                wgt = nb * inv;
+                acc[p][6] = __fadd2_rn(acc[p][6], nb);
+                wgt = __fmul2_rn(nb, inv);
             } else {
-                acc[q][6] += 1.0f;
-                wgt = inv;
+                acc[p][6] = __fadd2_rn(acc[p][6], m);
+                wgt = __fmul2_rn(inv, m);
             }
-            acc[q][0] = fmaf(wgt, d[0] * d[0], acc[q][0]);
-            acc[q][1] = fmaf(wgt, d[1] * d[1], acc[q][1]);
-            acc[q][2] = fmaf(wgt, d[2] * d[2], acc[q][2]);
-            acc[q][3] = fmaf(wgt, d[0] * d[1], acc[q][3]);
-            acc[q][4] = fmaf(wgt, d[0] * d[2], acc[q][4]);
-            acc[q][5] = fmaf(wgt, d[1] * d[2], acc[q][5]);
+            /* d d^T in xyz order: d_A = da, d_B = db, d_G = dg */
+            const float2 dgg = __fmul2_rn(dg[p], dg[p]), dag = __fmul2_rn(da2, dg[p]), dbg = __fmul2_rn(db2, dg[p]);
+            float2 pr[6];
+            pr[A] = daa; pr[B] = dbb; pr[G] = dgg;
+            pr[3 + A + B - 1] = dab; pr[3 + A + G - 1] = dag; pr[3 + B + G - 1] = dbg;
+#pragma unroll
+            for (int e = 0; e < 6; e++) acc[p][e] = __ffma2_rn(wgt, pr[e], acc[p][e]);
         }
     }
 }
@@ -482,14 +541,27 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
     const float *P = a.proj + (size_t)cond * g.V * (size_t)Nd * Nd;
     const size_t NN = (size_t)N * N, NdNd = (size_t)Nd * Nd;
     const float ba = vox_base(ia, N, g.vs), bb = vox_base(ib, N, g.vs);
-    float bg[4];
+    /* o_g of the 4 voxels: off_g and t_g are the same for every view of a
+     * column-aligned axis (checked on the host) */
+    float2 dg[2];
+    bool okq[4];
+    {
+        const ViewFrame &f0 = a.frames[(size_t)cond * g.V];
+        const float offg = f0.off[G], tg = f0.t[G];
+        float d[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) bg[q] = vox_base(igb + q, N, g.vs);
-    float acc[4][7];
+        for (int q = 0; q < 4; q++) {
+            d[q] = __fsub_rn(__fsub_rn(vox_base(igb + q, N, g.vs), offg), tg);
+            okq[q] = q < nq;
+        }
+        dg[0] = make_float2(d[0], d[1]);
+        dg[1] = make_float2(d[2], d[3]);
+    }
+    float2 acc[2][7];
 #pragma unroll
-    for (int q = 0; q < 4; q++)
+    for (int p = 0; p < 2; p++)
 #pragma unroll
-        for (int e = 0; e < 7; e++) acc[q][e] = 0.f;
+        for (int e = 0; e < 7; e++) acc[p][e] = bc2(0.f);
     for (int c0 = 0; c0 < a.n_views; c0 += kFrameChunk) {
         const int nc = min(kFrameChunk, a.n_views - c0);
         __syncthreads();
@@ -501,58 +573,79 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
         __syncthreads();
         if (nq > 0)
             for (int jj = 0; jj < nc; jj++)
-                back_view<MODE, G>(g, fr[jj], magsig, ba, bb, bg, nq, P + (size_t)fr[jj].view * NdNd, acc);
+                back_view<MODE, G>(g, fr[jj], magsig, ba, bb, dg, okq, P + (size_t)fr[jj].view * NdNd, acc);
     }
     if (!col_ok) return;
+    if (MODE != B_PLAIN && !a.coef) {
+        /* fold the basis-independent moments into the channels:
+         * tmp_k += g_kc (|S_k|^2 sum r - S_k^T (sum r d d^T / d.d) S_k), channel by
+         * channel for the thread's 4 voxels at once */
+        const BasisConst *Bc = a.basis;
+        int lvq[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            int lx, ly, lz;
+            xyz_of<G>(ca, cb, sg * 4 + q, lx, ly, lz);
+            lvq[q] = sacc_slot(lx + 8 * ly + 64 * lz);
+        }
+        for (int k = 0; k < K; k++) {
+            const float gk = Bc->g[cond * K + k];
+            if (gk == 0.f) continue;
+            const float s0 = Bc->S[3 * k], s1 = Bc->S[3 * k + 1], s2 = Bc->S[3 * k + 2], s2k = Bc->S2[k];
+            const float e0 = s0 * s0, e1 = s1 * s1, e2 = s2 * s2;
+            const float e3 = 2.f * s0 * s1, e4 = 2.f * s0 * s2, e5 = 2.f * s1 * s2;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (q >= nq) continue;
+                const float2 *ap = acc[q >> 1];
+#define XR_AQ(e) ((q & 1) ? ap[e].y : ap[e].x)
+                const float sAs = e0 * XR_AQ(0) + e1 * XR_AQ(1) + e2 * XR_AQ(2) + e3 * XR_AQ(3) + e4 * XR_AQ(4) +
+                                  e5 * XR_AQ(5);
+                sacc[k * 512 + lvq[q]] += gk * fmaf(s2k, XR_AQ(6), -sAs);
+#undef XR_AQ
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         if (q >= nq) continue;
+        float aq[7];
+#pragma unroll
+        for (int e = 0; e < 7; e++) aq[e] = (q & 1) ? acc[q >> 1][e].y : acc[q >> 1][e].x;
         if (MODE == B_PLAIN) {
             /* voxelProduct (ir.cu:1637-1654) / voxelPlus (ir.cu:1682-1693) */
             int x, y, z;
             xyz_of<G>(ia, ib, igb + q, x, y, z);
             T *vp = reinterpret_cast<T *>(a.vol) + (size_t)x + (size_t)N * y + NN * z;
-            const float tmp = acc[q][0], fac = acc[q][1], mu = ldf<T>(vp);
+            const float tmp = aq[0], fac = aq[1], mu = ldf<T>(vp);
             const uint32_t key = (uint32_t)((size_t)x + (size_t)N * y + NN * z);
             if (a.art) stu<T>(vp, __fadd_rn(mu, __fmul_rn(a.alpha, tmp)), key, a.sr);
             else stu<T>(vp, (fac == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu, tmp), fac), key, a.sr);
-        } else {
+        } else {   /* backwardOrth(ByMD) (ir.cu:366-423, :233-292): the voxel's rotated basis */
             int lx, ly, lz;
             xyz_of<G>(ca, cb, sg * 4 + q, lx, ly, lz);
             const int lv = sacc_slot(lx + 8 * ly + 64 * lz);
             const BasisConst *Bc = a.basis;
-            if (a.coef) {   /* backwardOrth(ByMD) (ir.cu:366-423, :233-292): the voxel's rotated basis */
-                int x, y, z;
-                xyz_of<G>(ia, ib, igb + q, x, y, z);
-                float R[9];
-                src_rotation(a.coef, a.coef_kind, NN * N, (size_t)x + (size_t)N * y + NN * z, R);
-                const float G0 = Bc->G[3 * cond], G1 = Bc->G[3 * cond + 1], G2 = Bc->G[3 * cond + 2];
-                for (int k = 0; k < K; k++) {
-                    float S[3];
-                    orth_basis(Bc, k, R, S);
-                    const float h = S[0] * G0 + S[1] * G1 + S[2] * G2;
-                    const float sAs = S[0] * S[0] * acc[q][0] + S[1] * S[1] * acc[q][1] + S[2] * S[2] * acc[q][2] +
-                                      2.f * (S[0] * S[1] * acc[q][3] + S[0] * S[2] * acc[q][4] +
-                                             S[1] * S[2] * acc[q][5]);
-                    sacc[k * 512 + lv] +=
-                        (h * h) * fmaf(S[0] * S[0] + S[1] * S[1] + S[2] * S[2], acc[q][6], -sAs);
-                }
-                continue;
-            }
+            int x, y, z;
+            xyz_of<G>(ia, ib, igb + q, x, y, z);
+            float R[9];
+            src_rotation(a.coef, a.coef_kind, NN * N, (size_t)x + (size_t)N * y + NN * z, R);
+            const float G0 = Bc->G[3 * cond], G1 = Bc->G[3 * cond + 1], G2 = Bc->G[3 * cond + 2];
             for (int k = 0; k < K; k++) {
-                const float gk = Bc->g[cond * K + k];
-                if (gk == 0.f) continue;
-                const float s0 = Bc->S[3 * k], s1 = Bc->S[3 * k + 1], s2 = Bc->S[3 * k + 2];
-                const float sAs = s0 * s0 * acc[q][0] + s1 * s1 * acc[q][1] + s2 * s2 * acc[q][2] +
-                                  2.f * (s0 * s1 * acc[q][3] + s0 * s2 * acc[q][4] + s1 * s2 * acc[q][5]);
-                sacc[k * 512 + lv] += gk * fmaf(Bc->S2[k], acc[q][6], -sAs);
+                float S[3];
+                orth_basis(Bc, k, R, S);
+                const float h = S[0] * G0 + S[1] * G1 + S[2] * G2;
+                const float sAs = S[0] * S[0] * aq[0] + S[1] * S[1] * aq[1] + S[2] * S[2] * aq[2] +
+                                  2.f * (S[0] * S[1] * aq[3] + S[0] * S[2] * aq[4] + S[1] * S[2] * aq[5]);
+                sacc[k * 512 + lv] += (h * h) * fmaf(S[0] * S[0] + S[1] * S[1] + S[2] * S[2], aq[6], -sAs);
             }
         }
     }
 }
 
 template <int MODE, typename T>
-__global__ void __launch_bounds__(kBackThreads, 4) k_back_col(BackColArgs a) {
+__global__ void __launch_bounds__(kBackThreads, 5) k_back_col(BackColArgs a) {
     __shared__ ViewFrame fr[kFrameChunk];
     extern __shared__ float sacc[];   /* XTT / SENS: K x 512 per-voxel accumulators */
     const GeomConst &g = a.g;

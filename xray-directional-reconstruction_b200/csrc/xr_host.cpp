@@ -271,6 +271,9 @@ static int aligned_axis(const std::vector<ViewFrame> &h, int cond, int V, float 
             }
         }
         if (f.src[g] != 0.0f || f.eu[g] != 0.0f) return -1;
+        /* the column kernels compute o_g = (p_g - off_g) - t_g once per voxel
+         * for all views: off_g (= +-INIT_OFFSET_z, exact) and t_g must not vary */
+        if (f.off[g] != f0.off[g] || f.t[g] != f0.t[g]) return -1;
     }
     return g;
 }

@@ -38,6 +38,18 @@ __device__ __forceinline__ void fix_split(float xs, int &h, int &l) {
     l = __float_as_int(__fmaf_rn(__fsub_rn(xs, hf), kFixLoScale, kRoundMagic)) - kRoundMagicBits;
 }
 
+/* fix_split of two contributions at once (packed FP32x2 arithmetic on
+ * sm_100, each lane rounded exactly as the scalar form). */
+__device__ __forceinline__ void fix_split2(float2 xs, int2 &h, int2 &l) {
+    const float2 t = __fadd2_rn(xs, make_float2(kRoundMagic, kRoundMagic));
+    const float2 hf = __fadd2_rn(t, make_float2(-kRoundMagic, -kRoundMagic));
+    h = make_int2(__float_as_int(t.x) - kRoundMagicBits, __float_as_int(t.y) - kRoundMagicBits);
+    /* xs - hf (exact) as fma(hf, -1, xs), then one rounding of its 2^20 multiple */
+    const float2 r = __ffma2_rn(hf, make_float2(-1.0f, -1.0f), xs);
+    const float2 lt = __ffma2_rn(r, make_float2(kFixLoScale, kFixLoScale), make_float2(kRoundMagic, kRoundMagic));
+    l = make_int2(__float_as_int(lt.x) - kRoundMagicBits, __float_as_int(lt.y) - kRoundMagicBits);
+}
+
 /* tile word layout per buffer: [hi: cap ints][lo: cap ints] */
 __device__ __forceinline__ void fix_add(int *hi, int cap, float xs) {
     int h, l;
