@@ -41,8 +41,9 @@ PKG = os.path.join(ROOT, "xray-directional-reconstruction_b200")
 
 W = dict(N=256, Nd=384, V=180, C=3, K=13, batch=5, sdd=1000.0, sod=500.0, det=2.0, n_fibers=12, seed=5)
 # --size profile: the same kernels on a smaller case for ncu captures (volume
-# 192^3 x 13 = 368 MB, still larger than L2).
-W_PROFILE = dict(W, N=192, Nd=288, V=90)
+# 192^3 x 13 = 368 MB, still larger than L2), with the full workload's 36 views
+# per subset and axis, so per-launch instruction counts scale by voxel-views.
+W_PROFILE = dict(W, N=192, Nd=288, V=180)
 WORKLOAD = ("XTT 256^3 x K13, 3 axes x 180 views, 384^2 detector, OS-EM 5 subsets, FP32 "
             "(12 seeded fiber cylinders, SOD 500 / SDD 1000 mm, 1 mm voxels)")
 METRIC = "XTT 256^3x13 projector GB/s (effective, forward+back per OS-EM epoch)"
@@ -150,20 +151,43 @@ def conv_roofline(local: int, N: int = 256, reps: int = 3):
             "infer_ms": ms, "flops_per_inference": flops, "workload": f"{N}^3 x {channels}, depth {depth}, width {width}"}
 
 
-def profile_traffic(kernel: str):
-    """Per-launch DRAM bytes of `kernel` at this workload from the committed
-    ncu summary, if present (profiles/*.md line 'traffic_per_launch <kernel> <bytes>')."""
-    d = os.path.join(ROOT, "profiles")
-    if not os.path.isdir(d):
+PROFILE_JSON = os.path.join(ROOT, "profiles", "xtt_projectors_ncu.json")
+
+
+def profile_figures():
+    """Per-kernel figures of one ncu capture of the projector kernels on the
+    profile case (profiles/xtt_projectors_ncu.json: warp instructions and DRAM
+    bytes per launch, the voxel-views and sizes of that launch, the command)."""
+    if not os.path.exists(PROFILE_JSON):
         return None
-    for fn in sorted(os.listdir(d)):
-        if not fn.endswith((".md", ".txt")):
-            continue
-        for line in open(os.path.join(d, fn)):
-            m = re.match(r"\s*traffic_per_launch\s+(\S+)\s+([0-9.eE+]+)", line)
-            if m and m.group(1) == kernel:
-                return float(m.group(2))
-    return None
+    return json.load(open(PROFILE_JSON))
+
+
+def issue_roofline(kernel: str, launch_s: float, vox_views: float, n_vox: float, det_px_views: float,
+                   sm_mhz: float, hbm_peak: float):
+    """Roofline of a projector kernel against the resource that binds it: warp
+    instruction issue (4 schedulers per SM, one warp instruction per cycle
+    each).  achieved = warp instructions per launch / launch time, where the
+    instructions per launch are the captured count per voxel-view times this
+    launch's voxel-views; peak = 148 SMs x 4 x the SM clock sampled during
+    the timed region.  traffic = the captured DRAM read and write bytes, each
+    scaled to this launch by the unit the capture names for it (voxels for
+    volume-side traffic, pixel-views for detector images), and
+    hbm_frac_actual = traffic / launch time / measured HBM copy bandwidth."""
+    figs = profile_figures()
+    if not figs or kernel not in figs.get("kernels", {}):
+        return None
+    k = figs["kernels"][kernel]
+    inst = k["warp_inst_per_launch"] / k["voxel_views_per_launch"] * vox_views
+    unit = {"voxels": (n_vox, k["voxels_per_launch"]), "pixel_views": (det_px_views, k["pixel_views_per_launch"])}
+    traffic = sum(k[f"dram_{d}_bytes_per_launch"] * unit[k[f"scale_{d}"]][0] / unit[k[f"scale_{d}"]][1]
+                  for d in ("read", "write"))
+    peak = 148 * 4 * sm_mhz * 1e6
+    return {"bound": "issue", "kernel": kernel, "achieved": inst / launch_s / 1e9, "peak": peak / 1e9,
+            "unit": "G warp-instructions/s", "frac": inst / launch_s / peak, "traffic": traffic,
+            "hbm_frac_actual": traffic / launch_s / (hbm_peak * 1e9), "warp_inst_per_voxel_view":
+            k["warp_inst_per_launch"] / k["voxel_views_per_launch"], "sm_mhz": sm_mhz,
+            "source": os.path.relpath(PROFILE_JSON, ROOT) + " (" + figs.get("case", "") + ")"}
 
 
 class ClockSampler:
@@ -505,10 +529,132 @@ def run_c4(args, local):
     line = {"mode": "uneven_batch", "specimens": per, "epochs_timed": E, "storage": "bf16 volumes and sinograms, "
             "stochastic rounding", "sequential_ms_per_epoch": seq_ms / E, "batched_ms_per_epoch": bat_ms / E,
             "speedup_batched": seq_ms / bat_ms, "gvoxel_views_per_s_batched": 2 * vox_views / (bat_ms / E / 1e3) / 1e9,
-            "note": "batched time by host clock around synchronized epoch calls; sequential by CUDA events"}
-    print(json.dumps(line), flush=True)
+            "note": "batched time by host clock around synchronized epoch calls; sequential by CUDA events; each "
+                    "specimen's BF16 result against an FP32 run of the same epochs on the GPU (the FP64 oracle "
+                    "comparison of batched BF16 sessions is in the GPU tests, at sizes the oracle finishes)"}
     for sp in specs:
         sp["ctx"].close()
+    torch.cuda.synchronize()
+    torch.cuda.set_stream(torch.cuda.default_stream())
+    return line
+
+
+C2 = dict(N=256, Nd=384, V=360, n_ell=20, seed=2, photons=1e5, mu_per_mm=0.002, epochs=50, batch=5, lam=0.005)
+
+
+def ellipsoids_dev(N, n_ell, seed):
+    """Additive random ellipsoids on the device (the generator of
+    tests/scans.ellipsoid_phantom: centres and semi-axes uniform within 0.8 of
+    the half field of view, random orientation, values U[0.1, 1.0]); z-major."""
+    import torch
+    rng = np.random.default_rng(seed)
+    c = torch.arange(N, device="cuda", dtype=torch.float32) - (N - 1) / 2.0
+    vol = torch.zeros((N, N, N), device="cuda")
+    half = 0.8 * N / 2.0
+    for _ in range(n_ell):
+        ctr = rng.uniform(-half, half, 3) * 0.5
+        ax = rng.uniform(0.1, 1.0, 3) * half * 0.5
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        a, b, cc, d = q
+        R = np.array([[a * a + b * b - cc * cc - d * d, 2 * (b * cc - a * d), 2 * (b * d + a * cc)],
+                      [2 * (b * cc + a * d), a * a - b * b + cc * cc - d * d, 2 * (cc * d - a * b)],
+                      [2 * (b * d - a * cc), 2 * (cc * d + a * b), a * a - b * b - cc * cc + d * d]])
+        val = rng.uniform(0.1, 1.0)
+        Rt = torch.tensor(R / ax[None, :], device="cuda", dtype=torch.float32)   # columns scaled by 1/axes
+        for z in range(N):
+            zz = c[z] - ctr[2]
+            yy = (c - ctr[1])[:, None]
+            xx = (c - ctr[0])[None, :]
+            u = [xx * Rt[0, i] + yy * Rt[1, i] + zz * Rt[2, i] for i in range(3)]
+            inside = (u[0] ** 2 + u[1] ** 2 + u[2] ** 2) <= 1.0
+            vol[z] += inside.float() * val
+    return vol
+
+
+def run_c2(args, local):
+    """Plain cone-beam FDK + OS-ART (the reference's FDK::reconstruct then
+    IR::reconstruct with Method::ART, reconstruct.cu:1651-1724, :23-156):
+    256^3 volume of 20 seeded ellipsoids, 360 views over 360 degrees, 384^2
+    detector, SOD 500 / SDD 1000 mm, 1 mm voxels.  Noisy data: the phantom's
+    values are attenuation in units of 0.002 / mm (value 1 = 0.2 / cm), counts
+    I ~ Poisson(1e5 exp(-b)) per ray, b = -ln(max(I, 1) / 1e5).  FDK with the
+    Ram-Lak filter; its volume, moved from the FDK frame (source at -sod,
+    centred grid) to the iterative one (+1 voxel on each axis) and scaled by
+    the least-squares factor <A f, b> / <A f, A f>, starts 50 OS-ART epochs (5
+    subsets, lambda 0.005: the step the ray length of 256 voxels allows).
+    Device times by CUDA events (the library's per-class timers)."""
+    import torch
+    xr = load_pkg()
+    P = C2
+    N, Nd, V = P["N"], P["Nd"], P["V"]
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx = xr.Context.create(W["sdd"], W["sod"], W["det"], N, Nd, V, np.eye(3, dtype=np.float32).reshape(1, 9),
+                            device=local)
+    ctx.set_stream(stream.cuda_stream)
+    mu = ellipsoids_dev(N, P["n_ell"], P["seed"]).contiguous()
+    b = torch.empty((1, V, Nd, Nd), dtype=torch.float32, device="cuda")
+    ctx.dev_forward(mu.data_ptr(), b.data_ptr(), False)
+    g = torch.Generator(device="cuda").manual_seed(P["seed"])
+    counts = torch.poisson(P["photons"] * torch.exp(-b * P["mu_per_mm"]), generator=g)
+    bn = (-torch.log(counts.clamp_min(1.0) / P["photons"]) / P["mu_per_mm"]).contiguous()
+    torch.cuda.synchronize()
+    noise_rel = float(torch.linalg.vector_norm(bn - b) / torch.linalg.vector_norm(b))
+    # FDK on host buffers (the reference's call surface), device time by its timer
+    ctx.set_option(xr.Option.TIMING, 1)
+    ctx.reset_timings()
+    t0 = time.perf_counter()
+    f_vol, _ = ctx.fdk_reconstruct(bn.cpu().numpy(), xr.Rotate.CW, xr.Filter.RAMLAK)
+    fdk_wall = time.perf_counter() - t0
+    fdk_ms = ctx.timings()["fdk"][0]
+    f = torch.from_numpy(f_vol[0]).cuda().roll(shifts=(1, 1, 1), dims=(0, 1, 2)).contiguous()
+    af = torch.empty_like(b)
+    ctx.dev_forward(f.data_ptr(), af.data_ptr(), False)
+    torch.cuda.synchronize()
+    scale = float((af.double() * bn.double()).sum() / (af.double() * af.double()).sum())
+    vol = (f * scale).contiguous()
+    r_fdk, _ = ctx.dev_residual(vol.data_ptr(), bn.data_ptr(), False)
+    err_fdk = float(torch.linalg.vector_norm(vol - mu) / torch.linalg.vector_norm(mu))
+    ctx.reset_timings()
+    ctx.dev_session_begin(bn.data_ptr(), vol.data_ptr(), False, P["epochs"], P["batch"], method=xr.Method.ART,
+                          lam=P["lam"])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(P["epochs"]):
+        ctx.dev_session_epoch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    art_ms = e0.elapsed_time(e1)
+    tim = ctx.timings()
+    ctx.dev_session_end(0, 0)
+    ctx.set_option(xr.Option.TIMING, 0)
+    r_art, _ = ctx.dev_residual(vol.data_ptr(), bn.data_ptr(), False)
+    r_clean, _ = ctx.dev_residual(vol.data_ptr(), b.data_ptr(), False)
+    err_art = float(torch.linalg.vector_norm(vol - mu) / torch.linalg.vector_norm(mu))
+    bv = bytes_view(1, N, Nd)
+    fwd_ms, back_ms = tim["forward"][0] / P["epochs"], tim["back"][0] / P["epochs"]
+    line = {"workload": f"plain cone-beam {N}^3, {V} views over 360 deg, {Nd}^2 detector, {P['n_ell']} ellipsoids, "
+            f"Poisson {P['photons']:.0e} photons; FDK (Ram-Lak) + {P['epochs']} OS-ART epochs ({P['batch']} subsets, "
+            f"lambda {P['lam']})", "noise_rel_l2": noise_rel,
+            "fdk_ms": fdk_ms, "fdk_host_call_s": fdk_wall, "fdk_scale_to_iterative_units": scale,
+            "residual_rel_l2_noisy_after_fdk": r_fdk, "residual_rel_l2_noisy_after_art": r_art,
+            "residual_rel_l2_clean_after_art": r_clean, "volume_rel_error_after_fdk": err_fdk,
+            "volume_rel_error_after_art": err_art, "art_ms_per_epoch": art_ms / P["epochs"],
+            "forward_ms_per_epoch": fwd_ms, "back_ms_per_epoch": back_ms,
+            "forward_effective_gbs": V * bv / (fwd_ms * 1e-3) / 1e9,
+            "back_effective_gbs": V * bv / (back_ms * 1e-3) / 1e9,
+            "forward_compulsory_hbm_frac": (5 * N ** 3 * 4 + V * Nd * Nd * 4) / (fwd_ms * 1e-3) / 1e9 /
+            measured_peaks()[0],
+            "back_compulsory_hbm_frac": (5 * 2 * N ** 3 * 4 + V * Nd * Nd * 4) / (back_ms * 1e-3) / 1e9 /
+            measured_peaks()[0],
+            "note": "effective GB/s charge bytes_view = N^3*4 + Nd^2*4 per view; compulsory = per subset launch the "
+                    "volume read (and written by the back) once plus its views' images"}
+    ctx.close()
+    del mu, b, bn, counts, vol, f, af
+    torch.cuda.empty_cache()
+    return line
 
 
 def run_fiber(args, local):
@@ -582,6 +728,8 @@ def main():
     ap.add_argument("--arms", default="plain_f32,learned_bf16", help="--ttr arms (also plain_bf16, learned_f32)")
     ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-residual comparison of the default run")
     ap.add_argument("--c4", action="store_true", help="uneven batch of 8 specimens (BF16), batched vs sequential")
+    ap.add_argument("--c2", action="store_true", help="plain cone-beam FDK + 50 OS-ART epochs at 256^3, 360 views")
+    ap.add_argument("--no-configs", action="store_true", help="skip the FDK+ART and uneven-batch lines of the default run")
     ap.add_argument("--fiber", action="store_true", help="fiber-model forward and epoch timing (128^3 x 4)")
     ap.add_argument("--conv", type=int, default=0, metavar="N",
                     help="only the warm-start network's tensor-core roofline on an N^3 x 13 volume")
@@ -608,14 +756,16 @@ def main():
             torch.cuda.set_stream(torch.cuda.Stream())
             print(json.dumps(conv_roofline(local, args.conv)), flush=True)
         return
-    if args.ttr or args.c4 or args.fiber:
+    if args.ttr or args.c4 or args.fiber or args.c2:
         if rank == 0:          # one GPU: these comparisons run on rank 0 only
             if args.ttr:
                 print(json.dumps(run_ttr(args, local)), flush=True)
             elif args.fiber:
                 print(json.dumps(run_fiber(args, local)), flush=True)
+            elif args.c2:
+                print(json.dumps(run_c2(args, local)), flush=True)
             else:
-                run_c4(args, local)
+                print(json.dumps(run_c4(args, local)), flush=True)
         return
     if world > 1:
         rp.init("nccl")
@@ -664,9 +814,11 @@ def main():
     rel, _ = ctx.dev_residual(d_vol.data_ptr(), d_b.data_ptr(), True)   # ||A mu - b|| / ||b|| after the epochs
     ctx.dev_session_end(0, 0)
 
-    def epoch_ms(storage, graphs, steps):
+    def epoch_ms(storage, graphs, steps, split=None):
         """Mean epoch time of a fresh session (same inputs) with the given
-        storage type and graph replay; warm-up epochs untimed."""
+        storage type and graph replay; warm-up epochs untimed.  split: a dict
+        that receives the per-class device times per epoch (direct epochs
+        only: timing events are not recorded inside graphs)."""
         ctx.set_option(xr.Option.STORAGE, storage)
         ctx.set_option(xr.Option.GRAPHS, graphs)
         dt = {0: torch.float32, 1: torch.bfloat16, 2: torch.float16}[storage]
@@ -683,14 +835,23 @@ def main():
             ctx.dev_session_epoch()
         a1.record(stream)
         torch.cuda.synchronize()
+        ms = a0.elapsed_time(a1) / steps
+        if split is not None:
+            ctx.set_option(xr.Option.TIMING, 1)
+            ctx.reset_timings()
+            ctx.dev_session_epoch()
+            torch.cuda.synchronize()
+            split.update({k: v[0] for k, v in ctx.timings().items() if v[1]})
+            ctx.set_option(xr.Option.TIMING, 0)
         ctx.dev_session_end(0, 0)
         ctx.set_option(xr.Option.GRAPHS, 0)
         ctx.set_option(xr.Option.STORAGE, 0)
         del db, dv
-        return a0.elapsed_time(a1) / steps
+        return ms
 
-    variants = {"f32_graphs": epoch_ms(0, 1, args.steps), "bf16": epoch_ms(1, 0, args.steps),
-                "bf16_graphs": epoch_ms(1, 1, args.steps)}
+    bf16_split = {}
+    variants = {"f32_graphs": epoch_ms(0, 1, args.steps), "bf16": epoch_ms(1, 0, args.steps, bf16_split),
+                "bf16_graphs": epoch_ms(1, 1, args.steps), "bf16_kernel_ms": bf16_split}
 
     bv = bytes_view(K, N, Nd)
     per_gpu_bytes = 2 * C * V * bv
@@ -711,14 +872,29 @@ def main():
         dom, dom_ms, dom_n, units = "k_back_col<1,float>", back_ms, back_n, C * subset
     peak, peak_kind = measured_peaks()
     avg_launch_s = dom_ms / max(dom_n, 1) / 1e3
-    achieved = units * bv / avg_launch_s / 1e9
-    traffic = profile_traffic(dom)
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": dom, "peak_kind": peak_kind,
-                "avg_launch_ms": avg_launch_s * 1e3, "units_per_launch": units,
-                "bytes_per_unit": bv,
-                "note": "effective: one launch reads the volume once for all its views; traffic = ncu DRAM "
-                        "bytes per launch"}
+    # compulsory DRAM bytes of one launch: the forward reads the volume once and
+    # writes its views' detector images; the back reads the volume, the
+    # per-subset sensitivity and the ratio images and writes the volume
+    if dom.startswith("k_fwd"):
+        # channels whose grating weight (S_k . G)^2 is zero for an axis are not read
+        grat = rot[:, :, 2]                                  # G = elemR e_z per axis
+        active = float(np.mean([(np.abs(s_basis @ gv) > 1e-6).sum() for gv in grat]))
+        compulsory = active * N ** 3 * 4 + units * Nd * Nd * 4
+    else:
+        compulsory = 3 * K * N ** 3 * 4 + units * Nd * Nd * 4
+    hbm = {"bound": "hbm", "kernel": dom, "achieved": compulsory / avg_launch_s / 1e9, "peak": peak, "unit": "GB/s",
+           "frac": compulsory / avg_launch_s / 1e9 / peak, "peak_kind": peak_kind, "bytes_per_launch": compulsory,
+           "note": "compulsory bytes of one launch (each operand moved once) over its CUDA-event time"}
+    effective = {"kernel": dom, "gbs": units * bv / avg_launch_s / 1e9, "bytes_per_unit": bv, "units_per_launch": units,
+                 "note": "bytes_view = K*N^3*4 + Nd^2*4 charged per view: one volume read serves every view of the "
+                         "launch, so this exceeds the HBM peak and is not a roofline fraction"}
+    sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    roofline = issue_roofline(dom, avg_launch_s, float(N) ** 3 * units, float(N) ** 3, float(Nd * Nd) * units,
+                              sm_mhz, peak)
+    if roofline is None:           # no captured instruction counts: the HBM view alone
+        roofline = dict(hbm, traffic=None)
+    roofline.update({"avg_launch_ms": avg_launch_s * 1e3, "units_per_launch": units, "peak_kind": "sampled SM clock"
+                     if roofline["bound"] == "issue" else peak_kind})
     # kernels in the timed region: per subset n_groups forward launches, one
     # ratio launch, one back launch
     launches = int(fwd_n * n_groups + tim["ratio"][1] + back_n)
@@ -798,6 +974,10 @@ def main():
     conv = None
     if world == 1 and args.size == "full":
         conv = conv_roofline(local)
+    c2 = c4 = None
+    if world == 1 and args.size == "full" and not args.no_configs:
+        c2 = run_c2(args, local)
+        c4 = run_c4(args, local)
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -805,9 +985,11 @@ def main():
                        "subsets": W["batch"], "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (volume 872 MB, sinograms 318 MB)",
                        "residual_rel_l2_after": rel},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+            "e2e": e2e, "roofline": roofline, "roofline_hbm": hbm, "effective_projector": effective,
+            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in tim.items() if v[1]},
-            "variants_ms_per_step": variants, "time_to_residual": ttr, "roofline_conv": conv}
+            "variants_ms_per_step": variants, "time_to_residual": ttr, "roofline_conv": conv,
+            "fdk_art_256": c2, "uneven_batch_bf16": c4}
     print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

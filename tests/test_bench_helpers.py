@@ -39,3 +39,24 @@ def test_angle_stats_unsigned_and_masked():
     md_a[:, 1] = 0.0                                # empty voxels are left out
     assert b.angle_stats(md_a, md_b, mask)["voxels"] == (N - 2) * N * N
     assert b.angle_stats(md_a, md_b, torch.zeros(N, N, N, dtype=torch.bool)) == {"voxels": 0}
+
+
+def test_issue_roofline_scales_the_captured_counts():
+    """The bench's roofline of a projector kernel: the captured warp
+    instructions per voxel-view times this launch's voxel-views, over the
+    launch time, against 148 SMs x 4 schedulers x the SM clock; traffic scaled
+    by the unit the capture names for reads and writes."""
+    bench = _bench()
+    figs = bench.profile_figures()
+    assert figs is not None and "k_fwd_col<1,g,float>" in figs["kernels"]
+    k = figs["kernels"]["k_fwd_col<1,g,float>"]
+    per_vv = k["warp_inst_per_launch"] / k["voxel_views_per_launch"]
+    r = bench.issue_roofline("k_fwd_col<1,g,float>", 2e-3, 1e9, 2e7, 1e6, 1965.0, 6452.2)
+    assert r["bound"] == "issue"
+    assert abs(r["achieved"] - per_vv * 1e9 / 2e-3 / 1e9) < 1e-6 * r["achieved"]
+    assert abs(r["peak"] - 148 * 4 * 1965e6 / 1e9) < 1e-9
+    exp_traffic = (k["dram_read_bytes_per_launch"] * 2e7 / k["voxels_per_launch"] +
+                   k["dram_write_bytes_per_launch"] * 1e6 / k["pixel_views_per_launch"])
+    assert abs(r["traffic"] - exp_traffic) < 1e-6 * exp_traffic
+    assert 0 < r["frac"] == r["achieved"] / r["peak"]
+    assert bench.issue_roofline("no_such_kernel", 1e-3, 1.0, 1.0, 1.0, 1965.0, 6452.2) is None
