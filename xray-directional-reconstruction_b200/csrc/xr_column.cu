@@ -126,6 +126,7 @@ struct FwdColArgs {
     const float *coef;        /* mode 3: per-voxel rotation planes           */
     int coef_kind;            /* 0: (phi, cos theta); 1: main direction      */
     int nbg, nba;             /* bricks along g and a                        */
+    int zlo, zhi;             /* only bricks whose first z lies in [zlo, zhi) */
 };
 
 template <int MODE, int G, typename T>
@@ -151,6 +152,10 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
     const int brick = blockIdx.x;
     const int g0 = (brick % a.nbg) * 16, a0 = ((brick / a.nbg) % a.nba) * 16, b0 = (brick / (a.nbg * a.nba)) * 8;
     const int g1 = min(g0 + 16, N) - 1, a1 = min(a0 + 16, N) - 1, b1 = min(b0 + 8, N) - 1;
+    {   /* z of the brick's first voxel: g for column axis z, b otherwise */
+        const int z0 = (G == 2) ? g0 : b0;
+        if (z0 < a.zlo || z0 >= a.zhi) return;
+    }
 
     const int tid = threadIdx.x;
     for (int i = tid; i < 4 * kTileCap; i += kFwdThreads) smem[i] = 0;
@@ -755,10 +760,12 @@ cudaError_t check_exact_rdet(float det, float rdet, unsigned *d_flag, unsigned *
 cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, const int *d_conds, int n_cond, int G,
                                const float *d_magsig, const void *vol, float *out, int mode, int views_per_cta,
-                               int storage, cudaStream_t s, const float *coef, int coef_kind) {
+                               int storage, cudaStream_t s, const float *coef, int coef_kind, int zlo, int zhi) {
     if (n_views <= 0 || n_cond <= 0) return cudaSuccess;
     if (coef && mode == 1) mode = 3;
     FwdColArgs a;
+    a.zlo = zlo;
+    a.zhi = zhi;
     a.coef_kind = coef_kind;
     a.g = g;
     a.frames = frames;

@@ -288,7 +288,7 @@ static const ColInfo *dcol(xr_ctx *c) { return (const ColInfo *)c->colinfo.p; }
  * vol is the channel base (plain: the axis's own volume when one axis). */
 static cudaError_t forward_dispatch(xr_ctx *c, const int *vl, int n_views, const std::vector<int> &conds,
                                     const void *vol, float *out, int mode, int storage,
-                                    const float *coef = nullptr, int coef_kind = 0) {
+                                    const float *coef = nullptr, int coef_kind = 0, int zlo = 0, int zhi = 1 << 30) {
     const ViewFrame *fr = (const ViewFrame *)c->frames.p;
     const ColInfo *ci = dcol(c);
     std::vector<int> grp[3];
@@ -314,14 +314,15 @@ static cudaError_t forward_dispatch(xr_ctx *c, const int *vl, int n_views, const
                 for (int cond : grp[g]) {
                     cudaError_t e = launch_forward_col(c->gc, dbasis(c), fr, vl, n_views, &ci->all[cond], 1, g,
                                                        ci->magsig, vol, out, mode, c->views_per_cta, storage,
-                                                       c->stream, coef, coef_kind);
+                                                       c->stream, coef, coef_kind, zlo, zhi);
                     if (e != cudaSuccess) return e;
                 }
                 continue;
             }
         }
         cudaError_t e = launch_forward_col(c->gc, dbasis(c), fr, vl, n_views, dl, (int)grp[g].size(), g, ci->magsig,
-                                           vol, out, mode, c->views_per_cta, storage, c->stream, coef, coef_kind);
+                                           vol, out, mode, c->views_per_cta, storage, c->stream, coef, coef_kind, zlo,
+                                           zhi);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -475,11 +476,28 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
             const int *vl = (const int *)c->subsets.p + (size_t)orders[b] * s.subset_size;
             {
                 Timed t(c, XR_T_FORWARD);
-                const cudaError_t e =
-                    s.fiber ? launch_fiber_forward(c->gc, fr, vl, s.subset_size, c->C, (const float *)s.d_vol, proj,
-                                                   str)
-                            : forward_dispatch(c, vl, s.subset_size, all_conds(c), s.d_vol, proj, 1, s.storage, s.coef,
-                                               s.coef_kind);
+                cudaError_t e = cudaSuccess;
+                if (s.vol_slabs > 0 && !s.fiber) {
+                    /* the volume arrives by z-slabs: each slab's bricks start as
+                     * soon as its upload event has fired (column axes), the
+                     * general kernels after the last slab */
+                    const int S = s.vol_slabs, zs = ((c->N + S - 1) / S + 15) / 16 * 16;
+                    for (int i = 0; i < S && e == cudaSuccess; i++) {
+                        e = cudaStreamWaitEvent(str, s.slab_ev[i], 0);
+                        if (e == cudaSuccess && c->all_aligned)
+                            e = forward_dispatch(c, vl, s.subset_size, all_conds(c), s.d_vol, proj, 1, s.storage,
+                                                 s.coef, s.coef_kind, i * zs, i == S - 1 ? (1 << 30) : (i + 1) * zs);
+                    }
+                    if (e == cudaSuccess && !c->all_aligned)
+                        e = forward_dispatch(c, vl, s.subset_size, all_conds(c), s.d_vol, proj, 1, s.storage, s.coef,
+                                             s.coef_kind);
+                    s.vol_slabs = 0;
+                } else {
+                    e = s.fiber ? launch_fiber_forward(c->gc, fr, vl, s.subset_size, c->C, (const float *)s.d_vol, proj,
+                                                       str)
+                                : forward_dispatch(c, vl, s.subset_size, all_conds(c), s.d_vol, proj, 1, s.storage,
+                                                   s.coef, s.coef_kind);
+                }
                 if ((st = cuda_check(c, e, s.fiber ? "fiber forward" : "XTT forward"))) return st;
             }
             {
@@ -487,7 +505,8 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                 if (s.sino_ready) {
                     if ((st = cuda_check(c, cudaStreamWaitEvent(str, s.sino_ready, 0), "cudaStreamWaitEvent")))
                         return st;
-                    s.sino_ready = nullptr;
+                    s.sino_ready = s.sino_rest;   /* the next subset's ratio waits for the rest */
+                    s.sino_rest = nullptr;
                 }
                 /* the (phi, cos theta) forward is not chord-normalised (forwardOrth ->
                  * projRatio, reconstruct.cu:1086-1099); the main-direction one is
@@ -782,6 +801,8 @@ void xr_destroy(xr_ctx *c) {
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (cudaEvent_t e : c->copy_ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->slab_ev)
+        if (e) cudaEventDestroy(e);
     delete c;
 }
 
@@ -931,10 +952,14 @@ static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, 
             std::copy(o.begin(), o.end(), s.ir_orders.begin() + r * batch);
         }
     }
-    if (s.xtt && !s.fiber && c->all_aligned && !s.art) {
+    if (s.xtt && !s.fiber && c->all_aligned && !s.art &&
+        !(coef == nullptr && c->sens_batch == batch && c->sens_rotation == rotation)) {
         /* factor_k of every subset (geometry only): sum over the subset's views
-         * of (|B x S_k| |S_k . G|)^2 (ir.cu:1847), once per session. */
+         * of (|B x S_k| |S_k . G|)^2 (ir.cu:1847), once per session, and kept
+         * on the context for the next session of the same subsets and
+         * rotation (the rotated-basis variants depend on their planes: not kept). */
         const size_t N3 = (size_t)c->N * c->N * c->N;
+        c->sens_batch = 0;
         if ((st = ensure(c, c->sens, (size_t)batch * c->K * N3 * sizeof(float), "sensitivity"))) return st;
         const ColInfo *ci = dcol(c);
         for (int sub = 0; sub < batch; sub++) {
@@ -946,6 +971,10 @@ static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, 
                                                coef, coef_kind),
                             "sensitivity");
             if (st) return st;
+        }
+        if (!coef) {
+            c->sens_batch = batch;
+            c->sens_rotation = rotation;
         }
     }
     st = cuda_check(c, cudaStreamSynchronize(c->stream), "session begin");
@@ -1348,6 +1377,9 @@ static xr_status ensure_copy_stream(xr_ctx *c) {
     for (cudaEvent_t &e : c->copy_ev)
         if (!e && (st = cuda_check(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")))
             return st;
+    for (cudaEvent_t &e : c->slab_ev)
+        if (!e && (st = cuda_check(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")))
+            return st;
     return XR_OK;
 }
 
@@ -1429,19 +1461,82 @@ xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
         ~CopyWait() { cudaStreamSynchronize(s); }
     } copy_wait{cs};
     if ((st = stream_after(c, cs, c->stream, c->copy_ev[0]))) return st;   /* earlier work on the buffers */
-    if ((st = upload_planes_s_on(c, c->scratch_vol, voxel, c->K, N3, c->storage, "volume", cs))) return st;
-    if ((st = cuda_check(c, cudaEventRecord(c->copy_ev[1], cs), "cudaEventRecord"))) return st;
-    if ((st = upload_planes_s_on(c, c->scratch_sino, sino, c->C, blk, sino_st(c), "sinogram", cs))) return st;
-    if ((st = cuda_check(c, cudaEventRecord(c->copy_ev[2], cs), "cudaEventRecord"))) return st;
+    /* FP32 storage, direct epochs: the uploads are staged so the first
+     * subset's work overlaps them (below); else volume, then sinogram */
+    const bool staged = c->storage == 0 && sino_st(c) == 0 && !c->use_graphs && epoch > 0;
+    if (!staged) {
+        if ((st = upload_planes_s_on(c, c->scratch_vol, voxel, c->K, N3, c->storage, "volume", cs))) return st;
+        if ((st = cuda_check(c, cudaEventRecord(c->copy_ev[1], cs), "cudaEventRecord"))) return st;
+        if ((st = upload_planes_s_on(c, c->scratch_sino, sino, c->C, blk, sino_st(c), "sinogram", cs))) return st;
+        if ((st = cuda_check(c, cudaEventRecord(c->copy_ev[2], cs), "cudaEventRecord"))) return st;
+    } else {
+        for (int i = 0; i < c->K; i++)
+            if (!voxel[i]) return fail(c, XR_ERR_ARG, "null host pointer: volume");
+        for (int i = 0; i < c->C; i++)
+            if (!sino[i]) return fail(c, XR_ERR_ARG, "null host pointer: sinogram");
+        if ((st = ensure(c, c->scratch_vol, (size_t)c->K * N3 * sizeof(float), "volume"))) return st;
+        if ((st = ensure(c, c->scratch_sino, (size_t)c->C * blk * sizeof(float), "sinogram"))) return st;
+    }
     if ((st = xr_dev_session_begin(c, c->scratch_sino.p, c->scratch_vol.p, 1, epoch, batch, dir, method, lambda)))
         return st;
-    /* the first subset's forward needs only the volume; its ratio waits for
-     * the sinogram (inside a captured epoch graph the wait comes first) */
-    st = cuda_check(c, cudaStreamWaitEvent(c->stream, c->copy_ev[1], 0), "cudaStreamWaitEvent");
-    if (!st && (c->use_graphs || epoch == 0))
-        st = cuda_check(c, cudaStreamWaitEvent(c->stream, c->copy_ev[2], 0), "cudaStreamWaitEvent");
-    else if (!st)
-        c->sess.sino_ready = c->copy_ev[2];
+    if (!staged) {
+        /* the first subset's forward needs only the volume; its ratio waits for
+         * the sinogram (inside a captured epoch graph the wait comes first) */
+        st = cuda_check(c, cudaStreamWaitEvent(c->stream, c->copy_ev[1], 0), "cudaStreamWaitEvent");
+        if (!st && (c->use_graphs || epoch == 0))
+            st = cuda_check(c, cudaStreamWaitEvent(c->stream, c->copy_ev[2], 0), "cudaStreamWaitEvent");
+        else if (!st)
+            c->sess.sino_ready = c->copy_ev[2];
+    } else {
+        /* Order on the copy stream: the first subset's views of the sinogram,
+         * the volume in z-slabs (the first forward starts on each slab as it
+         * lands), then the rest of the sinogram (waited for by the second
+         * subset's ratio).  The first epoch's subset order is the one its
+         * epoch call will draw: the persistent order shuffled by a fresh
+         * default engine (reconstruct.cu:858-859). */
+        std::vector<int> o = c->sess.order;
+        {
+            std::mt19937_64 eng;
+            std::shuffle(o.begin(), o.end(), eng);
+        }
+        const size_t NdNd = (size_t)c->Nd * c->Nd, NN = (size_t)c->N * c->N;
+        std::vector<char> first(c->V, 0);
+        for (int j = 0; j < c->sess.subset_size; j++) first[((long)o[0] + (long)batch * j) % c->V] = 1;
+        float *dsino = (float *)c->scratch_sino.p, *dvol = (float *)c->scratch_vol.p;
+        auto copy_views = [&](char want) -> xr_status {
+            for (int cond = 0; cond < c->C; cond++)
+                for (int v0 = 0; v0 < c->V;) {
+                    if (first[v0] != want) { v0++; continue; }
+                    int v1 = v0;
+                    while (v1 < c->V && first[v1] == want) v1++;
+                    xr_status e2 = cuda_check(c, cudaMemcpyAsync(dsino + cond * blk + v0 * NdNd, sino[cond] + v0 * NdNd,
+                                                                 (size_t)(v1 - v0) * NdNd * sizeof(float),
+                                                                 cudaMemcpyHostToDevice, cs), "sinogram");
+                    if (e2) return e2;
+                    v0 = v1;
+                }
+            return XR_OK;
+        };
+        st = copy_views(1);
+        if (!st) st = cuda_check(c, cudaEventRecord(c->copy_ev[2], cs), "cudaEventRecord");
+        const int S = xr_ctx::kSlabs, zs = ((c->N + S - 1) / S + 15) / 16 * 16;
+        for (int i = 0; i < S && !st; i++) {
+            const int z0 = std::min(c->N, i * zs), z1 = (i == S - 1) ? c->N : std::min(c->N, (i + 1) * zs);
+            for (int k = 0; k < c->K && !st && z1 > z0; k++)
+                st = cuda_check(c, cudaMemcpyAsync(dvol + k * N3 + z0 * NN, voxel[k] + z0 * NN,
+                                                   (size_t)(z1 - z0) * NN * sizeof(float), cudaMemcpyHostToDevice, cs),
+                                "volume");
+            if (!st) st = cuda_check(c, cudaEventRecord(c->slab_ev[i], cs), "cudaEventRecord");
+        }
+        if (!st) st = copy_views(0);
+        if (!st) st = cuda_check(c, cudaEventRecord(c->copy_ev[1], cs), "cudaEventRecord");
+        if (!st) {
+            c->sess.sino_ready = c->copy_ev[2];
+            c->sess.sino_rest = c->copy_ev[1];
+            c->sess.vol_slabs = S;
+            c->sess.slab_ev = c->slab_ev;
+        }
+    }
     if (st) {
         xr_dev_session_end(c, nullptr, nullptr);
         return st;

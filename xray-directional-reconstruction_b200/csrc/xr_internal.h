@@ -96,6 +96,9 @@ struct Session {
     int coef_kind = 0;                /* 0: (phi, cos theta); 1: main direction (3 planes) */
     bool fiber = false;               /* fiber model: fiber projectors, channel 0 updated   */
     cudaEvent_t sino_ready = nullptr; /* set: the first ratio launch waits for it (sinogram upload) */
+    cudaEvent_t sino_rest = nullptr;  /* set: the second ratio launch waits for it (rest of the sinogram) */
+    int vol_slabs = 0;                /* > 0: the first forward runs by z-slabs, each after its upload event */
+    const cudaEvent_t *slab_ev = nullptr;
     float *const *ratio_dst = nullptr; /* set: each view's final ratio image to these host planes */
     std::vector<int> order;            /* persistent subset order (XTT)     */
     std::vector<int> ir_orders;        /* C*epochs rows (IR)                */
@@ -145,6 +148,9 @@ struct xr_ctx {
     xr::DevBuf fdk_filt, fdk_weight, fdk_sf;
     bool dev_ready = false;
     double *h_loss = nullptr;          /* pinned, kLossSlots doubles                */
+    static constexpr int kSlabs = 8;   /* host-call volume upload in z-slabs */
+    cudaEvent_t slab_ev[kSlabs] = {};
+    int sens_batch = 0, sens_rotation = 0; /* the sensitivity buffer holds these subsets (0: nothing) */
     int static_rdet = -1;              /* xr_dev_forward_proj_only_static: its own
                                           result of the division check (-1: not run) */
 
@@ -203,10 +209,13 @@ cudaError_t launch_convert(long n, const void *src, int src_storage, void *dst, 
 
 /* ---- xr_column.cu: kernels for axes whose grating direction is a grid axis ---- */
 cudaError_t check_exact_rdet(float det, float rdet, unsigned *d_flag, unsigned *h_result, cudaStream_t s);
+/* zlo, zhi: only the bricks whose first voxel's z lies in [zlo, zhi) (z-slab
+ * launches over a volume that arrives slab by slab; slab bounds multiples of 16). */
 cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, const int *d_conds, int n_cond, int G,
                                const float *d_magsig, const void *vol, float *out, int mode, int views_per_cta,
-                               int storage, cudaStream_t s, const float *coef = nullptr, int coef_kind = 0);
+                               int storage, cudaStream_t s, const float *coef = nullptr, int coef_kind = 0,
+                               int zlo = 0, int zhi = 1 << 30);
 /* mode 0: plain (one axis, update in place); 1: XTT (fac_in = sensitivity);
  * 2: sensitivity of the listed views into fac_out. */
 cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
