@@ -34,7 +34,7 @@ namespace {
 constexpr int kTileCap = 64 * 64;
 constexpr int kFwdThreads = 512;               /* forward: 16 (g) x 16 x 8 brick, 4 voxels/thread */
 constexpr int kBackThreads = 128;              /* back: 8 x 8 x 8 brick, 4 voxels/thread          */
-constexpr int kFrameChunk = 128;
+constexpr int kFrameChunk = 48;                /* back: frames staged per pass (3.8 KB), 6 CTAs/SM */
 
 __device__ __forceinline__ float vox_base(int i, int N, float vs) {
     const float a = __fsub_rn(__fsub_rn(__fmul_rn(2.0f, (float)i), (float)N), 1.0f);
@@ -650,7 +650,7 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
 }
 
 template <int MODE, typename T>
-__global__ void __launch_bounds__(kBackThreads, 5) k_back_col(BackColArgs a) {
+__global__ void __launch_bounds__(kBackThreads, 6) k_back_col(BackColArgs a) {
     __shared__ ViewFrame fr[kFrameChunk];
     extern __shared__ float sacc[];   /* XTT / SENS: K x 512 per-voxel accumulators */
     const GeomConst &g = a.g;
