@@ -366,6 +366,7 @@ def run_ttr(args, local):
     import torch
     ws = load_warmstart()
     xr = load_pkg()
+    weights = args.weights or ws.WEIGHTS
     torch.cuda.set_device(local)
     scan = ws.Scan(W["N"], W["V"], device=local, n_fibers=W["n_fibers"])
     mu_true = scan.phantom(W["seed"])
@@ -386,10 +387,10 @@ def run_ttr(args, local):
         vol = torch.full((K, N, N, N), 0.01, dtype=dt, device="cuda")
         ms0, e0, r0 = 0.0, 0, None
         if learned:
-            if not os.path.exists(ws.WEIGHTS):
-                arms[name] = {"unavailable": "no trained weights at " + os.path.relpath(ws.WEIGHTS, ROOT)}
+            if not os.path.exists(weights):
+                arms[name] = {"unavailable": "no trained weights at " + os.path.relpath(weights, ROOT)}
                 return
-            net = ws.load_net(ws.WEIGHTS, local)
+            net = ws.load_net(weights, local)
             net.set_stream(scan.stream.cuda_stream)
             ms0 = ws.warm_start(scan, net, b, vol, args.early, W["batch"], storage, 0)
             e0 = args.early
@@ -429,6 +430,14 @@ def run_ttr(args, local):
         except Exception as ex:
             cross = {"error": f"{type(ex).__name__}: {ex}"}
     line["orientation_learned_bf16_vs_plain_f32"] = cross
+    line["network"] = os.path.relpath(weights, ROOT)
+    # gate: the learned arm's median orientation error within 0.25 degrees of plain FP32's
+    po = arms.get("plain_f32", {}).get("orientation_error_vs_truth", {})
+    lo = arms.get("learned_bf16", {}).get("orientation_error_vs_truth", {})
+    if "median_deg" in po and "median_deg" in lo:
+        line["orientation_gate"] = {"learned_median_deg": lo["median_deg"], "plain_median_deg": po["median_deg"],
+                                    "allowed_excess_deg": 0.25,
+                                    "pass": bool(lo["median_deg"] <= po["median_deg"] + 0.25)}
     line["orientation_note"] = ("angle between per-voxel main directions (calcEigenVector of sqrt|mu|) over the "
                                 "fiber voxels of the phantom; the truth is the orientation of the true volume")
     del md_arm, md_true
@@ -726,6 +735,7 @@ def main():
     ap.add_argument("--check-every", type=int, default=10)
     ap.add_argument("--early", type=int, default=5, help="--ttr: OS-EM epochs before the warm-start network")
     ap.add_argument("--arms", default="plain_f32,learned_bf16", help="--ttr arms (also plain_bf16, learned_f32)")
+    ap.add_argument("--weights", default="", help="--ttr: warm-start network file (default: the package's)")
     ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-residual comparison of the default run")
     ap.add_argument("--c4", action="store_true", help="uneven batch of 8 specimens (BF16), batched vs sequential")
     ap.add_argument("--c2", action="store_true", help="plain cone-beam FDK + 50 OS-ART epochs at 256^3, 360 views")
@@ -967,7 +977,8 @@ def main():
                t["speedup_learned_bf16_vs_plain_f32"], "note": "device time to the target, residual checked every "
                f"{t['check_every']} epochs outside the timed work; same data b = A mu_true (held-out phantom)",
                "orientation_learned_bf16_vs_plain_f32": t["orientation_learned_bf16_vs_plain_f32"],
-               "orientation_note": t["orientation_note"]}
+               "orientation_note": t["orientation_note"], "orientation_gate": t.get("orientation_gate"),
+               "network": t.get("network")}
         for k, a in t["arms"].items():
             ttr[k] = {x: a.get(x) for x in ("seconds", "epochs", "reached", "residual_final", "storage",
                                             "orientation_error_vs_truth", "unavailable") if x in a}

@@ -9,12 +9,18 @@ Pairs: a seeded fiber phantom mu_true (12 cylinders, radius U[2,5] voxels,
 direction uniform on the sphere, eta_k = |S_k x f|^2 inside), its noiseless
 XTT projections b = A mu_true, and the output of the reference-style
 XTT::reconstruct after `early_epochs` OS-EM epochs from a constant start
-(the voxelSqrt of the iterate).  The training target is mu_true itself: for
-noiseless, consistent data it is the fixed point the plain iteration
-converges to.  The network learns early iterate -> mu_true on random cubic
-crops.
+(the voxelSqrt of the iterate).  The training target is, by choice:
+  converged  the method's own converged reconstruction: plain FP32 OS-EM
+             from the same constant start run until the relative data
+             residual reaches `target_residual` (the iterate, no voxelSqrt).
+             The 13 channels are not all determined by 3 axes x V views, so
+             plain OS-EM converges to one particular solution of A mu = b;
+             this is the one a warm start should lead it to.
+  truth      mu_true itself (the phantom; a solution of A mu = b, though not
+             the one the iteration reaches from a constant start).
+The network learns early iterate -> target on random cubic crops.
 
-    python xray-directional-reconstruction_b200/warmstart.py train --out W.bin
+    python xray-directional-reconstruction_b200/warmstart.py train --target converged --depths 4 --out W.bin
 """
 from __future__ import annotations
 
@@ -187,11 +193,15 @@ class Scan:
 
 
 def make_pool(scan: Scan, seeds, crops_per: int, crop: int, early_epochs: int = 5, batch: int = 5,
-              mu0: float = 0.01, rng_seed: int = 0, storage: int = 0):
-    """Random crops of (early iterate, mu_true) pairs, stacked on the device:
+              mu0: float = 0.01, rng_seed: int = 0, storage: int = 0, target: str = "truth",
+              target_residual: float = 1e-3, max_epochs: int = 2000, check_every: int = 10, log=None):
+    """Random crops of (early iterate, target) pairs, stacked on the device:
     two (P, K, crop, crop, crop) FP32 tensors.  The early iterate runs with
-    volumes of the given storage type (FP32 data)."""
+    volumes of the given storage type (FP32 data); target "truth" is mu_true,
+    "converged" plain FP32 OS-EM from mu0 to `target_residual`."""
     import torch
+    if target not in ("truth", "converged"):
+        raise ValueError("target must be 'truth' or 'converged'")
     rng = np.random.default_rng(rng_seed)
     xs, ts = [], []
     N = scan.N
@@ -201,6 +211,14 @@ def make_pool(scan: Scan, seeds, crops_per: int, crop: int, early_epochs: int = 
         b = scan.project(mu)
         vol = torch.full(mu.shape, mu0, dtype=dt, device="cuda")
         scan.osem(b, vol, early_epochs, batch, storage=storage, sino_storage=0)
+        if target == "converged":
+            ref = torch.full(mu.shape, mu0, dtype=torch.float32, device="cuda")
+            e, ms, trace = scan.osem(b, ref, 0, batch, residual_every=check_every, target=target_residual,
+                                     max_epochs=max_epochs, final_sqrt=False)
+            if log is not None:
+                log.append({"seed": int(s), "epochs": e, "ms": ms, "residual": trace[-1][2] if trace else None})
+            del mu
+            mu = ref
         for _ in range(crops_per):
             o = rng.integers(0, N - crop + 1, 3)
             sl = (slice(None), slice(o[0], o[0] + crop), slice(o[1], o[1] + crop), slice(o[2], o[2] + crop))
@@ -258,7 +276,9 @@ def main(argv=None):
     ap.add_argument("--crops", type=int, default=4)
     ap.add_argument("--crop", type=int, default=64)
     ap.add_argument("--early", type=int, default=5)
-    ap.add_argument("--depth", type=int, default=6)
+    ap.add_argument("--depths", default="4", help="comma-separated network depths, each trained on the same pool")
+    ap.add_argument("--target", default="converged", choices=["converged", "truth"])
+    ap.add_argument("--target-residual", type=float, default=1e-3)
     ap.add_argument("--steps", type=int, default=12000)
     ap.add_argument("--lr", type=float, default=1.5e-3)
     ap.add_argument("--storage", type=int, default=1, help="volume storage of the early iterates (1 = BF16)")
@@ -268,21 +288,28 @@ def main(argv=None):
     torch.cuda.set_device(0)
     scan = Scan(args.N)
     t0 = time.time()
+    tlog = []
     xin, tgt = make_pool(scan, range(args.seed0, args.seed0 + args.phantoms), args.crops, args.crop, args.early,
-                         storage=args.storage)
+                         storage=args.storage, target=args.target, target_residual=args.target_residual, log=tlog)
     t1 = time.time()
-    net = xr.Net(scan.K, 32, args.depth, seed=0)
-    net.set_stream(scan.stream.cuda_stream)
-    trace = train(net, xin, tgt, args.steps, args.lr)
-    torch.cuda.synchronize()
-    t2 = time.time()
-    os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
-    net.save(args.out)
+    depths = [int(d) for d in args.depths.split(",")]
+    recs = []
+    for depth in depths:
+        t2 = time.time()
+        net = xr.Net(scan.K, 32, depth, seed=0)
+        net.set_stream(scan.stream.cuda_stream)
+        trace = train(net, xin, tgt, args.steps, args.lr)
+        torch.cuda.synchronize()
+        t3 = time.time()
+        out = args.out if len(depths) == 1 else args.out.replace(".bin", f"_d{depth}.bin")
+        os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+        net.save(out)
+        net.close()
+        recs.append({"out": os.path.basename(out), "depth": depth, "train_s": t3 - t2, "loss_trace": trace})
     rec = {"pairs": int(xin.shape[0]), "phantoms": args.phantoms, "seeds": [args.seed0, args.seed0 + args.phantoms - 1],
-           "N": args.N, "crop": args.crop, "early_epochs": args.early, "depth": args.depth, "steps": args.steps,
-           "lr": args.lr,
-           "storage": args.storage,
-           "pool_s": t1 - t0, "train_s": t2 - t1, "loss_trace": trace}
+           "N": args.N, "crop": args.crop, "crops_per_phantom": args.crops, "early_epochs": args.early,
+           "target": args.target, "target_residual": args.target_residual, "steps": args.steps, "lr": args.lr,
+           "storage": args.storage, "pool_s": t1 - t0, "targets": tlog, "networks": recs}
     print(json.dumps(rec))
     if args.log:
         with open(args.log, "w") as f:
