@@ -666,6 +666,28 @@ def run_c2(args, local):
     return line
 
 
+def run_reference_gpu(d_b, local, epochs: int = 1):
+    """The reference's own CUDA kernels on this GPU (reconstruct/src/ir.cu
+    built for sm_100a, oracle/_ref/libxrref_gpu.so), driven like its
+    XTT::reconstruct: one launch and one device synchronize per y slab and
+    view (reconstruct.cu:857-911), on the same workload and data as the
+    timed epochs (b = A mu_true, mu = 0.01).  Times of whole epochs by CUDA
+    events inside the driver."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefGPU, Scan
+    if not RefGPU.available():
+        return {"unavailable": "oracle/_ref/libxrref_gpu.so not built (make -C oracle ref with the reference sources)"}
+    s = Scan(sdd=W["sdd"], sod=W["sod"], det=W["det"], N=W["N"], Nd=W["Nd"], V=W["V"], rot=three_axes(),
+             trans=np.zeros((3, 3)), offset=np.zeros((3, 3)), basis=basis13())
+    b = d_b.cpu().numpy()
+    v0 = np.full((s.K, s.N, s.N, s.N), 0.01, np.float32)
+    _, _, losses, ms = RefGPU().xtt_reconstruct(s, b, v0, epochs, W["batch"], want_ratio=False)
+    return {"ms_per_epoch": float(np.mean(ms)), "epochs": epochs, "loss_first_epoch": float(losses[0]),
+            "launches_per_epoch": int(2 * s.C * s.V * s.N + s.C * s.V * 2 + W["batch"] * s.N * (1 + s.K)),
+            "note": "the reference's ir.cu kernels compiled for this B200 and its per-slab launch + "
+                    "cudaDeviceSynchronize structure; FP32, same workload and data as the timed epochs"}
+
+
 def run_fiber(args, local):
     """Fiber model (fiber.cu, fiberModelReconstruct): forwardProjFiber over
     every (axis, view) pair, and OS-EM epochs (5 subsets) of forward, ratio and
@@ -740,6 +762,7 @@ def main():
     ap.add_argument("--c4", action="store_true", help="uneven batch of 8 specimens (BF16), batched vs sequential")
     ap.add_argument("--c2", action="store_true", help="plain cone-beam FDK + 50 OS-ART epochs at 256^3, 360 views")
     ap.add_argument("--no-configs", action="store_true", help="skip the FDK+ART and uneven-batch lines of the default run")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the epoch of the reference's CUDA kernels")
     ap.add_argument("--fiber", action="store_true", help="fiber-model forward and epoch timing (128^3 x 4)")
     ap.add_argument("--conv", type=int, default=0, metavar="N",
                     help="only the warm-start network's tensor-core roofline on an N^3 x 13 volume")
@@ -967,6 +990,15 @@ def main():
                "sample": f"{n_views} of {C * V} views (forward+ratio+back, all K), reference ir.cu kernels "
                          "compiled for the host, OpenMP"}
 
+    ref_gpu = None
+    if world == 1 and args.size == "full" and not args.no_ref_gpu:
+        try:
+            ref_gpu = run_reference_gpu(d_b, local)
+            if "ms_per_epoch" in ref_gpu:
+                ref_gpu["libxr_ms_per_epoch"] = t_ms
+                ref_gpu["libxr_speedup"] = ref_gpu["ms_per_epoch"] / t_ms
+        except Exception as ex:      # the reference's run is reported, it does not cost the line
+            ref_gpu = {"error": f"{type(ex).__name__}: {ex}"}
     ttr = None
     if world == 1 and not args.no_ttr and args.size == "full":
         ctx.close()
@@ -1000,7 +1032,7 @@ def main():
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in tim.items() if v[1]},
             "variants_ms_per_step": variants, "time_to_residual": ttr, "roofline_conv": conv,
-            "fdk_art_256": c2, "uneven_batch_bf16": c4}
+            "fdk_art_256": c2, "uneven_batch_bf16": c4, "reference_gpu": ref_gpu}
     print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -480,3 +480,39 @@ class RefHost:
                                           int(rotate_ccw), int(art), ctypes.c_float(lam), _p(losses))
         return (np.stack(vols).reshape(s.K, s.N, s.N, s.N), np.stack(sino).reshape(s.C, s.V, s.Nd, s.Nd),
                 losses)
+
+
+class RefGPU:
+    """The reference's own CUDA kernels (reconstruct/src/ir.cu built for the
+    B200 into oracle/_ref/libxrref_gpu.so) driven like XTT::reconstruct, one
+    launch and synchronize per y slab and view (oracle/ref_gpu)."""
+
+    def __init__(self):
+        path = os.path.join(HERE, "_ref", "libxrref_gpu.so")
+        if not os.path.exists(path):
+            build(ref=True)
+        self.lib = ctypes.CDLL(path)
+        self.lib.xr_refgpu_xtt_reconstruct.restype = ctypes.c_int
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(os.path.join(HERE, "_ref", "libxrref_gpu.so"))
+
+    def xtt_reconstruct(self, s: Scan, sino, vol, epoch, batch, rotate_ccw=0, art=False, lam=1e-2,
+                        want_ratio=True):
+        """Returns (vol after voxelSqrt (K, N, N, N), last ratio images or None,
+        losses (epoch,), milliseconds per epoch (epoch,))."""
+        sino = np.ascontiguousarray(sino, np.float32).ravel()
+        v = np.ascontiguousarray(vol, np.float32).ravel().copy()
+        ratio = np.zeros_like(sino) if want_ratio else None
+        losses = np.zeros(max(epoch, 1), np.float32)
+        ms = np.zeros(max(epoch, 1), np.float64)
+        st = self.lib.xr_refgpu_xtt_reconstruct(
+            ctypes.c_float(s.sdd), ctypes.c_float(s.sod), ctypes.c_float(s.det), s.N, s.Nd, s.V, s.C, s.K,
+            _p(s.rot), _p(s.trans), _p(s.offset), _p(s.basis), _p(sino), _p(v),
+            _p(ratio) if want_ratio else None, int(epoch), int(batch), int(rotate_ccw), int(art),
+            ctypes.c_float(lam), _p(losses), ms.ctypes.data_as(_D))
+        if st:
+            raise RuntimeError(f"reference GPU run failed: CUDA error {st}")
+        return (v.reshape(s.K, s.N, s.N, s.N), ratio.reshape(s.C, s.V, s.Nd, s.Nd) if want_ratio else None,
+                losses[:epoch], ms[:epoch])
