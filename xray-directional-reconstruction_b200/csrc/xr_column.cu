@@ -198,8 +198,12 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
 
     const int lane = tid & 31, w = tid >> 5;
     const int seg = lane & 3;
-    const int ia = a0 + (w & 3) * 4 + ((lane >> 2) & 3);
-    const int ib = b0 + (w >> 2) * 2 + (lane >> 4);
+    /* A warp's 8 columns are spread over the brick, 4 apart in a and in b:
+     * columns that project onto the same detector pixel in one atomic
+     * instruction serialise, and two columns d apart coincide in u only in
+     * views within about 1/(d B) radians of their alignment with the ray. */
+    const int ia = a0 + (w & 3) + 4 * ((lane >> 2) & 3);
+    const int ib = b0 + (w >> 2) + 4 * (lane >> 4);
     const int igb = g0 + seg * 4;
     const bool col_ok = ia < N && ib < N;
     const float ba = vox_base(ia, N, g.vs), bb = vox_base(ib, N, g.vs);
