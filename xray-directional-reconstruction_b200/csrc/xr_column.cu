@@ -432,7 +432,6 @@ struct BackColArgs {
     int sr;                   /* 16-bit volumes: stochastic rounding of updates */
     const float *coef;        /* non-null: per-voxel rotated basis (backwardOrth) */
     int coef_kind;            /* 0: (phi, cos theta); 1: main direction            */
-    int prefetch;             /* 16-bit XTT: copy the brick's volume to shared memory early */
 };
 
 /* Shared-memory slot of brick voxel lv (x + 8y + 64z) in the per-voxel
@@ -668,22 +667,6 @@ __global__ void __launch_bounds__(kBackThreads, 6) k_back_col(BackColArgs a) {
     if (MODE != B_PLAIN) {
         for (int i = tid; i < K * 512; i += kBackThreads) sacc[i] = 0.0f;
     }
-    /* 16-bit volumes: the brick's 8-voxel rows (16 bytes, half a DRAM sector;
-     * the other half is the neighbouring brick's) are copied to shared memory
-     * asynchronously now, so their latency hides behind the projections
-     * instead of stalling the update at the end */
-    T *svol = reinterpret_cast<T *>(sacc + K * 512);
-    const bool pre = MODE == B_XTT && sizeof(T) == 2 && a.prefetch && bx0 + 8 <= N && by0 + 8 <= N && bz0 + 8 <= N;
-    if (pre) {
-        for (int r = tid; r < K * 64; r += kBackThreads) {
-            const int k = r >> 6, yy = r & 7, zz = (r >> 3) & 7;
-            const T *src = reinterpret_cast<const T *>(a.vol) + (size_t)bx0 + (size_t)N * (by0 + yy) +
-                           NN * (bz0 + zz) + (size_t)k * N3;
-            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(svol + k * 512 + yy * 8 + zz * 64);
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    }
     for (int ci = 0; ci < a.n_cond; ci++) {
         const int cond = a.conds[ci];
         const int G = a.axis_g[cond];   /* uniform over the CTA */
@@ -693,10 +676,6 @@ __global__ void __launch_bounds__(kBackThreads, 6) k_back_col(BackColArgs a) {
         __syncthreads();
     }
     if (MODE == B_PLAIN) return;
-    if (pre) {
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        __syncthreads();
-    }
     /* home layout: brick-linear voxel order */
     for (int lv = tid; lv < 512; lv += kBackThreads) {
         const int x = bx0 + (lv & 7), y = by0 + ((lv >> 3) & 7), z = bz0 + (lv >> 6);
@@ -715,7 +694,7 @@ __global__ void __launch_bounds__(kBackThreads, 6) k_back_col(BackColArgs a) {
             for (int j = 0; j < 8; j++) {
                 const int k = k0 + j;
                 if (k < K) {
-                    mu[j] = pre ? ldf<T>(svol + k * 512 + lv) : ldf<T>(reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3);
+                    mu[j] = ldf<T>(reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3);
                     f[j] = a.art ? 0.f : __ldg(a.fac_in + idx + (size_t)k * N3);
                 }
             }
@@ -854,11 +833,7 @@ cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const
     a.alpha = alpha;
     const int nb8 = (g.N + 7) / 8;
     const unsigned blocks = (unsigned)((long)nb8 * nb8 * nb8);
-    /* 16-bit XTT updates prefetch the brick's volume (16-byte rows: N a
-     * multiple of 8 and a 16-byte aligned volume) */
-    a.prefetch = (mode == B_XTT && storage != kF32 && g.N % 8 == 0 && (reinterpret_cast<uintptr_t>(vol) & 15) == 0);
-    const size_t smem = (mode == B_PLAIN) ? 0
-                                          : (size_t)g.K * 512 * sizeof(float) + (a.prefetch ? (size_t)g.K * 512 * 2 : 0);
+    const size_t smem = (mode == B_PLAIN) ? 0 : (size_t)g.K * 512 * sizeof(float);
 #define XR_BACK_COL(M, TT)                                                                                        \
     do {                                                                                                          \
         cudaError_t e = cudaFuncSetAttribute(k_back_col<M, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
