@@ -174,3 +174,42 @@ def test_orth_coefficient_steps(oracle):
     got = de.cpu().numpy().ravel()
     assert np.array_equal(got[n3:], ref[n3:])
     assert np.abs(got[:n3] - ref[:n3]).max() <= 1e-6
+
+
+def test_kept_sensitivity_follows_the_session_kind(oracle):
+    """The per-subset sensitivity of a plain XTT MLEM session is kept on the
+    context for the next session of the same subsets and rotation; a
+    rotated-basis session in between computes its own into the same buffer,
+    so the next plain session must compute it again.  Plain -> orth -> plain
+    (CW) -> plain (CCW) on one context, each against the oracle."""
+    xr = load_xr()
+    s, ctx, coef = _case(three_axes(), 12, 20, 8, 13, 58)
+    truth = fiber_phantom(s.N, 3, 59, s.basis)
+    sino_plain = {rot: oracle.forward_all(s, truth, 1 if rot else 0, True) for rot in (0, 1)}
+    sino_orth = _oracle_forward(oracle, s, truth, coef)
+    v0 = np.full((s.K, s.N, s.N, s.N), 0.05, np.float32)
+
+    def plain(rot):
+        ref, _, _ = oracle.xtt_reconstruct(s, sino_plain[rot], v0, 2, 3, rotate_ccw=rot)
+        ctx.set_option(xr.Option.XTT_SQRT, 1)      # ends with voxelSqrt, as the oracle
+        db, dv = torch.from_numpy(sino_plain[rot]).cuda(), torch.from_numpy(v0).cuda()
+        torch.cuda.synchronize()
+        ctx.dev_session_begin(db.data_ptr(), dv.data_ptr(), True, 2, 3, rotate=rot)
+        for _ in range(2):
+            ctx.dev_session_epoch()
+        ctx.dev_session_end(0, 0)
+        return rel_err(dv.cpu().numpy(), ref)
+
+    assert plain(0) <= TOL
+    ref = _oracle_session(oracle, s, sino_orth, v0, coef, 2, 3, False, 1e-3)
+    ctx.set_option(xr.Option.XTT_SQRT, 0)      # the rotated-basis session's iterate
+    db, dv, dc = (torch.from_numpy(a).cuda() for a in (sino_orth, v0, coef))
+    torch.cuda.synchronize()
+    ctx.dev_session_begin_orth(db.data_ptr(), dv.data_ptr(), dc.data_ptr(), 2, 3)
+    for _ in range(2):
+        ctx.dev_session_epoch()
+    ctx.dev_session_end(0, 0)
+    assert rel_err(dv.cpu().numpy(), ref) <= TOL
+    assert plain(0) <= TOL          # recomputed after the orth session
+    assert plain(0) <= TOL          # kept
+    assert plain(1) <= TOL          # another rotation: recomputed

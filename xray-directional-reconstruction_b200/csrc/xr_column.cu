@@ -518,13 +518,15 @@ __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f
                 acc[p][6] = __fadd2_rn(acc[p][6], m);
                 wgt = __fmul2_rn(inv, m);
             }
-            /* d d^T in xyz order: d_A = da, d_B = db, d_G = dg */
-            const float2 dgg = __fmul2_rn(dg[p], dg[p]), dag = __fmul2_rn(da2, dg[p]), dbg = __fmul2_rn(db2, dg[p]);
-            float2 pr[6];
-            pr[A] = daa; pr[B] = dbb; pr[G] = dgg;
-            pr[3 + A + B - 1] = dab; pr[3 + A + G - 1] = dag; pr[3 + B + G - 1] = dbg;
-#pragma unroll
-            for (int e = 0; e < 6; e++) acc[p][e] = __ffma2_rn(wgt, pr[e], acc[p][e]);
+            /* sum wgt d d^T in the column frame: d_G = dg does not depend on
+             * the view, so its products need only sum wgt, sum wgt da and
+             * sum wgt db (turned into xyz moments after the view loop) */
+            acc[p][0] = __ffma2_rn(wgt, daa, acc[p][0]);
+            acc[p][1] = __ffma2_rn(wgt, dbb, acc[p][1]);
+            acc[p][2] = __ffma2_rn(wgt, dab, acc[p][2]);
+            acc[p][3] = __ffma2_rn(wgt, da2, acc[p][3]);
+            acc[p][4] = __ffma2_rn(wgt, db2, acc[p][4]);
+            acc[p][5] = __fadd2_rn(acc[p][5], wgt);
         }
     }
 }
@@ -584,6 +586,21 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
                 back_view<MODE, G>(g, fr[jj], magsig, ba, bb, dg, okq, P + (size_t)fr[jj].view * NdNd, acc);
     }
     if (!col_ok) return;
+    if (MODE != B_PLAIN) {
+        /* column-frame sums (wgt da^2, wgt db^2, wgt da db, wgt da, wgt db, wgt)
+         * -> xyz moments (xx, yy, zz, xy, xz, yz) with d_A = da, d_B = db, d_G = dg */
+        constexpr int AB = 3 + A + B - 1, AG = 3 + A + G - 1, BG = 3 + B + G - 1;
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+            const float2 c[6] = {acc[p][0], acc[p][1], acc[p][2], acc[p][3], acc[p][4], acc[p][5]};
+            acc[p][A] = c[0];
+            acc[p][B] = c[1];
+            acc[p][G] = __fmul2_rn(__fmul2_rn(dg[p], dg[p]), c[5]);
+            acc[p][AB] = c[2];
+            acc[p][AG] = __fmul2_rn(dg[p], c[3]);
+            acc[p][BG] = __fmul2_rn(dg[p], c[4]);
+        }
+    }
     if (MODE != B_PLAIN && !a.coef) {
         /* fold the basis-independent moments into the channels:
          * tmp_k += g_kc (|S_k|^2 sum r - S_k^T (sum r d d^T / d.d) S_k), channel by
