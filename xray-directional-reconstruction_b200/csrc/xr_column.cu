@@ -297,7 +297,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
         for (int o = 16; o > 0; o >>= 1) bound = fmaxf(bound, __shfl_xor_sync(0xffffffffu, bound, o));
         if ((tid & 31) == 0) s_red[tid >> 5] = bound;
         /* M in the column frame: (aa, bb, ab, ag, bg, gg), so that per view
-         * d^T M d = aa da^2 + bb db^2 + ab da db + dg (ag da + bg db + gg dg) */
+         * d^T M d = aa da^2 + bb db^2 + ab da db + dg (ag da + bg db + gg dg) with
+         * (da, db) fixed per column and view and dg fixed per voxel */
         constexpr int AB = 3 + A + B - 1, AG = 3 + A + G - 1, BG = 3 + B + G - 1;
         constexpr int perm[6] = {A, B, AB, AG, BG, G};
 #pragma unroll
@@ -305,6 +306,11 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
             valp[p] = make_float2(val[2 * p], val[2 * p + 1]);
 #pragma unroll
             for (int e = 0; e < 6; e++) mp[p][e] = make_float2(m[2 * p][perm[e]], m[2 * p + 1][perm[e]]);
+            /* d_g does not depend on the view: fold it into (ag, bg, gg) once, so
+             * per view d^T M d = aa da^2 + bb db^2 + ab da db + ag' da + bg' db + gg' */
+            mp[p][3] = __fmul2_rn(mp[p][3], dgp[p]);
+            mp[p][4] = __fmul2_rn(mp[p][4], dgp[p]);
+            mp[p][5] = __fmul2_rn(mp[p][5], __fmul2_rn(dgp[p], dgp[p]));
         }
     }
     __syncthreads();
@@ -356,9 +362,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
 #pragma unroll
                         for (int e = 0; e < 6; e++) m[e] = (q & 1) ? mp[q >> 1][e].y : mp[q >> 1][e].x;
                         const float dd = fmaf(dgs, dgs, dab2.x);
-                        const float al = fmaf(m[0], daa.x, fmaf(m[1], dbb.x, m[2] * dab.x));
-                        const float be = fmaf(m[3], da, fmaf(m[4], db, m[5] * dgs));
-                        const float q2 = fmaf(dgs, be, al);
+                        const float q2 =
+                            fmaf(m[3], da, fmaf(m[4], db, fmaf(m[0], daa.x, fmaf(m[1], dbb.x, fmaf(m[2], dab.x, m[5])))));
                         const float vq = (q & 1) ? valp[q >> 1].y : valp[q >> 1].x;
                         pvs = fmaf(q2, __fdividef(-1.0f, dd), vq) * fscale;
                     }
