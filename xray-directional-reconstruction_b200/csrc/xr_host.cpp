@@ -328,6 +328,30 @@ static cudaError_t forward_dispatch(xr_ctx *c, const int *vl, int n_views, const
     return cudaSuccess;
 }
 
+/* forwardProjFiber of the listed views of every axis: the column kernel for
+ * each group of column-aligned axes, the general kernel per other axis. */
+static cudaError_t fiber_forward_dispatch(xr_ctx *c, const int *vl, int n_views, const float *vol, float *out) {
+    const ViewFrame *fr = (const ViewFrame *)c->frames.p;
+    const ColInfo *ci = dcol(c);
+    int n_in_group[3] = {0, 0, 0};
+    for (int cond = 0; cond < c->C; cond++) {
+        const int g = c->axis_g[cond];
+        if (g >= 0) {
+            n_in_group[g]++;
+            continue;
+        }
+        cudaError_t e = launch_fiber_forward(c->gc, fr, vl, n_views, &ci->all[cond], 1, vol, out, c->stream);
+        if (e != cudaSuccess) return e;
+    }
+    for (int g = 0; g < 3; g++) {
+        if (n_in_group[g] == 0) continue;
+        cudaError_t e = launch_fiber_forward_col(c->gc, fr, vl, n_views, ci->group[g], n_in_group[g], g, ci->magsig,
+                                                 vol, out, c->stream);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 static std::vector<int> all_conds(const xr_ctx *c) {
     std::vector<int> v(c->C);
     for (int i = 0; i < c->C; i++) v[i] = i;
@@ -493,8 +517,7 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                                              s.coef_kind);
                     s.vol_slabs = 0;
                 } else {
-                    e = s.fiber ? launch_fiber_forward(c->gc, fr, vl, s.subset_size, c->C, (const float *)s.d_vol, proj,
-                                                       str)
+                    e = s.fiber ? fiber_forward_dispatch(c, vl, s.subset_size, (const float *)s.d_vol, proj)
                                 : forward_dispatch(c, vl, s.subset_size, all_conds(c), s.d_vol, proj, 1, s.storage,
                                                    s.coef, s.coef_kind);
                 }
@@ -536,8 +559,9 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                 Timed t(c, XR_T_BACK);
                 cudaError_t e;
                 if (s.fiber) {
-                    e = launch_fiber_back(c->gc, fr, vl, s.subset_size, c->C, proj, (float *)s.d_vol, s.art, alpha,
-                                          str);
+                    const ColInfo *ci = dcol(c);
+                    e = launch_fiber_back(c->gc, fr, vl, s.subset_size, c->C, ci->axis_g, ci->magsig, proj,
+                                          (float *)s.d_vol, s.art, alpha, (int *)c->fiber_flag.p, str);
                 } else if (c->all_aligned) {
                     const ColInfo *ci = dcol(c);
                     const float *sens =
@@ -785,6 +809,7 @@ void xr_destroy(xr_ctx *c) {
     release(c->proj);
     release(c->subsets);
     release(c->loss);
+    release(c->fiber_flag);
     release(c->scratch_vol);
     release(c->scratch_sino);
     release(c->scratch_md);
@@ -939,6 +964,11 @@ static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, 
     if (st) return st;
     const size_t npx = (size_t)c->C * c->V * c->Nd * c->Nd;
     if ((st = ensure(c, c->proj, npx * sizeof(float), "projections"))) return st;
+    if (fiber) {
+        if ((st = ensure(c, c->fiber_flag, sizeof(int), "fiber flag"))) return st;
+        st = cuda_check(c, cudaMemsetAsync(c->fiber_flag.p, 0, sizeof(int), c->stream), "clear fiber flag");
+        if (st) return st;
+    }
     s.order.resize(batch);
     for (int i = 0; i < batch; i++) s.order[i] = i;
     if (!s.xtt) {
@@ -1104,8 +1134,7 @@ static xr_status forward_into(xr_ctx *c, const void *d_vol, float *d_out, int ro
         Timed t(c, XR_T_FORWARD);
         const cudaError_t e =
             mode == kFiberMode
-                ? launch_fiber_forward(c->gc, (const ViewFrame *)c->frames.p, (const int *)lst.p, c->V, c->C,
-                                       (const float *)d_vol, d_out, c->stream)
+                ? fiber_forward_dispatch(c, (const int *)lst.p, c->V, (const float *)d_vol, d_out)
                 : forward_dispatch(c, (const int *)lst.p, c->V, all_conds(c), d_vol, d_out, mode, storage, coef,
                                    coef_kind);
         st = cuda_check(c, e, "forward");

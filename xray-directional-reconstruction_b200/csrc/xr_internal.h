@@ -141,6 +141,7 @@ struct xr_ctx {
     xr::DevBuf proj;                   /* C*V*Nd*Nd: forward / ratio images         */
     xr::DevBuf subsets;                /* batch*subset_size view indices            */
     xr::DevBuf loss;                   /* doubles: loss accumulators                */
+    xr::DevBuf fiber_flag;             /* int: a fiber session's ratio images held inf/NaN */
     xr::DevBuf scratch_vol, scratch_sino, scratch_md, stage;
     xr::DevBuf basis_dev;              /* BasisConst                                */
     xr::DevBuf fdk_frames;             /* C*V ViewFrame with the FDK source         */
@@ -250,15 +251,23 @@ cudaError_t launch_angle_from_md(long nvox, const float *md, float *angle, cudaS
 cudaError_t launch_direction_normalization(long nvox, float *md, cudaStream_t s);
 
 /* ---- xr_fiber.cu: the fiber model (reconstruct/src/fiber.cu) ---- */
-/* forwardProjFiber of the listed views of n_cond axes into out (C blocks of
+/* forwardProjFiber of the listed views of the axes d_conds[0..n_cond) into out (C blocks of
  * V*Nd*Nd, accumulated): c * vs * ratio * |(B x G).(mu_0, mu_1, mu_2) + mu_3|
  * per tap, rayCastingFiber's frame; vol holds min(K, 4) FP32 planes of N^3. */
 cudaError_t launch_fiber_forward(const GeomConst &g, const ViewFrame *frames, const int *view_list, int n_views,
-                                 int n_cond, const float *vol, float *out, cudaStream_t s);
+                                 const int *d_conds, int n_cond, const float *vol, float *out, cudaStream_t s);
+/* the same for n_cond axes of column axis G (d_magsig: sign(ev[G]) * mag) */
+cudaError_t launch_fiber_forward_col(const GeomConst &g, const ViewFrame *frames, const int *view_list, int n_views,
+                                     const int *d_conds, int n_cond, int G, const float *d_magsig, const float *vol,
+                                     float *out, cudaStream_t s);
 /* backwardProjFiber of the listed views of n_cond axes fused with the update
- * of channel 0 (voxelProduct, or voxelPlus with step alpha when art). */
+ * of channel 0 (voxelProduct, or voxelPlus with step alpha when art).
+ * d_axis_g / d_magsig: per axis the column axis (-1: general) and
+ * sign(ev[g]) * mag; *d_nonfinite (a device int the caller clears once per
+ * session) is set when a ratio image read holds an infinity or a NaN. */
 cudaError_t launch_fiber_back(const GeomConst &g, const ViewFrame *frames, const int *view_list, int n_views,
-                              int n_cond, const float *proj, float *vol, int art, float alpha, cudaStream_t s);
+                              int n_cond, const int *d_axis_g, const float *d_magsig, const float *proj, float *vol,
+                              int art, float alpha, int *d_nonfinite, cudaStream_t s);
 
 /* ---- xr_fdk.cu ---- */
 cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_cond, const float *sino,
