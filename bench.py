@@ -548,6 +548,71 @@ def run_c4(args, local):
     return line
 
 
+def run_c3(args, local):
+    """XTT plain vs batched at 128^3 x 13 (12 seeded fiber cylinders, 3
+    sample-rotation axes x 120 views, 192^2 detector, OS-EM 5 subsets, FP32):
+    the same epochs with the forward splat as one launch per column axis
+    (XR_OPT_AXES_ONE_LAUNCH 0; the back-projection always covers all axes and
+    K channels in one launch) and as one launch over all axes (1); device
+    time by CUDA events after warm-up epochs, the forward / back split from
+    the library's per-class timers, the two forward operators compared."""
+    import torch
+    xr = load_pkg()
+    N, Nd, V, K, C = 128, 192, 120, 13, 3
+    basis = basis13()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx = xr.Context.create(W["sdd"], W["sod"], W["det"], N, Nd, V, three_axes(), None, None, basis, device=local)
+    ctx.set_stream(stream.cuda_stream)
+    mu = torch.from_numpy(fiber_phantom(N, 12, 3, basis)).cuda()
+    b = torch.empty((C, V, Nd, Nd), dtype=torch.float32, device="cuda")
+    ctx.dev_forward(mu.data_ptr(), b.data_ptr(), True)
+    arms = {}
+    fwd = {}
+    for name, opt in (("launch_per_column_axis", 0), ("one_launch", 1)):
+        ctx.set_option(xr.Option.AXES_ONE_LAUNCH, opt)
+        p = torch.empty_like(b)
+        ctx.dev_forward(mu.data_ptr(), p.data_ptr(), True)
+        fwd[name] = p
+        v = torch.full((K, N, N, N), 0.01, dtype=torch.float32, device="cuda")
+        ctx.dev_session_begin(b.data_ptr(), v.data_ptr(), True, args.warmup + 2 * args.steps, 5)
+        for _ in range(args.warmup):
+            ctx.dev_session_epoch()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.dev_session_epoch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ctx.set_option(xr.Option.TIMING, 1)
+        ctx.reset_timings()
+        for _ in range(args.steps):
+            ctx.dev_session_epoch()
+        torch.cuda.synchronize()
+        tim = ctx.timings()
+        ctx.set_option(xr.Option.TIMING, 0)
+        ctx.dev_session_end(0, 0)
+        arms[name] = {"epoch_ms": e0.elapsed_time(e1) / args.steps,
+                      "forward_ms": tim["forward"][0] / args.steps, "back_ms": tim["back"][0] / args.steps,
+                      "ratio_ms": tim["ratio"][0] / args.steps,
+                      "forward_launches_per_epoch": 5 * (3 if opt == 0 else 1)}
+    ctx.set_option(xr.Option.AXES_ONE_LAUNCH, 2)
+    a, o = fwd["launch_per_column_axis"].double(), fwd["one_launch"].double()
+    bv = bytes_view(K, N, Nd)
+    line = {"mode": "xtt_plain_vs_batched", "workload": f"XTT {N}^3 x K{K}, {C} axes x {V} views, {Nd}^2 detector, "
+            "OS-EM 5 subsets, FP32 (12 seeded fiber cylinders)", "arms": arms,
+            "speedup_one_launch": arms["launch_per_column_axis"]["epoch_ms"] / arms["one_launch"]["epoch_ms"],
+            "effective_gbs_one_launch": 2 * C * V * bv / (arms["one_launch"]["epoch_ms"] * 1e-3) / 1e9,
+            "forward_max_rel_diff_between_arms": float((a - o).abs().max() / a.abs().max()),
+            "default": "one launch for all axes below 2048 bricks per axis (N < 192), one per column axis above",
+            "steps": args.steps, "warmup": args.warmup}
+    ctx.close()
+    torch.cuda.synchronize()
+    torch.cuda.set_stream(torch.cuda.default_stream())
+    return line
+
+
 C2 = dict(N=256, Nd=384, V=360, n_ell=20, seed=2, photons=1e5, mu_per_mm=0.002, epochs=50, batch=5, lam=0.005)
 
 
@@ -761,6 +826,7 @@ def main():
     ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-residual comparison of the default run")
     ap.add_argument("--c4", action="store_true", help="uneven batch of 8 specimens (BF16), batched vs sequential")
     ap.add_argument("--c2", action="store_true", help="plain cone-beam FDK + 50 OS-ART epochs at 256^3, 360 views")
+    ap.add_argument("--c3", action="store_true", help="XTT 128^3 x 13: forward per column axis vs one launch")
     ap.add_argument("--no-configs", action="store_true", help="skip the FDK+ART and uneven-batch lines of the default run")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the epoch of the reference's CUDA kernels")
     ap.add_argument("--fiber", action="store_true", help="fiber-model forward and epoch timing (128^3 x 4)")
@@ -789,10 +855,12 @@ def main():
             torch.cuda.set_stream(torch.cuda.Stream())
             print(json.dumps(conv_roofline(local, args.conv)), flush=True)
         return
-    if args.ttr or args.c4 or args.fiber or args.c2:
+    if args.ttr or args.c4 or args.fiber or args.c2 or args.c3:
         if rank == 0:          # one GPU: these comparisons run on rank 0 only
             if args.ttr:
                 print(json.dumps(run_ttr(args, local)), flush=True)
+            elif args.c3:
+                print(json.dumps(run_c3(args, local)), flush=True)
             elif args.fiber:
                 print(json.dumps(run_fiber(args, local)), flush=True)
             elif args.c2:
@@ -897,6 +965,8 @@ def main():
     subset = (V + W["batch"] - 1) // W["batch"]
     rot = three_axes().reshape(C, 3, 3)
     n_groups = len({int(np.argmax(np.abs(r[:, 2]))) for r in rot})
+    if ((N + 15) // 16) ** 2 * ((N + 7) // 8) < 2048:   # XR_OPT_AXES_ONE_LAUNCH's default: one launch for all axes
+        n_groups = 1
     fwd_ms, fwd_n = tim["forward"]
     back_ms, back_n = tim["back"]
     if fwd_ms >= back_ms:
@@ -1017,9 +1087,10 @@ def main():
     conv = None
     if world == 1 and args.size == "full":
         conv = conv_roofline(local)
-    c2 = c4 = None
+    c2 = c3 = c4 = None
     if world == 1 and args.size == "full" and not args.no_configs:
         c2 = run_c2(args, local)
+        c3 = run_c3(args, local)
         c4 = run_c4(args, local)
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
@@ -1032,7 +1103,7 @@ def main():
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in tim.items() if v[1]},
             "variants_ms_per_step": variants, "time_to_residual": ttr, "roofline_conv": conv,
-            "fdk_art_256": c2, "uneven_batch_bf16": c4, "reference_gpu": ref_gpu}
+            "fdk_art_256": c2, "xtt_plain_vs_batched_128": c3, "uneven_batch_bf16": c4, "reference_gpu": ref_gpu}
     print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

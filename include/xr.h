@@ -108,10 +108,18 @@ enum {
                                   rounding, 0 round to nearest even.  Nearest
                                   rounding drops every update below half a unit
                                   in the last place, so late OS-EM epochs stall */
-    XR_OPT_XTT_SQRT = 8        /* 1 (default): an XTT session ends with the
+    XR_OPT_XTT_SQRT = 8,       /* 1 (default): an XTT session ends with the
                                   reference's voxelSqrt (reconstruct.cu:919-922);
                                   0: it leaves the iterate itself, so a later
                                   session can continue it                         */
+    XR_OPT_AXES_ONE_LAUNCH = 9 /* XTT forward splat of the rotation axes whose
+                                  grating is a grid axis: 1 all of them in one
+                                  launch (each CTA's axis picks its column axis);
+                                  0 one launch per column axis; 2 (default) one
+                                  launch when a single axis has fewer than 2048
+                                  bricks of 16 x 16 x 8 voxels (N < 192), where
+                                  the per-axis launches would have to split the
+                                  views of a subset over CTAs to fill the GPU   */
 };
 
 /* ---- context ----------------------------------------------------------- */

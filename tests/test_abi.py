@@ -246,3 +246,17 @@ def test_fiber_arguments_rejected():
                 call()
             assert e.value.status == 6
         bad.close()
+
+
+def test_axes_one_launch_option_values():
+    """XR_OPT_AXES_ONE_LAUNCH takes 0 (a launch per column axis), 1 (one launch
+    for all axes) and 2 (automatic, the default); anything else is XR_ERR_ARG."""
+    xr = load_xr()
+    ctx = xr.Context.create(1000, 500, 2, 8, 12, 4, np.eye(3, dtype=np.float32).ravel())
+    for v in (0, 1, 2):
+        ctx.set_option(xr.Option.AXES_ONE_LAUNCH, v)
+    for v in (-1, 3):
+        with pytest.raises(xr.XRError) as e:
+            ctx.set_option(xr.Option.AXES_ONE_LAUNCH, v)
+        assert e.value.status == 1
+    ctx.close()

@@ -41,10 +41,14 @@ def make(N, Nd, V, C=1, K=1, seed=0, shifts=True, sdd=1000.0, sod=500.0, det=2.0
     return s, ctx
 
 
+@pytest.mark.parametrize("axes_one_launch", [0, 1], ids=["launch_per_column_axis", "one_launch"])
 @pytest.mark.parametrize("xtt", [False, True])
-def test_forward_operator(oracle, xtt):
-    """a1-a5: forward splat + chord-length normalisation, every axis/view."""
+def test_forward_operator(oracle, xtt, axes_one_launch):
+    """a1-a5: forward splat + chord-length normalisation, every axis/view; the
+    three axes (column axes z, x, y) as one launch per column axis and as one
+    launch for all (XR_OPT_AXES_ONE_LAUNCH)."""
     s, ctx = make(24, 36, 16, C=3, K=13 if xtt else 1, seed=1)
+    ctx.set_option(load_xr().Option.AXES_ONE_LAUNCH, axes_one_launch)
     rng = np.random.default_rng(2)
     vol = rng.uniform(0, 1, (s.K if xtt else 1, s.N, s.N, s.N)).astype(np.float32)
     got = ctx.forward(vol, xtt)
@@ -99,12 +103,14 @@ def test_ir_reconstruct_small(oracle, method):
     assert np.allclose(gl, rl, rtol=1e-4)
 
 
+@pytest.mark.parametrize("axes_one_launch", [0, 1], ids=["launch_per_column_axis", "one_launch"])
 @pytest.mark.parametrize("method", ["MLEM", "ART"])
-def test_xtt_reconstruct_small(oracle, method):
+def test_xtt_reconstruct_small(oracle, method, axes_one_launch):
     """a4, a8, a9, a10, a11: XTT::reconstruct, 3 axes, K = 13, sqrt at the end;
     the returned ratio images are the reference's last ratio images."""
     xr = load_xr()
     s, ctx = make(16, 24, 12, C=3, K=13, seed=9)
+    ctx.set_option(xr.Option.AXES_ONE_LAUNCH, axes_one_launch)
     truth = fiber_phantom(s.N, 4, 10, s.basis)
     b = oracle.forward_all(s, truth, 0, True)
     v0 = np.full((s.K, s.N, s.N, s.N), 0.01, np.float32)

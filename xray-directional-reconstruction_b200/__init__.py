@@ -83,6 +83,7 @@ class Option(enum.IntEnum):
     SINO_STORAGE = 6
     ROUNDING = 7
     XTT_SQRT = 8
+    AXES_ONE_LAUNCH = 9
 
 
 class Storage(enum.IntEnum):

@@ -118,7 +118,7 @@ struct FwdColArgs {
     const ViewFrame *frames;
     const int *view_list;
     int n_views, vpc;
-    const int *conds;         /* n_cond axis indices, all with column axis G */
+    const int *conds;         /* n_cond axis indices (k_fwd_col: all with column axis G) */
     const float *magsig;      /* per axis: sign(ev[g]) * mag                 */
     const void *vol;          /* storage type T                              */
     float *out;
@@ -127,10 +127,12 @@ struct FwdColArgs {
     int coef_kind;            /* 0: (phi, cos theta); 1: main direction      */
     int nbg, nba;             /* bricks along g and a                        */
     int zlo, zhi;             /* only bricks whose first z lies in [zlo, zhi) */
+    const int *axis_g;        /* k_fwd_col_axes: per axis its column axis    */
 };
 
+/* One CTA's work: brick blockIdx.x, views chunk blockIdx.z of axis cond. */
 template <int MODE, int G, typename T>
-__global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
+__device__ __forceinline__ void fwd_col_brick(const FwdColArgs &a, const int cond) {
     const T *vol = reinterpret_cast<const T *>(a.vol);
     constexpr int A = Ax<G>::A, B = Ax<G>::B;
     /* Two detector tiles (double-buffered over views) in two-word fixed
@@ -143,7 +145,6 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
 
     const GeomConst &g = a.g;
     const int N = g.N, Nd = g.Nd;
-    const int cond = a.conds[blockIdx.y];
     const float magsig = a.magsig[cond];
     const int j0 = blockIdx.z * a.vpc;
     const int nv = min(a.vpc, a.n_views - j0);
@@ -404,6 +405,23 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
             }
         }
     }
+}
+
+/* Axes of one column axis G (blockIdx.y indexes a.conds). */
+template <int MODE, int G, typename T>
+__global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col(FwdColArgs a) {
+    fwd_col_brick<MODE, G, T>(a, a.conds[blockIdx.y]);
+}
+
+/* Every listed axis in one launch, whatever its column axis: the CTA's axis
+ * picks the instance (uniform over the CTA). */
+template <int MODE, typename T>
+__global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col_axes(FwdColArgs a) {
+    const int cond = a.conds[blockIdx.y];
+    const int G = a.axis_g[cond];
+    if (G == 0) fwd_col_brick<MODE, 0, T>(a, cond);
+    else if (G == 1) fwd_col_brick<MODE, 1, T>(a, cond);
+    else fwd_col_brick<MODE, 2, T>(a, cond);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -765,13 +783,16 @@ cudaError_t check_exact_rdet(float det, float rdet, unsigned *d_flag, unsigned *
 cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, const int *d_conds, int n_cond, int G,
                                const float *d_magsig, const void *vol, float *out, int mode, int views_per_cta,
-                               int storage, cudaStream_t s, const float *coef, int coef_kind, int zlo, int zhi) {
+                               int storage, cudaStream_t s, const float *coef, int coef_kind, int zlo, int zhi,
+                               const int *d_axis_g) {
     if (n_views <= 0 || n_cond <= 0) return cudaSuccess;
     if (coef && mode == 1) mode = 3;
     FwdColArgs a;
     a.zlo = zlo;
     a.zhi = zhi;
     a.coef_kind = coef_kind;
+    a.axis_g = d_axis_g;
+    if (G < 0 && (!d_axis_g || mode == 0)) return cudaErrorInvalidValue;
     a.g = g;
     a.frames = frames;
     a.view_list = view_list;
@@ -804,9 +825,17 @@ cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, co
         if (e != cudaSuccess) return e;                                                                           \
         k_fwd_col<M, GG, TT><<<grid, kFwdThreads, smem, s>>>(a);                                                  \
     } while (0)
+#define XR_FWD_AXES(M, TT)                                                                                        \
+    do {                                                                                                          \
+        cudaError_t e = cudaFuncSetAttribute(k_fwd_col_axes<M, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                             (int)smem);                                                          \
+        if (e != cudaSuccess) return e;                                                                           \
+        k_fwd_col_axes<M, TT><<<grid, kFwdThreads, smem, s>>>(a);                                                 \
+    } while (0)
 #define XR_FWD_COL_G(M, TT)                                                                                       \
     do {                                                                                                          \
-        if (G == 0) XR_FWD_COL(M, 0, TT); else if (G == 1) XR_FWD_COL(M, 1, TT); else XR_FWD_COL(M, 2, TT);      \
+        if (G < 0 && M != 0) XR_FWD_AXES(M == 0 ? 1 : M, TT);                                                     \
+        else if (G == 0) XR_FWD_COL(M, 0, TT); else if (G == 1) XR_FWD_COL(M, 1, TT); else XR_FWD_COL(M, 2, TT); \
     } while (0)
     if (mode == 2) {
         XR_FWD_COL_G(2, float);
@@ -824,6 +853,7 @@ cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, co
         else XR_FWD_COL_G(1, float);
     }
 #undef XR_FWD_COL_G
+#undef XR_FWD_AXES
 #undef XR_FWD_COL
     return cudaGetLastError();
 }

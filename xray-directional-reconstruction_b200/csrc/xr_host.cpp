@@ -302,6 +302,14 @@ static cudaError_t forward_dispatch(xr_ctx *c, const int *vl, int n_views, const
             grp[g].push_back(cond);
         }
     }
+    const long bricks = (long)((c->N + 15) / 16) * ((c->N + 15) / 16) * ((c->N + 7) / 8);
+    const bool one = c->axes_one_launch == 1 || (c->axes_one_launch == 2 && bricks < 2048);
+    if (one && (int)conds.size() == c->C && c->all_aligned &&
+        (!grp[0].empty() + !grp[1].empty() + !grp[2].empty()) > 1 && mode != 0) {
+        /* every axis, several column axes: one launch (per-CTA column axis) */
+        return launch_forward_col(c->gc, dbasis(c), fr, vl, n_views, ci->all, c->C, -1, ci->magsig, vol, out, mode,
+                                  c->views_per_cta, storage, c->stream, coef, coef_kind, zlo, zhi, ci->axis_g);
+    }
     for (int g = 0; g < 3; g++) {
         if (grp[g].empty()) continue;
         /* the device group list holds every axis of column axis g in order;
@@ -876,6 +884,10 @@ xr_status xr_set_option(xr_ctx *c, int key, int value) {
             return XR_OK;
         case XR_OPT_GRAPHS: c->use_graphs = value != 0; return XR_OK;
         case XR_OPT_XTT_SQRT: c->xtt_sqrt = value != 0; return XR_OK;
+        case XR_OPT_AXES_ONE_LAUNCH:
+            if (value < 0 || value > 2) return fail(c, XR_ERR_ARG, "axes per launch must be 0, 1 or 2");
+            c->axes_one_launch = value;
+            return XR_OK;
         case XR_OPT_ROUNDING:
             if (value < 0 || value > 1) return fail(c, XR_ERR_ARG, "rounding must be 0 (nearest) or 1 (stochastic)");
             if (c->sess.active) return fail(c, XR_ERR_STATE, "rounding cannot change during a session");

@@ -128,6 +128,7 @@ struct xr_ctx {
     bool stochastic = true;           /* 16-bit updates: stochastic rounding */
     bool xtt_sqrt = true;             /* XTT session end applies voxelSqrt   */
     bool use_graphs = false;
+    int axes_one_launch = 2;          /* XTT forward: column-aligned axes in one launch (XR_OPT_AXES_ONE_LAUNCH) */
 
     xr::GeomConst gc{};
     xr::BasisConst bc{};
@@ -211,12 +212,14 @@ cudaError_t launch_convert(long n, const void *src, int src_storage, void *dst, 
 /* ---- xr_column.cu: kernels for axes whose grating direction is a grid axis ---- */
 cudaError_t check_exact_rdet(float det, float rdet, unsigned *d_flag, unsigned *h_result, cudaStream_t s);
 /* zlo, zhi: only the bricks whose first voxel's z lies in [zlo, zhi) (z-slab
- * launches over a volume that arrives slab by slab; slab bounds multiples of 16). */
+ * launches over a volume that arrives slab by slab; slab bounds multiples of 16).
+ * G < 0 (modes 1-3): the listed axes may have different column axes, given
+ * per axis by d_axis_g; one launch covers them all. */
 cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                                const int *view_list, int n_views, const int *d_conds, int n_cond, int G,
                                const float *d_magsig, const void *vol, float *out, int mode, int views_per_cta,
                                int storage, cudaStream_t s, const float *coef = nullptr, int coef_kind = 0,
-                               int zlo = 0, int zhi = 1 << 30);
+                               int zlo = 0, int zhi = 1 << 30, const int *d_axis_g = nullptr);
 /* mode 0: plain (one axis, update in place); 1: XTT (fac_in = sensitivity);
  * 2: sensitivity of the listed views into fac_out. */
 cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
