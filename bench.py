@@ -240,11 +240,26 @@ class ClockSampler:
         return out
 
 
-def cpu_reference_sample(mu_host: np.ndarray, b_host: np.ndarray, n_views: int, warm: int = 0):
+def bench_config(args, world: int):
+    """The workload named in both arms' JSON lines (the same dict)."""
+    N, Nd, V, C, K = W["N"], W["Nd"], W["V"], W["C"], W["K"]
+    vol_mb, sino_mb = K * N ** 3 * 4 / 2 ** 20, C * V * Nd * Nd * 4 / 2 ** 20
+    return {"workload": WORKLOAD if args.size == "full" else
+            f"XTT {N}^3 x K{K}, {C} axes x {V} views, {Nd}^2 detector, OS-EM {W['batch']} subsets, FP32 "
+            "(profile case: the kernels of the full workload at a size ncu captures)",
+            "N": N, "K": K, "axes": C, "views": V, "detector": Nd, "subsets": W["batch"],
+            "parallelism": f"replicas x{world}",
+            "l2": f"inputs larger than L2 (volume {vol_mb:.0f} MiB, sinograms {sino_mb:.0f} MiB)"}
+
+
+def cpu_reference_sample(mu_host: np.ndarray, b_host, n_views: int, warm: int = 0, first: int = 0):
     """Time the reference's own projector kernels (reconstruct/src/ir.cu built
-    for the host, OpenMP over detector/voxel rows) on n_views views of the
-    same workload: forward + correlation + ratio, then the back-projection of
-    every y slab.  Returns (seconds, threads)."""
+    for the host, OpenMP over detector/voxel rows) on n_views (axis, view)
+    pairs of the workload, starting at pair `first` of a fixed sequence that
+    visits the three axes in turn: per pair forward + correlation + ratio
+    against the measured image, then the back-projection of every y slab.
+    mu_host is the current iterate; b_host(cond, n) returns the measured image
+    of a pair (flat float32).  Returns (seconds, threads)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import RefHost, Scan
     s = Scan(sdd=W["sdd"], sod=W["sod"], det=W["det"], N=W["N"], Nd=W["Nd"], V=W["V"], rot=three_axes(),
@@ -257,11 +272,11 @@ def cpu_reference_sample(mu_host: np.ndarray, b_host: np.ndarray, n_views: int, 
     fac = np.zeros(Nd * Nd, np.float32)
     tmp = np.zeros(N * N * K, np.float32)
     bfac = np.zeros(N * N * K, np.float32)
-    views = [(c, (v * 37) % s.V) for c in range(s.C) for v in range(s.V)]
     t_total = 0.0
     for i in range(warm + n_views):
-        cond, n = views[i % len(views)]
-        sino = np.ascontiguousarray(b_host[cond].reshape(-1))
+        cond, n = reference_pair(first + i)
+        sino = np.zeros(s.V * Nd * Nd, np.float32)
+        sino[n * Nd * Nd:(n + 1) * Nd * Nd] = b_host(cond, n)
         t0 = time.perf_counter()
         R.forward_view(cond, n, vol, proj, fac, 1)
         R.correlation(cond, n, proj, fac)
@@ -277,31 +292,68 @@ def cpu_reference_sample(mu_host: np.ndarray, b_host: np.ndarray, n_views: int, 
     return t_total, threads
 
 
+def reference_pair(i: int):
+    """(axis, view) of the i-th pair of the CPU samples: the axes in turn, the
+    views of each axis in a stride-37 order over the scan."""
+    return i % W["C"], (37 * (i // W["C"])) % W["V"]
+
+
+def reference_measured(mu_true: np.ndarray):
+    """The measured images b = A mu_true of the sampled pairs, made with the
+    reference's own host forward operator (forwardProjXTT +
+    correlationProjByLength) of the phantom the GPU arm reconstructs."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefHost, Scan
+    s = Scan(sdd=W["sdd"], sod=W["sod"], det=W["det"], N=W["N"], Nd=W["Nd"], V=W["V"], rot=three_axes(),
+             trans=np.zeros((3, 3)), offset=np.zeros((3, 3)), basis=basis13())
+    R = RefHost(parallel=True)
+    R.setup(s)
+    Nd = s.Nd
+    vol = np.ascontiguousarray(mu_true.reshape(-1))
+    cache = {}
+
+    def get(cond, n):
+        if (cond, n) not in cache:
+            proj = np.zeros(s.V * Nd * Nd, np.float32)
+            fac = np.zeros(Nd * Nd, np.float32)
+            R.forward_view(cond, n, vol, proj, fac, 1)
+            R.correlation(cond, n, proj, fac)
+            cache[(cond, n)] = proj[n * Nd * Nd:(n + 1) * Nd * Nd].copy()
+        return cache[(cond, n)]
+    return get
+
+
 def run_reference(args, rank):
     """--impl reference: the reference's CPU implementation of the path on
-    the host cores (oracle/_ref, its own ir.cu), same metric and config."""
+    the host cores (oracle/_ref, its own ir.cu), same metric and config: the
+    phantom the GPU arm reconstructs, its measured images made by the
+    reference's own forward operator, the OS-EM start mu = 0.01; each step a
+    sample of 3 (axis, view) pairs (one per axis) of the epoch's 540."""
     if rank != 0:
         return
     bv = bytes_view(W["K"], W["N"], W["Nd"])
-    mu = fiber_phantom(W["N"], W["n_fibers"], W["seed"], basis13())
-    rng = np.random.default_rng(1)
-    b = rng.uniform(0.0, 50.0, (W["C"], W["V"], W["Nd"], W["Nd"])).astype(np.float32)
-    per_step_views = 1
+    mu_true = fiber_phantom(W["N"], W["n_fibers"], W["seed"], basis13())
+    b = reference_measured(mu_true)
+    mu = np.full_like(mu_true, 0.01)
+    per_step_views = 3
     times = []
     threads = 1
     for i in range(args.warmup + args.steps):
-        t, threads = cpu_reference_sample(mu, b, per_step_views, 0)
+        t, threads = cpu_reference_sample(mu, b, per_step_views, 0, first=i * per_step_views)
         if i >= args.warmup:
             times.append(t)
     t_step = float(np.mean(times))
     value = 2 * per_step_views * bv / t_step / 1e9
+    sample = (f"{per_step_views} of {W['C'] * W['V']} (axis, view) pairs per step (one per axis), forward + "
+              "correlation + ratio + back-projection of all K channels; reference ir.cu kernels compiled for the "
+              "host, OpenMP; same phantom and OS-EM start as the GPU arm, measured images by the reference's own "
+              "forward operator")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample": f"{per_step_views} view (forward+ratio+back, all K) per step"},
+            "config": bench_config(args, 1),
             "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "reference",
-                             "sample": f"{per_step_views} of {W['C'] * W['V']} views per step, reference ir.cu "
-                                       "kernels compiled for the host, OpenMP"},
+                             "sample": sample},
             "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -1054,11 +1106,14 @@ def main():
 
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        n_views = 2
-        t, threads = cpu_reference_sample(mu_true, d_b.cpu().numpy(), n_views, 0)
+        n_views = 3
+        hb = d_b.cpu().numpy()
+        t, threads = cpu_reference_sample(np.full_like(mu_true, 0.01), lambda cond, n: hb[cond, n].ravel(),
+                                          n_views, 0)
         cpu = {"value": 2 * n_views * bv / t / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
-               "sample": f"{n_views} of {C * V} views (forward+ratio+back, all K), reference ir.cu kernels "
-                         "compiled for the host, OpenMP"}
+               "sample": f"{n_views} of {C * V} (axis, view) pairs (one per axis), forward + correlation + ratio + "
+                         "back-projection of all K channels, reference ir.cu kernels compiled for the host, OpenMP; "
+                         "the GPU arm's measured images and OS-EM start"}
 
     ref_gpu = None
     if world == 1 and args.size == "full" and not args.no_ref_gpu:
@@ -1095,10 +1150,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "N": N, "K": K, "axes": C, "views": V, "detector": Nd,
-                       "subsets": W["batch"], "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (volume 872 MB, sinograms 318 MB)",
-                       "residual_rel_l2_after": rel},
+            "config": bench_config(args, world), "residual_rel_l2_after": rel,
             "e2e": e2e, "roofline": roofline, "roofline_hbm": hbm, "effective_projector": effective,
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in tim.items() if v[1]},
