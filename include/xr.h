@@ -112,7 +112,7 @@ enum {
                                   reference's voxelSqrt (reconstruct.cu:919-922);
                                   0: it leaves the iterate itself, so a later
                                   session can continue it                         */
-    XR_OPT_AXES_ONE_LAUNCH = 9 /* XTT forward splat of the rotation axes whose
+    XR_OPT_AXES_ONE_LAUNCH = 9,/* XTT forward splat of the rotation axes whose
                                   grating is a grid axis: 1 all of them in one
                                   launch (each CTA's axis picks its column axis);
                                   0 one launch per column axis; 2 (default) one
@@ -120,6 +120,12 @@ enum {
                                   bricks of 16 x 16 x 8 voxels (N < 192), where
                                   the per-axis launches would have to split the
                                   views of a subset over CTAs to fill the GPU   */
+    XR_OPT_RATIO_TEXTURE = 10  /* 1 (default): XTT sessions whose axes are all
+                                  column-aligned keep the subset's ratio images
+                                  in a 2D-layered CUDA array as well, and the
+                                  back-projection gathers each voxel's 4 taps
+                                  with one texture instruction; 0: it loads
+                                  them from the linear images                    */
 };
 
 /* ---- context ----------------------------------------------------------- */

@@ -260,3 +260,12 @@ def test_axes_one_launch_option_values():
             ctx.set_option(xr.Option.AXES_ONE_LAUNCH, v)
         assert e.value.status == 1
     ctx.close()
+
+
+def test_ratio_texture_option_values():
+    """XR_OPT_RATIO_TEXTURE takes 0 or 1 outside a session."""
+    xr = load_xr()
+    ctx = xr.Context.create(1000, 500, 2, 8, 12, 4, np.eye(3, dtype=np.float32).ravel())
+    for v in (0, 1):
+        ctx.set_option(xr.Option.RATIO_TEXTURE, v)
+    ctx.close()

@@ -103,14 +103,20 @@ def test_ir_reconstruct_small(oracle, method):
     assert np.allclose(gl, rl, rtol=1e-4)
 
 
-@pytest.mark.parametrize("axes_one_launch", [0, 1], ids=["launch_per_column_axis", "one_launch"])
+@pytest.mark.parametrize("variant", [(0, 1), (1, 1), (1, 0)],
+                         ids=["launch_per_column_axis", "one_launch", "one_launch_linear_ratio_loads"])
 @pytest.mark.parametrize("method", ["MLEM", "ART"])
-def test_xtt_reconstruct_small(oracle, method, axes_one_launch):
+def test_xtt_reconstruct_small(oracle, method, variant):
     """a4, a8, a9, a10, a11: XTT::reconstruct, 3 axes, K = 13, sqrt at the end;
-    the returned ratio images are the reference's last ratio images."""
+    the returned ratio images are the reference's last ratio images.  The
+    forward as one launch per column axis or one for all axes
+    (XR_OPT_AXES_ONE_LAUNCH); the back-projection gathering its taps from the
+    layered ratio texture or loading them from the linear images
+    (XR_OPT_RATIO_TEXTURE)."""
     xr = load_xr()
     s, ctx = make(16, 24, 12, C=3, K=13, seed=9)
-    ctx.set_option(xr.Option.AXES_ONE_LAUNCH, axes_one_launch)
+    ctx.set_option(xr.Option.AXES_ONE_LAUNCH, variant[0])
+    ctx.set_option(xr.Option.RATIO_TEXTURE, variant[1])
     truth = fiber_phantom(s.N, 4, 10, s.basis)
     b = oracle.forward_all(s, truth, 0, True)
     v0 = np.full((s.K, s.N, s.N, s.N), 0.01, np.float32)

@@ -84,6 +84,7 @@ class Option(enum.IntEnum):
     ROUNDING = 7
     XTT_SQRT = 8
     AXES_ONE_LAUNCH = 9
+    RATIO_TEXTURE = 10
 
 
 class Storage(enum.IntEnum):

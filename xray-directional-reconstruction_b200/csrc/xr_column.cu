@@ -435,7 +435,21 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col_axes(FwdColArgs a) {
 /*   SENS:  moments sum(1), sum(d d^T / d.d) folded into factor_k, written    */
 /*          to global (geometry only; once per subset).                       */
 /* ------------------------------------------------------------------------ */
-enum { B_PLAIN = 0, B_XTT = 1, B_SENS = 2 };
+/* B_XTT_TEX: B_XTT with the 4 taps of each voxel-view gathered in one
+ * texture instruction from the subset's ratio images in a 2D-layered array. */
+enum { B_PLAIN = 0, B_XTT = 1, B_SENS = 2, B_XTT_TEX = 3 };
+
+/* The 2 x 2 texels around unnormalised coordinates (x, y) of layer `layer`
+ * (tld4, component r): (T[y1][x0], T[y1][x1], T[y0][x1], T[y0][x0]) with
+ * x0 = floor(x - 0.5), x1 = x0 + 1 and likewise y; coordinates outside the
+ * layer clamp to its edge. */
+__device__ __forceinline__ float4 gather_a2d(cudaTextureObject_t t, int layer, float x, float y) {
+    float4 r;
+    asm("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %7}];"
+        : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+        : "l"(t), "r"(layer), "f"(x), "f"(y));
+    return r;
+}
 
 struct BackColArgs {
     GeomConst g;
@@ -455,6 +469,7 @@ struct BackColArgs {
     int sr;                   /* 16-bit volumes: stochastic rounding of updates */
     const float *coef;        /* non-null: per-voxel rotated basis (backwardOrth) */
     int coef_kind;            /* 0: (phi, cos theta); 1: main direction            */
+    cudaTextureObject_t rtex; /* B_XTT_TEX: the ratio images, layer = axis * n_views + position */
 };
 
 /* Shared-memory slot of brick voxel lv (x + 8y + 64z) in the per-voxel
@@ -470,7 +485,8 @@ __device__ __forceinline__ int sacc_slot(int lv) { return lv ^ ((lv >> 5) & 7) ^
  * dg: o_g of the voxels (per axis, view-independent); okq: voxel in range. */
 template <int MODE, int G>
 __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f, float magsig, float ba, float bb,
-                                          const float2 dg[2], const bool okq[4], const float *Pv, float2 acc[2][7]) {
+                                          const float2 dg[2], const bool okq[4], const float *Pv, float2 acc[2][7],
+                                          cudaTextureObject_t rtex, int layer) {
     constexpr int A = Ax<G>::A, B = Ax<G>::B;
     const int Nd = g.Nd;
     float u, coeff, da, db;
@@ -482,6 +498,7 @@ __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f
     const float *Pc = Pv + iu;
     /* the products of d = (d_A, d_B, d_G) that do not involve d_G */
     const float2 daa = bc2(da * da), dbb = bc2(db * db), dab = bc2(da * db), da2 = bc2(da), db2 = bc2(db);
+    const float xu = __int2float_rn(iu + 1);   /* gathers texels iu, iu + 1 */
     /* Two phases: first both pairs' taps and their 16 gathers (a voxel off
      * the detector reads row 0 and is dropped), then the accumulation. */
     float2 fv[2], gv[2], p0[2], p1[2], p2[2], p3[2];
@@ -503,7 +520,14 @@ __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f
         const float2 fi = make_float2(floorf(ut.x), floorf(ut.y));
         fv[p] = __ffma2_rn(fi, bc2(-1.0f), ut);
         gv[p] = __ffma2_rn(fv[p], bc2(-1.0f), bc2(1.0f));
-        if (MODE != B_SENS) {
+        if (MODE == B_XTT_TEX) {
+            const float4 t0 = gather_a2d(rtex, layer, xu, fi.x + 1.0f);
+            const float4 t1 = gather_a2d(rtex, layer, xu, fi.y + 1.0f);
+            p0[p] = make_float2(t0.w, t1.w);
+            p1[p] = make_float2(t0.z, t1.z);
+            p2[p] = make_float2(t0.x, t1.x);
+            p3[p] = make_float2(t0.y, t1.y);
+        } else if (MODE != B_SENS) {
             const float *q0 = Pc + Nd * (ok[2 * p] ? (int)fi.x : 0);
             const float *q1 = Pc + Nd * (ok[2 * p + 1] ? (int)fi.y : 0);
             p0[p] = make_float2(__ldg(q0), __ldg(q1));
@@ -534,7 +558,7 @@ __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f
             const float2 dd = __ffma2_rn(dg[p], dg[p], dab2);
             const float2 inv = make_float2(__fdividef(1.0f, dd.x), __fdividef(1.0f, dd.y));  /* ~2 ulp */
             float2 wgt;
-            if (MODE == B_XTT) {
+            if (MODE == B_XTT || MODE == B_XTT_TEX) {
                 acc[p][6] = __fadd2_rn(acc[p][6], nb);
                 wgt = __fmul2_rn(nb, inv);
             } else {
@@ -606,7 +630,8 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
         __syncthreads();
         if (nq > 0)
             for (int jj = 0; jj < nc; jj++)
-                back_view<MODE, G>(g, fr[jj], magsig, ba, bb, dg, okq, P + (size_t)fr[jj].view * NdNd, acc);
+                back_view<MODE, G>(g, fr[jj], magsig, ba, bb, dg, okq, P + (size_t)fr[jj].view * NdNd, acc, a.rtex,
+                                   cond * a.n_views + c0 + jj);
     }
     if (!col_ok) return;
     if (MODE != B_PLAIN) {
@@ -862,8 +887,10 @@ cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const
                             const int *view_list, int n_views, const int *d_conds, int n_cond, const int *d_axis_g,
                             const float *d_magsig, const float *proj, void *vol, const float *fac_in, float *fac_out,
                             int mode, int art, float alpha, int storage, cudaStream_t s, const float *coef,
-                            int coef_kind) {
+                            int coef_kind, cudaTextureObject_t rtex) {
     BackColArgs a;
+    a.rtex = rtex;
+    if (mode == B_XTT && rtex) mode = B_XTT_TEX;
     a.coef = coef;
     a.coef_kind = coef_kind;
     a.sr = (storage & kStoreStochastic) != 0;
@@ -896,11 +923,17 @@ cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const
     if (mode == B_SENS) {
         XR_BACK_COL(B_SENS, float);
     } else if (storage == kBF16) {
-        if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, __nv_bfloat16); else XR_BACK_COL(B_XTT, __nv_bfloat16);
+        if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, __nv_bfloat16);
+        else if (mode == B_XTT_TEX) XR_BACK_COL(B_XTT_TEX, __nv_bfloat16);
+        else XR_BACK_COL(B_XTT, __nv_bfloat16);
     } else if (storage == kF16) {
-        if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, __half); else XR_BACK_COL(B_XTT, __half);
+        if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, __half);
+        else if (mode == B_XTT_TEX) XR_BACK_COL(B_XTT_TEX, __half);
+        else XR_BACK_COL(B_XTT, __half);
     } else {
-        if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, float); else XR_BACK_COL(B_XTT, float);
+        if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, float);
+        else if (mode == B_XTT_TEX) XR_BACK_COL(B_XTT_TEX, float);
+        else XR_BACK_COL(B_XTT, float);
     }
 #undef XR_BACK_COL
     return cudaGetLastError();

@@ -544,7 +544,8 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                  * (forwardOrthByMD -> correlationProjByLength, reconstruct.cu:1501-1509) */
                 const float *nrm = ((s.coef && s.coef_kind == 0) || s.fiber) ? nullptr : norm;
                 if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, c->C, proj, nrm,
-                                                     s.d_sino, s.art, dl, s.sino_storage, str), "ratio")))
+                                                     s.d_sino, s.art, dl, s.sino_storage, str,
+                                                     s.rtex ? c->rsurf : 0), "ratio")))
                     return st;
             }
             if (s.ratio_dst) {
@@ -576,7 +577,7 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                         s.art ? nullptr : (const float *)c->sens.p + (size_t)orders[b] * c->K * N3;
                     e = launch_back_col(c->gc, dbasis(c), fr, vl, s.subset_size, ci->all, c->C, ci->axis_g,
                                         ci->magsig, proj, s.d_vol, sens, nullptr, 1, s.art, alpha, s.update_storage,
-                                        str, s.coef, s.coef_kind);
+                                        str, s.coef, s.coef_kind, s.rtex ? c->rtex : 0);
                 } else {
                     e = launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, 0, c->C, proj, s.d_vol, 1, s.art,
                                            alpha, s.update_storage, str, s.coef, s.coef_kind);
@@ -800,6 +801,8 @@ xr_status xr_init_params(const char *json_path, const char *tag, int device, xr_
     return XR_OK;
 }
 
+static void free_ratio_texture(xr_ctx *c);
+
 void xr_destroy(xr_ctx *c) {
     if (!c) return;
     if (c->dev_ready) {
@@ -818,6 +821,7 @@ void xr_destroy(xr_ctx *c) {
     release(c->subsets);
     release(c->loss);
     release(c->fiber_flag);
+    if (c->dev_ready) free_ratio_texture(c);
     release(c->scratch_vol);
     release(c->scratch_sino);
     release(c->scratch_md);
@@ -884,6 +888,10 @@ xr_status xr_set_option(xr_ctx *c, int key, int value) {
             return XR_OK;
         case XR_OPT_GRAPHS: c->use_graphs = value != 0; return XR_OK;
         case XR_OPT_XTT_SQRT: c->xtt_sqrt = value != 0; return XR_OK;
+        case XR_OPT_RATIO_TEXTURE:
+            if (c->sess.active) return fail(c, XR_ERR_STATE, "the ratio texture cannot change during a session");
+            c->ratio_texture = value != 0;
+            return XR_OK;
         case XR_OPT_AXES_ONE_LAUNCH:
             if (value < 0 || value > 2) return fail(c, XR_ERR_ARG, "axes per launch must be 0, 1 or 2");
             c->axes_one_launch = value;
@@ -929,6 +937,55 @@ xr_status xr_reset_timings(xr_ctx *c) {
 }
 
 /* ------------------------------------------------------------- sessions */
+
+static void free_ratio_texture(xr_ctx *c) {
+    if (c->rtex) cudaDestroyTextureObject(c->rtex);
+    if (c->rsurf) cudaDestroySurfaceObject(c->rsurf);
+    if (c->rarr) cudaFreeArray(c->rarr);
+    c->rtex = 0;
+    c->rsurf = 0;
+    c->rarr = nullptr;
+    c->rlayers = c->rnd = 0;
+}
+
+/* The 2D-layered array of a subset's ratio images (Nd x Nd floats, `layers`
+ * layers) with its texture (point sampling, clamped, unnormalised
+ * coordinates) and surface objects; kept while the shape stays.  Leaves
+ * c->rtex = 0 (the back kernel then loads from the linear images) when the
+ * device cannot hold that many layers. */
+static xr_status ensure_ratio_texture(xr_ctx *c, int layers) {
+    if (c->rarr && c->rlayers == layers && c->rnd == c->Nd) return XR_OK;
+    free_ratio_texture(c);
+    int max_layers = 0, max_wh = 0;
+    cudaDeviceGetAttribute(&max_layers, cudaDevAttrMaxSurface2DLayeredLayers, c->device);
+    cudaDeviceGetAttribute(&max_wh, cudaDevAttrMaxSurface2DLayeredWidth, c->device);
+    if (layers < 1 || layers > max_layers || c->Nd > max_wh) return XR_OK;
+    const cudaChannelFormatDesc fd = cudaCreateChannelDesc<float>();
+    xr_status st = cuda_check(c, cudaMalloc3DArray(&c->rarr, &fd, make_cudaExtent(c->Nd, c->Nd, layers),
+                                                   cudaArrayLayered | cudaArraySurfaceLoadStore),
+                              "ratio image array");
+    if (st) {
+        c->rarr = nullptr;
+        return st;
+    }
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = c->rarr;
+    cudaTextureDesc td{};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    if ((st = cuda_check(c, cudaCreateTextureObject(&c->rtex, &rd, &td, nullptr), "ratio texture")) ||
+        (st = cuda_check(c, cudaCreateSurfaceObject(&c->rsurf, &rd), "ratio surface"))) {
+        free_ratio_texture(c);
+        return st;
+    }
+    c->rlayers = layers;
+    c->rnd = c->Nd;
+    return XR_OK;
+}
+
 
 static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, int xtt, int epochs, int batch,
                                     xr_rotate dir, xr_method method, float lambda, const float *coef,
@@ -976,6 +1033,11 @@ static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, 
     if (st) return st;
     const size_t npx = (size_t)c->C * c->V * c->Nd * c->Nd;
     if ((st = ensure(c, c->proj, npx * sizeof(float), "projections"))) return st;
+    s.rtex = false;
+    if (s.xtt && !fiber && c->all_aligned && c->ratio_texture) {
+        if ((st = ensure_ratio_texture(c, c->C * s.subset_size))) return st;
+        s.rtex = c->rtex != 0;
+    }
     if (fiber) {
         if ((st = ensure(c, c->fiber_flag, sizeof(int), "fiber flag"))) return st;
         st = cuda_check(c, cudaMemsetAsync(c->fiber_flag.p, 0, sizeof(int), c->stream), "clear fiber flag");

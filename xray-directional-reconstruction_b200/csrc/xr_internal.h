@@ -98,6 +98,7 @@ struct Session {
     cudaEvent_t sino_ready = nullptr; /* set: the first ratio launch waits for it (sinogram upload) */
     cudaEvent_t sino_rest = nullptr;  /* set: the second ratio launch waits for it (rest of the sinogram) */
     int vol_slabs = 0;                /* > 0: the first forward runs by z-slabs, each after its upload event */
+    bool rtex = false;                /* XTT column session: ratio images through the layered texture */
     const cudaEvent_t *slab_ev = nullptr;
     float *const *ratio_dst = nullptr; /* set: each view's final ratio image to these host planes */
     std::vector<int> order;            /* persistent subset order (XTT)     */
@@ -143,6 +144,14 @@ struct xr_ctx {
     xr::DevBuf subsets;                /* batch*subset_size view indices            */
     xr::DevBuf loss;                   /* doubles: loss accumulators                */
     xr::DevBuf fiber_flag;             /* int: a fiber session's ratio images held inf/NaN */
+    /* XTT column sessions: the subset's ratio images as a 2D-layered array
+     * (layer = axis * subset size + list position), written by the ratio
+     * kernel through rsurf and gathered by the back kernel through rtex */
+    cudaArray_t rarr = nullptr;
+    cudaTextureObject_t rtex = 0;
+    cudaSurfaceObject_t rsurf = 0;
+    int rlayers = 0, rnd = 0;
+    bool ratio_texture = true;        /* XR_OPT_RATIO_TEXTURE */
     xr::DevBuf scratch_vol, scratch_sino, scratch_md, stage;
     xr::DevBuf basis_dev;              /* BasisConst                                */
     xr::DevBuf fdk_frames;             /* C*V ViewFrame with the FDK source         */
@@ -192,9 +201,12 @@ cudaError_t launch_forward(const GeomConst &g, const BasisConst *d_basis, const 
 /* Chord-length normaliser: norm = L / (norm + 1e-5) in place, every view. */
 cudaError_t launch_chord(const GeomConst &g, const ViewFrame *frames, float *norm, int n_cond, cudaStream_t s);
 /* Normalise (skipped when norm is null) + ratio (MLEM) or subtract (ART) on
- * listed views of every axis, FP64 loss sum added to *loss. */
+ * listed views of every axis, FP64 loss sum added to *loss.  surf (non-zero):
+ * the ratio images also go to layer (axis * n_views + list position) of that
+ * 2D-layered surface. */
 cudaError_t launch_ratio(const GeomConst &g, const int *view_list, int n_views, int n_cond, float *proj,
-                         const float *norm, const void *sino, int art, double *loss, int storage, cudaStream_t s);
+                         const float *norm, const void *sino, int art, double *loss, int storage, cudaStream_t s,
+                         cudaSurfaceObject_t surf = 0);
 /* Normalise only (proj *= norm) on every view: the forward operator A. */
 cudaError_t launch_normalize(const GeomConst &g, int n_cond, float *proj, const float *norm, cudaStream_t s);
 /* Back-projection of the listed views fused with the MLEM / ART update. */
@@ -226,7 +238,7 @@ cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const
                             const int *view_list, int n_views, const int *d_conds, int n_cond, const int *d_axis_g,
                             const float *d_magsig, const float *proj, void *vol, const float *fac_in, float *fac_out,
                             int mode, int art, float alpha, int storage, cudaStream_t s,
-                            const float *coef = nullptr, int coef_kind = 0);
+                            const float *coef = nullptr, int coef_kind = 0, cudaTextureObject_t rtex = 0);
 
 /* ---- xr_orient.cu ---- */
 /* calcNormalVectorThreeDirec (ir.cu:856-974) on every voxel: vol holds the

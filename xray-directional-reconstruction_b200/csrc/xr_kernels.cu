@@ -407,9 +407,12 @@ __device__ __forceinline__ double block_sum(double x) {
     return s;
 }
 
+/* surf (non-zero): each ratio value is also written to layer blockIdx.y
+ * (axis * n_views + list position) of a 2D-layered array, which the XTT back
+ * kernel gathers from; out-of-range writes are dropped (boundary mode zero). */
 template <typename T>
 __global__ void k_ratio(GeomConst g, const int *view_list, int n_views, float *proj, const float *norm,
-                        const T *sino, int art, double *loss) {
+                        const T *sino, int art, double *loss, cudaSurfaceObject_t surf) {
     const size_t NdNd = (size_t)g.Nd * g.Nd;
     const int cond = blockIdx.y / n_views, j = blockIdx.y % n_views;
     const size_t base = ((size_t)cond * g.V + view_list[j]) * NdNd;
@@ -426,6 +429,10 @@ __global__ void k_ratio(GeomConst g, const int *view_list, int n_views, float *p
             if (p > 2.0f) p = 2.0f;
         }
         proj[idx] = p;
+        if (surf) {
+            const int iy = (int)(i / (unsigned)g.Nd), ix = (int)(i - (size_t)iy * g.Nd);
+            surf2DLayeredwrite(p, surf, ix * (int)sizeof(float), iy, (int)blockIdx.y, cudaBoundaryModeZero);
+        }
     }
     const double s = block_sum(acc);
     if (threadIdx.x == 0 && loss) atomicAdd(loss, s);
@@ -693,18 +700,19 @@ cudaError_t launch_chord(const GeomConst &g, const ViewFrame *frames, float *nor
 }
 
 cudaError_t launch_ratio(const GeomConst &g, const int *view_list, int n_views, int n_cond, float *proj,
-                         const float *norm, const void *sino, int art, double *loss, int storage, cudaStream_t s) {
+                         const float *norm, const void *sino, int art, double *loss, int storage, cudaStream_t s,
+                         cudaSurfaceObject_t surf) {
     if (n_views <= 0) return cudaSuccess;
     const size_t NdNd = (size_t)g.Nd * g.Nd;
     int bx = (int)((NdNd + 255) / 256);
     if (bx > 64) bx = 64;
     const dim3 grid(bx, (unsigned)(n_views * n_cond));
     if (storage == kBF16)
-        k_ratio<<<grid, 256, 0, s>>>(g, view_list, n_views, proj, norm, (const __nv_bfloat16 *)sino, art, loss);
+        k_ratio<<<grid, 256, 0, s>>>(g, view_list, n_views, proj, norm, (const __nv_bfloat16 *)sino, art, loss, surf);
     else if (storage == kF16)
-        k_ratio<<<grid, 256, 0, s>>>(g, view_list, n_views, proj, norm, (const __half *)sino, art, loss);
+        k_ratio<<<grid, 256, 0, s>>>(g, view_list, n_views, proj, norm, (const __half *)sino, art, loss, surf);
     else
-        k_ratio<<<grid, 256, 0, s>>>(g, view_list, n_views, proj, norm, (const float *)sino, art, loss);
+        k_ratio<<<grid, 256, 0, s>>>(g, view_list, n_views, proj, norm, (const float *)sino, art, loss, surf);
     return cudaGetLastError();
 }
 
