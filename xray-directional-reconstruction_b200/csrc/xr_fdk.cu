@@ -11,7 +11,8 @@
  *   k_fdk_bp      one thread per voxel loops over all views, gathering the
  *                 bilinear taps and adding (sod/(sod+o_y))^2 * (2 pi/V) * tap
  *                 sum in the reference's view order (fdk.cu:62-170), one store
- *                 per voxel.
+ *                 per voxel; k_fdk_bp_col is the same for axes that rotate
+ *                 about a grid axis, with the ray set-up once per voxel column.
  * FP32 operations on the per-voxel path are explicitly rounded (no FMA
  * contraction), matching the reference's arithmetic.
  */
@@ -134,11 +135,138 @@ __global__ void __launch_bounds__(kBpThreads) k_fdk_bp(BpArgs a) {
     if (ok) a.vol[(size_t)a.cond * N * N * N + (size_t)x + (size_t)N * y + (size_t)N * N * z] = acc;
 }
 
+/* a / det, correctly rounded (one Markstein correction step with
+ * rdet = RN(1/det), checked bit for bit against IEEE division on this device
+ * when g.exact_rdet is set; else IEEE division). */
+__device__ __forceinline__ float fdk_div_det(float a, const GeomConst &g) {
+    if (!g.exact_rdet) return __fdiv_rn(a, g.det);
+    const float q = __fmul_rn(a, g.rdet);
+    const float r = __fmaf_rn(-q, g.det, a);
+    return __fmaf_rn(r, g.rdet, q);
+}
+
+template <int G>
+struct FdkAx {
+    static constexpr int A = (G == 0) ? 1 : 0;   /* the two other axes, ascending */
+    static constexpr int B = (G == 2) ? 1 : 2;
+};
+
+struct BpColArgs {
+    BpArgs b;
+    float magsig;              /* ev[G] * mag (ev = +-e_G for every view) */
+    int nbg, nba;              /* bricks of 16 along G and of 8 along A  */
+};
+
+/* The same back-projection for an axis whose every view has ev = +-e_G,
+ * src_G = eu_G = 0 and the same off_G and t_G (checked on the host): along
+ * a voxel column parallel to G the ray set-up (coeff, u and, unless G is y,
+ * the weight (sod / (sod + o_y))^2 * 2 pi / V) is the same bit for bit (the
+ * dropped terms of the three-term dot products are exact zeros), so a thread
+ * computes it once per view for its 4 voxels along G and per voxel only
+ * v = ((coeff * o_G) * ev_G mag) / det + Nd/2, the taps and the gather.  Each
+ * voxel still adds its views in order: the result equals k_fdk_bp's.
+ * Brick: 16 along G x 8 x 8, 256 threads = 64 columns x 4 segments. */
+template <int G>
+__global__ void __launch_bounds__(kBpThreads, 4) k_fdk_bp_col(BpColArgs c) {
+    __shared__ ViewFrame fr[kFrameChunk];
+    constexpr int A = FdkAx<G>::A, B = FdkAx<G>::B;
+    const BpArgs &a = c.b;
+    const GeomConst &g = a.g;
+    const int N = g.N, Nd = g.Nd;
+    const int b = blockIdx.x;
+    const int g0 = (b % c.nbg) * 16, a0 = ((b / c.nbg) % c.nba) * 8, b0 = (b / (c.nbg * c.nba)) * 8;
+    const int tid = threadIdx.x;
+    const int ia = a0 + (tid & 7), ib = b0 + ((tid >> 3) & 7), igb = g0 + (tid >> 6) * 4;
+    const bool col_ok = ia < N && ib < N;
+    const float ba = vox_base_fdk(ia, N, g.vs), bb = vox_base_fdk(ib, N, g.vs);
+    const size_t NdNd = (size_t)Nd * Nd;
+    const float *P = a.filt_sino + (size_t)a.src_block * g.V * NdNd;
+    const float Cw = __fdiv_rn(__fmul_rn(2.0f, (float)M_PI), (float)g.V);
+    float dg[4], acc[4] = {0.f, 0.f, 0.f, 0.f};
+    bool okv[4];
+    {
+        const ViewFrame &f0 = a.frames[(size_t)a.cond * g.V];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            okv[q] = col_ok && igb + q < N;
+            dg[q] = __fsub_rn(__fsub_rn(vox_base_fdk(igb + q, N, g.vs), f0.off[G]), f0.t[G]);
+        }
+    }
+    for (int c0 = 0; c0 < g.V; c0 += kFrameChunk) {
+        const int nc = min(kFrameChunk, g.V - c0);
+        __syncthreads();
+        for (int i = tid; i < nc * 5; i += kBpThreads) {
+            const int jj = i / 5, q = i % 5;
+            reinterpret_cast<float4 *>(&fr[jj])[q] =
+                reinterpret_cast<const float4 *>(&a.frames[(size_t)a.cond * g.V + c0 + jj])[q];
+        }
+        __syncthreads();
+        if (!col_ok) continue;
+        for (int jj = 0; jj < nc; jj++) {
+            const ViewFrame &f = fr[jj];
+            const float oa = __fsub_rn(__fsub_rn(ba, f.off[A]), f.t[A]);
+            const float ob = __fsub_rn(__fsub_rn(bb, f.off[B]), f.t[B]);
+            const float da = __fsub_rn(oa, f.src[A]), db = __fsub_rn(ob, f.src[B]);
+            const float coeff = __fdiv_rn(-f.ss, __fadd_rn(__fmul_rn(f.src[A], da), __fmul_rn(f.src[B], db)));
+            const float pa = __fadd_rn(f.src[A], __fmul_rn(coeff, da));
+            const float pb = __fadd_rn(f.src[B], __fmul_rn(coeff, db));
+            const float u = __fadd_rn(
+                fdk_div_det(__fmul_rn(__fadd_rn(__fmul_rn(pa, f.eu[A]), __fmul_rn(pb, f.eu[B])), g.mag), g), g.half);
+            if (!(0.55f < u && u < g.lim)) continue;
+            const float ut = __fsub_rn(u, 0.5f);
+            const float fiu = floorf(ut);
+            const int iu = (int)fiu;
+            const float fu = __fsub_rn(ut, fiu), gu = __fsub_rn(1.0f, fu);
+            /* (sod / (sod + o_y))^2 * 2 pi / V: per column unless y is the column axis */
+            float w = 0.f;
+            if (G != 1) {
+                const float U = __fdiv_rn(g.sod, __fadd_rn(g.sod, A == 1 ? oa : ob));
+                w = __fmul_rn(__fmul_rn(U, U), Cw);
+            }
+            const float *Pc = P + (size_t)f.view * NdNd + iu;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (!okv[q]) continue;
+                const float v = __fadd_rn(fdk_div_det(__fmul_rn(__fmul_rn(coeff, dg[q]), c.magsig), g), g.half);
+                if (!(0.55f < v && v < g.lim)) continue;
+                const float vt = __fsub_rn(v, 0.5f);
+                const float fiv = floorf(vt);
+                const int iv = (int)fiv;
+                const float fv = __fsub_rn(vt, fiv), gv = __fsub_rn(1.0f, fv);
+                const float c1 = __fmul_rn(gu, fv), c2 = __fmul_rn(fu, fv), c3 = __fmul_rn(fu, gv),
+                            c4 = __fmul_rn(gu, gv);
+                const float *pp = Pc + (size_t)Nd * iv;
+                const float p4 = __ldg(pp), p3 = __ldg(pp + 1), p1v = __ldg(pp + Nd), p2v = __ldg(pp + Nd + 1);
+                const float nb = __fadd_rn(
+                    __fadd_rn(__fadd_rn(__fmul_rn(c1, p1v), __fmul_rn(c2, p2v)), __fmul_rn(c3, p3)), __fmul_rn(c4, p4));
+                float wq = w;
+                if (G == 1) {   /* o_y = o_G: per voxel */
+                    const float U = __fdiv_rn(g.sod, __fadd_rn(g.sod, dg[q]));
+                    wq = __fmul_rn(__fmul_rn(U, U), Cw);
+                }
+                acc[q] = __fadd_rn(acc[q], __fmul_rn(wq, nb));
+            }
+        }
+    }
+    if (!col_ok) return;
+    const size_t NN = (size_t)N * N;
+    float *out = a.vol + (size_t)a.cond * NN * N;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (!okv[q]) continue;
+        int cc[3];
+        cc[A] = ia;
+        cc[B] = ib;
+        cc[G] = igb + q;
+        out[(size_t)cc[0] + (size_t)N * cc[1] + NN * cc[2]] = acc[q];
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_cond, const float *sino,
                        float *sino_filt, float *vol, const float *filt, float *weight, int axis_blocks,
-                       cudaStream_t s) {
+                       cudaStream_t s, const int *h_axis_g, const float *h_magsig) {
     {
         const dim3 blk(32, 8), grid((g.Nd + 31) / 32, (g.Nd + 7) / 8);
         k_fdk_weight<<<grid, blk, 0, s>>>(g, weight);
@@ -163,7 +291,20 @@ cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_co
         a.vol = vol;
         a.cond = c;
         a.src_block = axis_blocks ? c : 0;
-        k_fdk_bp<<<(unsigned)nb, kBpThreads, 0, s>>>(a);
+        const int G = h_axis_g ? h_axis_g[c] : -1;
+        if (G < 0) {
+            k_fdk_bp<<<(unsigned)nb, kBpThreads, 0, s>>>(a);
+            continue;
+        }
+        BpColArgs cb;
+        cb.b = a;
+        cb.magsig = h_magsig[c];
+        cb.nbg = (g.N + 15) / 16;
+        cb.nba = (g.N + 7) / 8;
+        const unsigned nbc = (unsigned)((long)cb.nbg * cb.nba * ((g.N + 7) / 8));
+        if (G == 0) k_fdk_bp_col<0><<<nbc, kBpThreads, 0, s>>>(cb);
+        else if (G == 1) k_fdk_bp_col<1><<<nbc, kBpThreads, 0, s>>>(cb);
+        else k_fdk_bp_col<2><<<nbc, kBpThreads, 0, s>>>(cb);
     }
     return cudaGetLastError();
 }

@@ -1788,6 +1788,13 @@ xr_status xr_fdk_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
         if ((st = ensure(c, x.fdk_frames, h.size() * sizeof(ViewFrame), "fdk frames"))) return st;
         cudaMemcpy(x.fdk_frames.p, h.data(), h.size() * sizeof(ViewFrame), cudaMemcpyHostToDevice);
         x.fdk_rotation = rotation;
+        x.fdk_axis_g.assign(c->C, -1);
+        x.fdk_magsig.assign(c->C, 0.f);
+        for (int cond = 0; cond < c->C; cond++) {
+            float sg = 0.f;
+            x.fdk_axis_g[cond] = aligned_axis(h, cond, c->V, &sg);
+            x.fdk_magsig[cond] = sg * c->gc.mag;
+        }
     }
     /* filter table, reconstruct.cu:1694-1698 (or Ram-Lak in the same scaling) */
     std::vector<float> filt(c->Nd);
@@ -1812,7 +1819,8 @@ xr_status xr_fdk_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
         st = cuda_check(c, launch_fdk(c->gc, (const ViewFrame *)x.fdk_frames.p, c->C,
                                       (const float *)c->scratch_sino.p, (float *)x.fdk_sf.p,
                                       (float *)c->scratch_vol.p, (const float *)x.fdk_filt.p,
-                                      (float *)x.fdk_weight.p, c->fdk_axis_blocks, c->stream), "fdk");
+                                      (float *)x.fdk_weight.p, c->fdk_axis_blocks, c->stream,
+                                      x.fdk_axis_g.data(), x.fdk_magsig.data()), "fdk");
     }
     if (st) return st;
     if ((st = download_planes(c, (const float *)c->scratch_vol.p, voxel, c->C, N3, "volume"))) return st;

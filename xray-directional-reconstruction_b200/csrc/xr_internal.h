@@ -123,6 +123,8 @@ struct xr_ctx {
     std::vector<int> load_index;
 
     int fdk_axis_blocks = 0;
+    std::vector<int> fdk_axis_g;       /* per axis: column axis of the FDK frames, -1 general */
+    std::vector<float> fdk_magsig;     /* per axis: ev[g] * mag of the FDK frames */
     int views_per_cta = 0;
     int storage = 0;
     int sino_storage = -1;            /* -1: same as storage */
@@ -285,9 +287,11 @@ cudaError_t launch_fiber_back(const GeomConst &g, const ViewFrame *frames, const
                               int art, float alpha, int *d_nonfinite, cudaStream_t s);
 
 /* ---- xr_fdk.cu ---- */
+/* h_axis_g / h_magsig (host arrays, may be null): per axis the column axis of
+ * its FDK frames (-1: general) and ev[g] * mag. */
 cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_cond, const float *sino,
                        float *sino_filt, float *vol, const float *filt, float *weight, int axis_blocks,
-                       cudaStream_t s);
+                       cudaStream_t s, const int *h_axis_g = nullptr, const float *h_magsig = nullptr);
 
 }  // namespace xr
 
