@@ -470,6 +470,7 @@ struct BackColArgs {
     const float *coef;        /* non-null: per-voxel rotated basis (backwardOrth) */
     int coef_kind;            /* 0: (phi, cos theta); 1: main direction            */
     cudaTextureObject_t rtex; /* B_XTT_TEX: the ratio images, layer = axis * n_views + position */
+    int brick0;               /* first brick of the launch (z-slab launches)  */
 };
 
 /* Shared-memory slot of brick voxel lv (x + 8y + 64z) in the per-voxel
@@ -724,7 +725,7 @@ __global__ void __launch_bounds__(kBackThreads, 6) k_back_col(BackColArgs a) {
     const GeomConst &g = a.g;
     const int N = g.N;
     const int nb8 = (N + 7) / 8;
-    const int b = blockIdx.x;
+    const int b = blockIdx.x + a.brick0;
     const int bx0 = (b % nb8) * 8, by0 = ((b / nb8) % nb8) * 8, bz0 = (b / (nb8 * nb8)) * 8;
     const int tid = threadIdx.x;
     const int K = g.K;
@@ -887,7 +888,7 @@ cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const
                             const int *view_list, int n_views, const int *d_conds, int n_cond, const int *d_axis_g,
                             const float *d_magsig, const float *proj, void *vol, const float *fac_in, float *fac_out,
                             int mode, int art, float alpha, int storage, cudaStream_t s, const float *coef,
-                            int coef_kind, cudaTextureObject_t rtex) {
+                            int coef_kind, cudaTextureObject_t rtex, int zb0, int zb1) {
     BackColArgs a;
     a.rtex = rtex;
     if (mode == B_XTT && rtex) mode = B_XTT_TEX;
@@ -911,7 +912,11 @@ cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const
     a.art = art;
     a.alpha = alpha;
     const int nb8 = (g.N + 7) / 8;
-    const unsigned blocks = (unsigned)((long)nb8 * nb8 * nb8);
+    if (zb1 < 0 || zb1 > nb8) zb1 = nb8;
+    if (zb0 < 0) zb0 = 0;
+    if (zb0 >= zb1) return cudaSuccess;
+    a.brick0 = zb0 * nb8 * nb8;
+    const unsigned blocks = (unsigned)((long)nb8 * nb8 * (zb1 - zb0));
     const size_t smem = (mode == B_PLAIN) ? 0 : (size_t)g.K * 512 * sizeof(float);
 #define XR_BACK_COL(M, TT)                                                                                        \
     do {                                                                                                          \

@@ -477,6 +477,35 @@ static bool floats(const JVal *v, std::vector<float> &out) {
     return true;
 }
 
+/* Host-call tail, after the last update of z-planes [z0, z1): voxelSqrt of
+ * those planes of every channel, their orientation, and the downloads of
+ * the slab's volume and orientation planes on the copy stream (session
+ * fields vol_dst / md_dst / ev_dst, FP32 storage). */
+static cudaError_t tail_slab(xr_ctx *c, int z0, int z1, int i) {
+    Session &s = c->sess;
+    cudaStream_t str = c->stream, cs = c->copy_stream;
+    const size_t NN = (size_t)c->N * c->N, N3 = NN * c->N, n = (size_t)(z1 - z0) * NN, o = (size_t)z0 * NN;
+    float *vol = (float *)s.d_vol;
+    cudaError_t e = cudaSuccess;
+    if (c->xtt_sqrt)   /* reconstruct.cu:919-922 */
+        for (int k = 0; k < c->K && e == cudaSuccess; k++) e = launch_sqrt_abs((long)n, vol + k * N3 + o, 0, str);
+    if (e == cudaSuccess) e = cudaEventRecord(c->slab_ev[i], str);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, c->slab_ev[i], 0);
+    for (int k = 0; k < c->K && e == cudaSuccess; k++)
+        e = cudaMemcpyAsync(s.vol_dst[k] + o, vol + k * N3 + o, n * sizeof(float), cudaMemcpyDeviceToHost, cs);
+    if (e != cudaSuccess || !s.tail_md) return e;
+    e = launch_orientation_range((long)N3, (long)o, (long)(o + n), c->K, dbasis(c), vol, s.tail_md, s.tail_ev, 0, str);
+    if (e == cudaSuccess) e = cudaEventRecord(c->tail_ev[i], str);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, c->tail_ev[i], 0);
+    for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+        e = cudaMemcpyAsync(s.md_dst[k] + o, s.tail_md + k * N3 + o, n * sizeof(float), cudaMemcpyDeviceToHost, cs);
+        if (e == cudaSuccess && s.tail_ev && s.ev_dst)
+            e = cudaMemcpyAsync(s.ev_dst[k] + o, s.tail_ev + k * N3 + o, n * sizeof(float), cudaMemcpyDeviceToHost,
+                                cs);
+    }
+    return e;
+}
+
 /* Enqueue one epoch's device work on the context stream for the given
  * subset orders (XTT: one row; IR: one row per axis). */
 static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
@@ -575,9 +604,19 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                     const ColInfo *ci = dcol(c);
                     const float *sens =
                         s.art ? nullptr : (const float *)c->sens.p + (size_t)orders[b] * c->K * N3;
-                    e = launch_back_col(c->gc, dbasis(c), fr, vl, s.subset_size, ci->all, c->C, ci->axis_g,
-                                        ci->magsig, proj, s.d_vol, sens, nullptr, 1, s.art, alpha, s.update_storage,
-                                        str, s.coef, s.coef_kind, s.rtex ? c->rtex : 0);
+                    const bool tail = s.tail_slabs > 0 && b == s.batch - 1;
+                    const int nb8 = (c->N + 7) / 8, S = tail ? s.tail_slabs : 1, zbs = (nb8 + S - 1) / S;
+                    e = cudaSuccess;
+                    for (int i = 0; i < S && e == cudaSuccess; i++) {
+                        const int zb0 = i * zbs, zb1 = tail ? std::min(nb8, zb0 + zbs) : -1;
+                        if (tail && zb0 >= zb1) break;
+                        e = launch_back_col(c->gc, dbasis(c), fr, vl, s.subset_size, ci->all, c->C, ci->axis_g,
+                                            ci->magsig, proj, s.d_vol, sens, nullptr, 1, s.art, alpha,
+                                            s.update_storage, str, s.coef, s.coef_kind, s.rtex ? c->rtex : 0, zb0,
+                                            zb1);
+                        if (e == cudaSuccess && tail) e = tail_slab(c, zb0 * 8, std::min(c->N, zb1 * 8), i);
+                    }
+                    if (tail && e == cudaSuccess) s.tail_done = true;
                 } else {
                     e = launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, 0, c->C, proj, s.d_vol, 1, s.art,
                                            alpha, s.update_storage, str, s.coef, s.coef_kind);
@@ -839,6 +878,8 @@ void xr_destroy(xr_ctx *c) {
     for (cudaEvent_t e : c->copy_ev)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : c->slab_ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->tail_ev)
         if (e) cudaEventDestroy(e);
     delete c;
 }
@@ -1158,7 +1199,7 @@ static xr_status session_end_impl(xr_ctx *c, float *d_md, float *d_ev,
     Session &s = c->sess;
     if (!s.active) return fail(c, XR_ERR_STATE, "no active session");
     xr_status st = XR_OK;
-    if (s.xtt && !s.fiber) {
+    if (s.xtt && !s.fiber && !s.tail_done) {
         const long nvox = (long)c->N * c->N * c->N;
         if (c->xtt_sqrt) {
             Timed t(c, XR_T_ORIENT);
@@ -1483,6 +1524,9 @@ static xr_status ensure_copy_stream(xr_ctx *c) {
     for (cudaEvent_t &e : c->slab_ev)
         if (!e && (st = cuda_check(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")))
             return st;
+    for (cudaEvent_t &e : c->tail_ev)
+        if (!e && (st = cuda_check(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")))
+            return st;
     return XR_OK;
 }
 
@@ -1644,22 +1688,34 @@ xr_status xr_xtt_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
         xr_dev_session_end(c, nullptr, nullptr);
         return st;
     }
-    /* the last epoch hands each view's final ratio image to the copy stream
-     * as soon as its subset is done (not inside a captured epoch graph) */
-    const bool early = !c->use_graphs && epoch > 0;
-    for (int ep = 0; ep < epoch; ep++) {
-        double l = 0;
-        if (early && ep == epoch - 1) c->sess.ratio_dst = sino;
-        st = xr_dev_session_epoch(c, losses ? &l : nullptr);
-        c->sess.ratio_dst = nullptr;
-        if (st) return st;
-        if (losses) losses[ep] = (float)l;
-    }
     float *d_md = nullptr, *d_ev = nullptr;
     if (md) {
         if ((st = ensure(c, c->scratch_md, 6 * N3 * sizeof(float), "orientation"))) return st;
         d_md = (float *)c->scratch_md.p;
         d_ev = evalue ? d_md + 3 * N3 : nullptr;
+    }
+    /* the last epoch hands each view's final ratio image to the copy stream
+     * as soon as its subset is done (not inside a captured epoch graph); with
+     * staged transfers its last back-projection also runs by z-slabs, each
+     * slab's voxelSqrt, orientation and downloads following at once */
+    const bool early = !c->use_graphs && epoch > 0;
+    for (int ep = 0; ep < epoch; ep++) {
+        double l = 0;
+        Session &s = c->sess;
+        if (early && ep == epoch - 1) s.ratio_dst = sino;
+        if (staged && ep == epoch - 1 && c->all_aligned) {
+            s.tail_slabs = xr_ctx::kSlabs;
+            s.vol_dst = voxel;
+            s.md_dst = md;
+            s.ev_dst = evalue;
+            s.tail_md = d_md;
+            s.tail_ev = d_ev;
+        }
+        st = xr_dev_session_epoch(c, losses ? &l : nullptr);
+        s.ratio_dst = nullptr;
+        s.tail_slabs = 0;
+        if (st) return st;
+        if (losses) losses[ep] = (float)l;
     }
     if (!early) {   /* the ratio images are final after the last epoch */
         if ((st = stream_after(c, cs, c->stream, c->copy_ev[0]))) return st;

@@ -99,6 +99,17 @@ struct Session {
     cudaEvent_t sino_rest = nullptr;  /* set: the second ratio launch waits for it (rest of the sinogram) */
     int vol_slabs = 0;                /* > 0: the first forward runs by z-slabs, each after its upload event */
     bool rtex = false;                /* XTT column session: ratio images through the layered texture */
+    /* Host-call tail: when tail_slabs > 0, the last subset of the next epoch
+     * back-projects by z-slabs and each slab is then voxelSqrt'ed, its
+     * orientation computed into tail_md / tail_ev (may be null) and its
+     * volume and orientation planes downloaded to vol_dst / md_dst / ev_dst
+     * on the copy stream while the next slab runs; tail_done records it. */
+    int tail_slabs = 0;
+    float *const *vol_dst = nullptr;
+    float *const *md_dst = nullptr;
+    float *const *ev_dst = nullptr;
+    float *tail_md = nullptr, *tail_ev = nullptr;
+    bool tail_done = false;
     const cudaEvent_t *slab_ev = nullptr;
     float *const *ratio_dst = nullptr; /* set: each view's final ratio image to these host planes */
     std::vector<int> order;            /* persistent subset order (XTT)     */
@@ -161,8 +172,9 @@ struct xr_ctx {
     xr::DevBuf fdk_filt, fdk_weight, fdk_sf;
     bool dev_ready = false;
     double *h_loss = nullptr;          /* pinned, kLossSlots doubles                */
-    static constexpr int kSlabs = 8;   /* host-call volume upload in z-slabs */
+    static constexpr int kSlabs = 8;   /* host-call volume upload and final download in z-slabs */
     cudaEvent_t slab_ev[kSlabs] = {};
+    cudaEvent_t tail_ev[kSlabs] = {};  /* final download: a slab's orientation is done */
     int sens_batch = 0, sens_rotation = 0; /* the sensitivity buffer holds these subsets (0: nothing) */
     int static_rdet = -1;              /* xr_dev_forward_proj_only_static: its own
                                           result of the division check (-1: not run) */
@@ -235,12 +247,14 @@ cudaError_t launch_forward_col(const GeomConst &g, const BasisConst *d_basis, co
                                int storage, cudaStream_t s, const float *coef = nullptr, int coef_kind = 0,
                                int zlo = 0, int zhi = 1 << 30, const int *d_axis_g = nullptr);
 /* mode 0: plain (one axis, update in place); 1: XTT (fac_in = sensitivity);
- * 2: sensitivity of the listed views into fac_out. */
+ * 2: sensitivity of the listed views into fac_out.  zb0, zb1: only the
+ * bricks of 8 z-planes numbered [zb0, zb1) (zb1 = -1: to the last). */
 cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const ViewFrame *frames,
                             const int *view_list, int n_views, const int *d_conds, int n_cond, const int *d_axis_g,
                             const float *d_magsig, const float *proj, void *vol, const float *fac_in, float *fac_out,
                             int mode, int art, float alpha, int storage, cudaStream_t s,
-                            const float *coef = nullptr, int coef_kind = 0, cudaTextureObject_t rtex = 0);
+                            const float *coef = nullptr, int coef_kind = 0, cudaTextureObject_t rtex = 0,
+                            int zb0 = 0, int zb1 = -1);
 
 /* ---- xr_orient.cu ---- */
 /* calcNormalVectorThreeDirec (ir.cu:856-974) on every voxel: vol holds the
@@ -264,6 +278,9 @@ cudaError_t launch_update_estimation_coef(long nvox, const BasisConst *d_basis, 
                                           cudaStream_t s);
 cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, const void *mu, float *md,
                                float *ev, int storage, cudaStream_t s);
+/* The same for voxels [i0, i1) of volumes with channel stride nvox. */
+cudaError_t launch_orientation_range(long nvox, long i0, long i1, int K, const BasisConst *d_basis, const void *mu,
+                                     float *md, float *ev, int storage, cudaStream_t s);
 cudaError_t launch_angle_from_md(long nvox, const float *md, float *angle, cudaStream_t s);
 cudaError_t launch_direction_normalization(long nvox, float *md, cudaStream_t s);
 

@@ -21,8 +21,9 @@ namespace xr {
 namespace {
 
 template <typename TS>
-__global__ void k_orientation(long nvox, int K, const BasisConst *B, const TS *mu, float *md, float *ev) {
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nvox; i += (long)gridDim.x * blockDim.x) {
+__global__ void k_orientation(long nvox, long i0, long i1, int K, const BasisConst *B, const TS *mu, float *md,
+                              float *ev) {
+    for (long i = i0 + (long)blockIdx.x * blockDim.x + threadIdx.x; i < i1; i += (long)gridDim.x * blockDim.x) {
         double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, mean = 0.0;
         for (int k = 0; k < K; k++) {
             const double m = (double)ldgf<TS>(mu + (long)k * nvox + i);
@@ -323,13 +324,24 @@ int grid_for(long n, int threads) {
 
 }  // namespace
 
+cudaError_t launch_orientation_range(long nvox, long i0, long i1, int K, const BasisConst *d_basis, const void *mu,
+                                     float *md, float *ev, int storage, cudaStream_t s) {
+    if (i0 < 0) i0 = 0;
+    if (i1 > nvox) i1 = nvox;
+    if (i1 <= i0) return cudaSuccess;
+    const int gr = grid_for(i1 - i0, 128);
+    if (storage == kBF16)
+        k_orientation<<<gr, 128, 0, s>>>(nvox, i0, i1, K, d_basis, (const __nv_bfloat16 *)mu, md, ev);
+    else if (storage == kF16)
+        k_orientation<<<gr, 128, 0, s>>>(nvox, i0, i1, K, d_basis, (const __half *)mu, md, ev);
+    else
+        k_orientation<<<gr, 128, 0, s>>>(nvox, i0, i1, K, d_basis, (const float *)mu, md, ev);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_orientation(long nvox, int K, const BasisConst *d_basis, const void *mu, float *md, float *ev,
                                int storage, cudaStream_t s) {
-    const int gr = grid_for(nvox, 128);
-    if (storage == kBF16) k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const __nv_bfloat16 *)mu, md, ev);
-    else if (storage == kF16) k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const __half *)mu, md, ev);
-    else k_orientation<<<gr, 128, 0, s>>>(nvox, K, d_basis, (const float *)mu, md, ev);
-    return cudaGetLastError();
+    return launch_orientation_range(nvox, 0, nvox, K, d_basis, mu, md, ev, storage, s);
 }
 
 cudaError_t launch_md_filter(int N, const float *md, float *out, float coef, cudaStream_t s) {
