@@ -138,14 +138,17 @@ class Scan:
 
     def osem(self, b, vol, epochs: int, batch: int = 5, storage: int = 0, sino_storage: int = -1,
              residual_every: int = 0, target: float = 0.0, max_epochs: int = 0, graphs: bool = False,
-             final_sqrt: bool = True):
+             final_sqrt: bool = True, fine_within: float = 0.05):
         """OS-EM (XTT MLEM) epochs on the device volume `vol` in place (b and
         vol of the given storage types).  With residual_every > 0, runs until
-        the relative data residual <= target or max_epochs.  final_sqrt: end
-        like the reference's XTT::reconstruct (voxelSqrt of the result), else
-        leave the iterate.  Returns (epochs run, device milliseconds of
-        session set-up + epochs, residual trace [(epoch, ms, residual)]);
-        residual checks are not timed."""
+        the relative data residual <= target or max_epochs, checking it every
+        residual_every epochs and after every epoch once it is within
+        fine_within (relative) of the target, so the epoch that reaches the
+        target is found exactly.  final_sqrt: end like the reference's
+        XTT::reconstruct (voxelSqrt of the result), else leave the iterate.
+        Returns (epochs run, device milliseconds of session set-up + epochs,
+        residual trace [(epoch, ms, residual)]); residual checks are not
+        timed."""
         import torch
         xr = self.xr
         self.ctx.set_option(xr.Option.XTT_SQRT, 1 if final_sqrt else 0)
@@ -159,8 +162,9 @@ class Scan:
         self.ctx.dev_session_begin(b.data_ptr(), vol.data_ptr(), True, total, batch)
         ms, trace, e = 0.0, [], 0
         first = True
+        step = residual_every
         while e < total:
-            n = min(residual_every, total - e) if residual_every else total
+            n = min(step, total - e) if residual_every else total
             if not first:
                 e0.record(self.stream)
             first = False
@@ -175,6 +179,8 @@ class Scan:
                 trace.append((e, ms, r))
                 if r <= target:
                     break
+                if r <= target * (1.0 + fine_within):
+                    step = 1
         self.ctx.dev_session_end(0, 0)
         self.ctx.set_option(xr.Option.STORAGE, 0)
         self.ctx.set_option(xr.Option.SINO_STORAGE, -1)
