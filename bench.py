@@ -1025,7 +1025,7 @@ def main():
     if fwd_ms >= back_ms:
         dom, dom_ms, dom_n, units = "k_fwd_col<1,g,float>", fwd_ms, fwd_n * n_groups, C * subset // n_groups
     else:
-        dom, dom_ms, dom_n, units = "k_back_col<1,float>", back_ms, back_n, C * subset
+        dom, dom_ms, dom_n, units = "k_back_col<3,float>", back_ms, back_n, C * subset
     peak, peak_kind = measured_peaks()
     avg_launch_s = dom_ms / max(dom_n, 1) / 1e3
     # compulsory DRAM bytes of one launch: the forward reads the volume once and
