@@ -120,11 +120,12 @@ enum {
                                   bricks of 16 x 16 x 8 voxels (N < 192), where
                                   the per-axis launches would have to split the
                                   views of a subset over CTAs to fill the GPU   */
-    XR_OPT_RATIO_TEXTURE = 10  /* 1 (default): XTT sessions whose axes are all
-                                  column-aligned keep the subset's ratio images
-                                  in a 2D-layered CUDA array as well, and the
-                                  back-projection gathers each voxel's 4 taps
-                                  with one texture instruction; 0: it loads
+    XR_OPT_RATIO_TEXTURE = 10  /* 1 (default): sessions keep the subset's ratio
+                                  images in a 2D-layered CUDA array as well (XTT
+                                  sessions whose axes are all column-aligned; IR
+                                  sessions for each column-aligned axis), and
+                                  the back-projection gathers each voxel's 4
+                                  taps with one texture instruction; 0: it loads
                                   them from the linear images                    */
 };
 

@@ -87,12 +87,15 @@ def test_forward_large_footprint_fallback(oracle):
     assert rel_err(got, ref) <= TOL
 
 
+@pytest.mark.parametrize("ratio_texture", [1, 0], ids=["texture_gather", "linear_loads"])
 @pytest.mark.parametrize("method", ["MLEM", "ART"])
-def test_ir_reconstruct_small(oracle, method):
+def test_ir_reconstruct_small(oracle, method, ratio_texture):
     """a6, a7, a9, a11: IR::reconstruct, 2 axes reconstructed independently,
-    V % batch != 0 (the subset wrap-around revisits views)."""
+    V % batch != 0 (the subset wrap-around revisits views); the back-projection
+    gathering its taps from the layered ratio texture or loading them."""
     xr = load_xr()
     s, ctx = make(24, 36, 14, C=2, seed=7)
+    ctx.set_option(xr.Option.RATIO_TEXTURE, ratio_texture)
     truth = ellipsoid_phantom(s.N, 5, 8)
     b = oracle.forward_all(s, truth, 0, False)
     v0 = np.ones((s.C, s.N, s.N, s.N), np.float32)

@@ -435,9 +435,12 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col_axes(FwdColArgs a) {
 /*   SENS:  moments sum(1), sum(d d^T / d.d) folded into factor_k, written    */
 /*          to global (geometry only; once per subset).                       */
 /* ------------------------------------------------------------------------ */
-/* B_XTT_TEX: B_XTT with the 4 taps of each voxel-view gathered in one
- * texture instruction from the subset's ratio images in a 2D-layered array. */
-enum { B_PLAIN = 0, B_XTT = 1, B_SENS = 2, B_XTT_TEX = 3 };
+/* B_XTT_TEX / B_PLAIN_TEX: B_XTT / B_PLAIN with the 4 taps of each
+ * voxel-view gathered in one texture instruction from the subset's ratio
+ * images in a 2D-layered array. */
+enum { B_PLAIN = 0, B_XTT = 1, B_SENS = 2, B_XTT_TEX = 3, B_PLAIN_TEX = 4 };
+__host__ __device__ constexpr bool b_plain(int m) { return m == B_PLAIN || m == B_PLAIN_TEX; }
+__host__ __device__ constexpr bool b_tex(int m) { return m == B_XTT_TEX || m == B_PLAIN_TEX; }
 
 /* The 2 x 2 texels around unnormalised coordinates (x, y) of layer `layer`
  * (tld4, component r): (T[y1][x0], T[y1][x1], T[y0][x1], T[y0][x0]) with
@@ -469,7 +472,7 @@ struct BackColArgs {
     int sr;                   /* 16-bit volumes: stochastic rounding of updates */
     const float *coef;        /* non-null: per-voxel rotated basis (backwardOrth) */
     int coef_kind;            /* 0: (phi, cos theta); 1: main direction            */
-    cudaTextureObject_t rtex; /* B_XTT_TEX: the ratio images, layer = axis * n_views + position */
+    cudaTextureObject_t rtex; /* *_TEX: the ratio images, layer = (index in conds) * n_views + position */
     int brick0;               /* first brick of the launch (z-slab launches)  */
 };
 
@@ -521,7 +524,7 @@ __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f
         const float2 fi = make_float2(floorf(ut.x), floorf(ut.y));
         fv[p] = __ffma2_rn(fi, bc2(-1.0f), ut);
         gv[p] = __ffma2_rn(fv[p], bc2(-1.0f), bc2(1.0f));
-        if (MODE == B_XTT_TEX) {
+        if (b_tex(MODE)) {
             const float4 t0 = gather_a2d(rtex, layer, xu, fi.x + 1.0f);
             const float4 t1 = gather_a2d(rtex, layer, xu, fi.y + 1.0f);
             p0[p] = make_float2(t0.w, t1.w);
@@ -552,7 +555,7 @@ __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f
                             __fmul2_rn(c4, p0[p]));
             nb = __fmul2_rn(nb, m);
         }
-        if (MODE == B_PLAIN) {
+        if (b_plain(MODE)) {
             acc[p][0] = __fadd2_rn(acc[p][0], nb);   /* tmp    (ir.cu:1750) */
             acc[p][1] = __fadd2_rn(acc[p][1], m);    /* factor (ir.cu:1749) */
         } else {
@@ -584,8 +587,8 @@ __device__ __forceinline__ void back_view(const GeomConst &g, const ViewFrame &f
  * PLAIN updates the voxels in place, XTT/SENS fold into the shared per-voxel
  * channel accumulators. */
 template <int MODE, int G, typename T>
-__device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, float *sacc, int cond, int bx0,
-                                          int by0, int bz0) {
+__device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, float *sacc, int ci, int cond,
+                                          int bx0, int by0, int bz0) {
     constexpr int A = Ax<G>::A, B = Ax<G>::B;
     const GeomConst &g = a.g;
     const int N = g.N, K = g.K, Nd = g.Nd;
@@ -632,10 +635,10 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
         if (nq > 0)
             for (int jj = 0; jj < nc; jj++)
                 back_view<MODE, G>(g, fr[jj], magsig, ba, bb, dg, okq, P + (size_t)fr[jj].view * NdNd, acc, a.rtex,
-                                   cond * a.n_views + c0 + jj);
+                                   ci * a.n_views + c0 + jj);
     }
     if (!col_ok) return;
-    if (MODE != B_PLAIN) {
+    if (!b_plain(MODE)) {
         /* column-frame sums (wgt da^2, wgt db^2, wgt da db, wgt da, wgt db, wgt)
          * -> xyz moments (xx, yy, zz, xy, xz, yz) with d_A = da, d_B = db, d_G = dg */
         constexpr int AB = 3 + A + B - 1, AG = 3 + A + G - 1, BG = 3 + B + G - 1;
@@ -650,7 +653,7 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
             acc[p][BG] = __fmul2_rn(dg[p], c[4]);
         }
     }
-    if (MODE != B_PLAIN && !a.coef) {
+    if (!b_plain(MODE) && !a.coef) {
         /* fold the basis-independent moments into the channels:
          * tmp_k += g_kc (|S_k|^2 sum r - S_k^T (sum r d d^T / d.d) S_k), channel by
          * channel for the thread's 4 voxels at once */
@@ -687,7 +690,7 @@ __device__ __forceinline__ void axis_pass(const BackColArgs &a, ViewFrame *fr, f
         float aq[7];
 #pragma unroll
         for (int e = 0; e < 7; e++) aq[e] = (q & 1) ? acc[q >> 1][e].y : acc[q >> 1][e].x;
-        if (MODE == B_PLAIN) {
+        if (b_plain(MODE)) {
             /* voxelProduct (ir.cu:1637-1654) / voxelPlus (ir.cu:1682-1693) */
             int x, y, z;
             xyz_of<G>(ia, ib, igb + q, x, y, z);
@@ -730,18 +733,18 @@ __global__ void __launch_bounds__(kBackThreads, 6) k_back_col(BackColArgs a) {
     const int tid = threadIdx.x;
     const int K = g.K;
     const size_t NN = (size_t)N * N, N3 = NN * N;
-    if (MODE != B_PLAIN) {
+    if (!b_plain(MODE)) {
         for (int i = tid; i < K * 512; i += kBackThreads) sacc[i] = 0.0f;
     }
     for (int ci = 0; ci < a.n_cond; ci++) {
         const int cond = a.conds[ci];
         const int G = a.axis_g[cond];   /* uniform over the CTA */
-        if (G == 0) axis_pass<MODE, 0, T>(a, fr, sacc, cond, bx0, by0, bz0);
-        else if (G == 1) axis_pass<MODE, 1, T>(a, fr, sacc, cond, bx0, by0, bz0);
-        else axis_pass<MODE, 2, T>(a, fr, sacc, cond, bx0, by0, bz0);
+        if (G == 0) axis_pass<MODE, 0, T>(a, fr, sacc, ci, cond, bx0, by0, bz0);
+        else if (G == 1) axis_pass<MODE, 1, T>(a, fr, sacc, ci, cond, bx0, by0, bz0);
+        else axis_pass<MODE, 2, T>(a, fr, sacc, ci, cond, bx0, by0, bz0);
         __syncthreads();
     }
-    if (MODE == B_PLAIN) return;
+    if (b_plain(MODE)) return;
     /* home layout: brick-linear voxel order */
     for (int lv = tid; lv < 512; lv += kBackThreads) {
         const int x = bx0 + (lv & 7), y = by0 + ((lv >> 3) & 7), z = bz0 + (lv >> 6);
@@ -891,7 +894,8 @@ cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const
                             int coef_kind, cudaTextureObject_t rtex, int zb0, int zb1) {
     BackColArgs a;
     a.rtex = rtex;
-    if (mode == B_XTT && rtex) mode = B_XTT_TEX;
+    if (rtex && mode == B_XTT) mode = B_XTT_TEX;
+    if (rtex && mode == B_PLAIN) mode = B_PLAIN_TEX;
     a.coef = coef;
     a.coef_kind = coef_kind;
     a.sr = (storage & kStoreStochastic) != 0;
@@ -917,7 +921,7 @@ cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const
     if (zb0 >= zb1) return cudaSuccess;
     a.brick0 = zb0 * nb8 * nb8;
     const unsigned blocks = (unsigned)((long)nb8 * nb8 * (zb1 - zb0));
-    const size_t smem = (mode == B_PLAIN) ? 0 : (size_t)g.K * 512 * sizeof(float);
+    const size_t smem = b_plain(mode) ? 0 : (size_t)g.K * 512 * sizeof(float);
 #define XR_BACK_COL(M, TT)                                                                                        \
     do {                                                                                                          \
         cudaError_t e = cudaFuncSetAttribute(k_back_col<M, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
@@ -929,14 +933,17 @@ cudaError_t launch_back_col(const GeomConst &g, const BasisConst *d_basis, const
         XR_BACK_COL(B_SENS, float);
     } else if (storage == kBF16) {
         if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, __nv_bfloat16);
+        else if (mode == B_PLAIN_TEX) XR_BACK_COL(B_PLAIN_TEX, __nv_bfloat16);
         else if (mode == B_XTT_TEX) XR_BACK_COL(B_XTT_TEX, __nv_bfloat16);
         else XR_BACK_COL(B_XTT, __nv_bfloat16);
     } else if (storage == kF16) {
         if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, __half);
+        else if (mode == B_PLAIN_TEX) XR_BACK_COL(B_PLAIN_TEX, __half);
         else if (mode == B_XTT_TEX) XR_BACK_COL(B_XTT_TEX, __half);
         else XR_BACK_COL(B_XTT, __half);
     } else {
         if (mode == B_PLAIN) XR_BACK_COL(B_PLAIN, float);
+        else if (mode == B_PLAIN_TEX) XR_BACK_COL(B_PLAIN_TEX, float);
         else if (mode == B_XTT_TEX) XR_BACK_COL(B_XTT_TEX, float);
         else XR_BACK_COL(B_XTT, float);
     }

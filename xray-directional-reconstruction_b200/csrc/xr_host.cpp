@@ -642,8 +642,10 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                 }
                 {
                     Timed t(c, XR_T_RATIO);
+                    const bool tex = s.rtex && c->axis_g[cond] >= 0;
                     if ((st = cuda_check(c, launch_ratio(c->gc, vl, s.subset_size, 1, pc, norm + (size_t)cond * blk,
-                                                         bc, s.art, dl + cond, s.sino_storage, str), "ratio")))
+                                                         bc, s.art, dl + cond, s.sino_storage, str,
+                                                         tex ? c->rsurf : 0), "ratio")))
                         return st;
                 }
                 {
@@ -653,7 +655,7 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                         const ColInfo *ci = dcol(c);
                         e = launch_back_col(c->gc, dbasis(c), fr, vl, s.subset_size, &ci->all[cond], 1, ci->axis_g,
                                             ci->magsig, proj, vc, nullptr, nullptr, 0, s.art, alpha, s.update_storage,
-                                            str);
+                                            str, nullptr, 0, s.rtex ? c->rtex : 0);
                     } else {
                         e = launch_back_update(c->gc, dbasis(c), fr, vl, s.subset_size, cond, 1, proj, vc, 0, s.art,
                                                alpha, s.update_storage, str);
@@ -1075,8 +1077,9 @@ static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, 
     const size_t npx = (size_t)c->C * c->V * c->Nd * c->Nd;
     if ((st = ensure(c, c->proj, npx * sizeof(float), "projections"))) return st;
     s.rtex = false;
-    if (s.xtt && !fiber && c->all_aligned && c->ratio_texture) {
-        if ((st = ensure_ratio_texture(c, c->C * s.subset_size))) return st;
+    if (!fiber && c->ratio_texture && (s.xtt ? c->all_aligned : true)) {
+        /* XTT: every axis's subset views; IR: one axis at a time */
+        if ((st = ensure_ratio_texture(c, (s.xtt ? c->C : 1) * s.subset_size))) return st;
         s.rtex = c->rtex != 0;
     }
     if (fiber) {
