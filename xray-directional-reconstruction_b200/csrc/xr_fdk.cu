@@ -7,7 +7,7 @@
  *   k_fdk_conv    every view's rows in one launch; a CTA stages one detector
  *                 row of the projection and of the weight in shared memory
  *                 and each thread sums filt[|u-j|] * src[j] * w[j] over j in
- *                 the reference's order (fdk.cu:28-43)
+ *                 the reference's order (fdk.cu:28-43) for 4 outputs at once
  *   k_fdk_bp      one thread per voxel loops over all views, gathering the
  *                 bilinear taps and adding (sod/(sod+o_y))^2 * (2 pi/V) * tap
  *                 sum in the reference's view order (fdk.cu:62-170), one store
@@ -47,26 +47,46 @@ __global__ void k_fdk_weight(GeomConst g, float *w) {
     w[u + g.Nd * v] = __fdiv_rn(g.sdd, __fsqrt_rn(r2));
 }
 
-/* grid (row v, view, axis); dst row = sum_j filt[|u-j|] src[j] w[j]. */
+/* grid (row v, view, axis); dst row = sum_j filt[|u-j|] src[j] w[j], each
+ * output's terms added in j order ((filt * src) * w, fdk.cu:28-43).  A thread
+ * owns 4 consecutive outputs u0..u0+3: per j it reads src[j] and w[j] once
+ * and the filter as a window sliding over the mirrored table
+ * fs[Nd - 1 + k] = filt[|k|], so each j costs one new filter value. */
+constexpr int kConvOut = 4;
+
 __global__ void k_fdk_conv(GeomConst g, const float *sino, float *dst, const float *filt, const float *w) {
     extern __shared__ float sm[];
     const int Nd = g.Nd;
-    float *srow = sm, *wrow = sm + Nd, *ft = sm + 2 * Nd;
+    float *srow = sm, *wrow = sm + Nd, *fs = sm + 2 * Nd;   /* fs: 2 Nd - 1 entries */
     const int v = blockIdx.x, view = blockIdx.y, cond = blockIdx.z;
     const size_t off = ((size_t)cond * g.V + view) * (size_t)Nd * Nd + (size_t)Nd * v;
     for (int j = threadIdx.x; j < Nd; j += blockDim.x) {
         srow[j] = sino[off + j];
         wrow[j] = w[(size_t)Nd * v + j];
-        ft[j] = filt[j];
     }
+    for (int k = threadIdx.x; k < 2 * Nd - 1; k += blockDim.x) fs[k] = filt[k >= Nd - 1 ? k - (Nd - 1) : (Nd - 1) - k];
     __syncthreads();
-    for (int u = threadIdx.x; u < Nd; u += blockDim.x) {
-        float acc = 0.0f;
+    for (int u0 = threadIdx.x * kConvOut; u0 < Nd; u0 += blockDim.x * kConvOut) {
+        /* window f[r] = filt[|u0 + r - j|] = fs[Nd - 1 + u0 + r - j]; indices
+         * beyond the table occur only for outputs u0 + r >= Nd (not stored) */
+        const int base = Nd - 1 + u0;
+        float acc[kConvOut] = {0.f, 0.f, 0.f, 0.f};
+        float f[kConvOut];
+#pragma unroll
+        for (int r = 0; r < kConvOut; r++) f[r] = (base + r < 2 * Nd - 1) ? fs[base + r] : 0.f;
+#pragma unroll 4
         for (int j = 0; j < Nd; j++) {
-            const float fk = ft[u > j ? u - j : j - u];
-            acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(fk, srow[j]), wrow[j]));
+            const float sj = srow[j], wj = wrow[j];
+#pragma unroll
+            for (int r = 0; r < kConvOut; r++) acc[r] = __fadd_rn(acc[r], __fmul_rn(__fmul_rn(f[r], sj), wj));
+            /* slide: f[r] <- fs[base + r - (j + 1)] */
+#pragma unroll
+            for (int r = kConvOut - 1; r > 0; r--) f[r] = f[r - 1];
+            f[0] = (base - j - 1 >= 0) ? fs[base - j - 1] : 0.f;
         }
-        dst[off + u] = acc;
+#pragma unroll
+        for (int r = 0; r < kConvOut; r++)
+            if (u0 + r < Nd) dst[off + u0 + r] = acc[r];
     }
 }
 
@@ -273,12 +293,14 @@ cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_co
     }
     {
         const dim3 grid((unsigned)g.Nd, (unsigned)g.V, (unsigned)n_cond);
-        const size_t smem = 3 * (size_t)g.Nd * sizeof(float);
+        const size_t smem = 4 * (size_t)g.Nd * sizeof(float);
         if (smem > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(k_fdk_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
-        k_fdk_conv<<<grid, 128, smem, s>>>(g, sino, sino_filt, filt, weight);
+        int thr = ((g.Nd + kConvOut - 1) / kConvOut + 31) / 32 * 32;   /* one group of outputs per thread */
+        thr = thr > 256 ? 256 : thr;
+        k_fdk_conv<<<grid, thr, smem, s>>>(g, sino, sino_filt, filt, weight);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
