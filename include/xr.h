@@ -125,8 +125,10 @@ enum {
                                   sessions whose axes are all column-aligned; IR
                                   sessions for each column-aligned axis), and
                                   the back-projection gathers each voxel's 4
-                                  taps with one texture instruction; 0: it loads
-                                  them from the linear images                    */
+                                  taps with one texture instruction; likewise
+                                  FDK's filtered projections for its column-form
+                                  back-projection; 0: they load the 4 taps from
+                                  the linear images                              */
 };
 
 /* ---- context ----------------------------------------------------------- */

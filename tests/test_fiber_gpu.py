@@ -125,12 +125,14 @@ def test_forward_fiber(oracle, axes, K):
         assert rel_err(got, ref) <= TOL, (rotation, rel_err(got, ref))
 
 
+@pytest.mark.parametrize("ratio_texture", [1, 0], ids=["texture_gather", "linear_loads"])
 @pytest.mark.parametrize("method", ["MLEM", "ART"])
 @pytest.mark.parametrize("K", [3, 4])
-def test_fiber_session(oracle, method, K):
+def test_fiber_session(oracle, method, K, ratio_texture):
     xr = load_xr()
     rot = np.concatenate([three_axes()[:2], oblique_rot(74, 1)])
     s, ctx = _case(rot, 12, 20, 9, K, 75)
+    ctx.set_option(xr.Option.RATIO_TEXTURE, ratio_texture)
     truth = np.abs(_fiber_volume(12, K, 76))
     truth[:3] *= fiber_phantom(12, 3, 77, np.eye(3, dtype=np.float32))[:3] > 0
     sino = _oracle_forward(oracle, s, truth)

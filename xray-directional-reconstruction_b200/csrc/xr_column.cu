@@ -27,6 +27,7 @@
 #include "xr_storage.cuh"
 #include "xr_tile.cuh"
 #include "xr_orth.cuh"
+#include "xr_tex.cuh"
 
 namespace xr {
 namespace {
@@ -441,18 +442,6 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_fwd_col_axes(FwdColArgs a) {
 enum { B_PLAIN = 0, B_XTT = 1, B_SENS = 2, B_XTT_TEX = 3, B_PLAIN_TEX = 4 };
 __host__ __device__ constexpr bool b_plain(int m) { return m == B_PLAIN || m == B_PLAIN_TEX; }
 __host__ __device__ constexpr bool b_tex(int m) { return m == B_XTT_TEX || m == B_PLAIN_TEX; }
-
-/* The 2 x 2 texels around unnormalised coordinates (x, y) of layer `layer`
- * (tld4, component r): (T[y1][x0], T[y1][x1], T[y0][x1], T[y0][x0]) with
- * x0 = floor(x - 0.5), x1 = x0 + 1 and likewise y; coordinates outside the
- * layer clamp to its edge. */
-__device__ __forceinline__ float4 gather_a2d(cudaTextureObject_t t, int layer, float x, float y) {
-    float4 r;
-    asm("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %7}];"
-        : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
-        : "l"(t), "r"(layer), "f"(x), "f"(y));
-    return r;
-}
 
 struct BackColArgs {
     GeomConst g;

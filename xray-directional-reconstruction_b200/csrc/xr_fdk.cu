@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include "xr_internal.h"
+#include "xr_tex.cuh"
 
 namespace xr {
 namespace {
@@ -54,7 +55,10 @@ __global__ void k_fdk_weight(GeomConst g, float *w) {
  * fs[Nd - 1 + k] = filt[|k|], so each j costs one new filter value. */
 constexpr int kConvOut = 4;
 
-__global__ void k_fdk_conv(GeomConst g, const float *sino, float *dst, const float *filt, const float *w) {
+/* surf (non-zero): the filtered rows also go to layer (axis * V + view) of
+ * that 2D-layered surface, which k_fdk_bp_col gathers from. */
+__global__ void k_fdk_conv(GeomConst g, const float *sino, float *dst, const float *filt, const float *w,
+                           cudaSurfaceObject_t surf) {
     extern __shared__ float sm[];
     const int Nd = g.Nd;
     float *srow = sm, *wrow = sm + Nd, *fs = sm + 2 * Nd;   /* fs: 2 Nd - 1 entries */
@@ -85,8 +89,13 @@ __global__ void k_fdk_conv(GeomConst g, const float *sino, float *dst, const flo
             f[0] = (base - j - 1 >= 0) ? fs[base - j - 1] : 0.f;
         }
 #pragma unroll
-        for (int r = 0; r < kConvOut; r++)
-            if (u0 + r < Nd) dst[off + u0 + r] = acc[r];
+        for (int r = 0; r < kConvOut; r++) {
+            if (u0 + r >= Nd) continue;
+            dst[off + u0 + r] = acc[r];
+            if (surf)
+                surf2DLayeredwrite(acc[r], surf, (u0 + r) * (int)sizeof(float), v, cond * g.V + view,
+                                   cudaBoundaryModeZero);
+        }
     }
 }
 
@@ -96,6 +105,7 @@ struct BpArgs {
     const float *filt_sino;    /* C blocks of filtered projections            */
     float *vol;                /* C channels of N^3                           */
     int cond, src_block;
+    cudaTextureObject_t ftex;  /* k_fdk_bp_col<G, true>: the filtered projections, layer = block * V + view */
 };
 
 __global__ void __launch_bounds__(kBpThreads) k_fdk_bp(BpArgs a) {
@@ -186,7 +196,7 @@ struct BpColArgs {
  * v = ((coeff * o_G) * ev_G mag) / det + Nd/2, the taps and the gather.  Each
  * voxel still adds its views in order: the result equals k_fdk_bp's.
  * Brick: 16 along G x 8 x 8, 256 threads = 64 columns x 4 segments. */
-template <int G>
+template <int G, bool TEX>
 __global__ void __launch_bounds__(kBpThreads, 4) k_fdk_bp_col(BpColArgs c) {
     __shared__ ViewFrame fr[kFrameChunk];
     constexpr int A = FdkAx<G>::A, B = FdkAx<G>::B;
@@ -244,6 +254,8 @@ __global__ void __launch_bounds__(kBpThreads, 4) k_fdk_bp_col(BpColArgs c) {
                 w = __fmul_rn(__fmul_rn(U, U), Cw);
             }
             const float *Pc = P + (size_t)f.view * NdNd + iu;
+            const float xu = __int2float_rn(iu + 1);   /* TEX: texels iu, iu + 1 */
+            const int layer = a.src_block * g.V + f.view;
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 if (!okv[q]) continue;
@@ -255,8 +267,20 @@ __global__ void __launch_bounds__(kBpThreads, 4) k_fdk_bp_col(BpColArgs c) {
                 const float fv = __fsub_rn(vt, fiv), gv = __fsub_rn(1.0f, fv);
                 const float c1 = __fmul_rn(gu, fv), c2 = __fmul_rn(fu, fv), c3 = __fmul_rn(fu, gv),
                             c4 = __fmul_rn(gu, gv);
-                const float *pp = Pc + (size_t)Nd * iv;
-                const float p4 = __ldg(pp), p3 = __ldg(pp + 1), p1v = __ldg(pp + Nd), p2v = __ldg(pp + Nd + 1);
+                float p4, p3, p1v, p2v;
+                if (TEX) {   /* one gather: the same four values, numBack's order */
+                    const float4 t = gather_a2d(a.ftex, layer, xu, __fadd_rn(fiv, 1.0f));
+                    p1v = t.x;
+                    p2v = t.y;
+                    p3 = t.z;
+                    p4 = t.w;
+                } else {
+                    const float *pp = Pc + (size_t)Nd * iv;
+                    p4 = __ldg(pp);
+                    p3 = __ldg(pp + 1);
+                    p1v = __ldg(pp + Nd);
+                    p2v = __ldg(pp + Nd + 1);
+                }
                 const float nb = __fadd_rn(
                     __fadd_rn(__fadd_rn(__fmul_rn(c1, p1v), __fmul_rn(c2, p2v)), __fmul_rn(c3, p3)), __fmul_rn(c4, p4));
                 float wq = w;
@@ -286,7 +310,8 @@ __global__ void __launch_bounds__(kBpThreads, 4) k_fdk_bp_col(BpColArgs c) {
 
 cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_cond, const float *sino,
                        float *sino_filt, float *vol, const float *filt, float *weight, int axis_blocks,
-                       cudaStream_t s, const int *h_axis_g, const float *h_magsig) {
+                       cudaStream_t s, const int *h_axis_g, const float *h_magsig, cudaSurfaceObject_t fsurf,
+                       cudaTextureObject_t ftex) {
     {
         const dim3 blk(32, 8), grid((g.Nd + 31) / 32, (g.Nd + 7) / 8);
         k_fdk_weight<<<grid, blk, 0, s>>>(g, weight);
@@ -300,7 +325,7 @@ cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_co
         }
         int thr = ((g.Nd + kConvOut - 1) / kConvOut + 31) / 32 * 32;   /* one group of outputs per thread */
         thr = thr > 256 ? 256 : thr;
-        k_fdk_conv<<<grid, thr, smem, s>>>(g, sino, sino_filt, filt, weight);
+        k_fdk_conv<<<grid, thr, smem, s>>>(g, sino, sino_filt, filt, weight, ftex ? fsurf : 0);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -313,6 +338,7 @@ cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_co
         a.vol = vol;
         a.cond = c;
         a.src_block = axis_blocks ? c : 0;
+        a.ftex = ftex;
         const int G = h_axis_g ? h_axis_g[c] : -1;
         if (G < 0) {
             k_fdk_bp<<<(unsigned)nb, kBpThreads, 0, s>>>(a);
@@ -324,9 +350,15 @@ cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_co
         cb.nbg = (g.N + 15) / 16;
         cb.nba = (g.N + 7) / 8;
         const unsigned nbc = (unsigned)((long)cb.nbg * cb.nba * ((g.N + 7) / 8));
-        if (G == 0) k_fdk_bp_col<0><<<nbc, kBpThreads, 0, s>>>(cb);
-        else if (G == 1) k_fdk_bp_col<1><<<nbc, kBpThreads, 0, s>>>(cb);
-        else k_fdk_bp_col<2><<<nbc, kBpThreads, 0, s>>>(cb);
+        if (ftex) {
+            if (G == 0) k_fdk_bp_col<0, true><<<nbc, kBpThreads, 0, s>>>(cb);
+            else if (G == 1) k_fdk_bp_col<1, true><<<nbc, kBpThreads, 0, s>>>(cb);
+            else k_fdk_bp_col<2, true><<<nbc, kBpThreads, 0, s>>>(cb);
+        } else {
+            if (G == 0) k_fdk_bp_col<0, false><<<nbc, kBpThreads, 0, s>>>(cb);
+            else if (G == 1) k_fdk_bp_col<1, false><<<nbc, kBpThreads, 0, s>>>(cb);
+            else k_fdk_bp_col<2, false><<<nbc, kBpThreads, 0, s>>>(cb);
+        }
     }
     return cudaGetLastError();
 }

@@ -22,6 +22,7 @@
 
 #include "xr_internal.h"
 #include "xr_tile.cuh"
+#include "xr_tex.cuh"
 
 namespace xr {
 namespace {
@@ -484,13 +485,17 @@ struct FiberBackColArgs {
     int art;
     float alpha;
     int nb;                    /* bricks per dimension */
+    cudaTextureObject_t rtex;  /* non-zero: the ratio images as a 2D-layered array, layer = axis * n_views + position */
 };
 
-/* One view of a column-aligned axis for a thread's segment of 4 voxels. */
+/* One view of a column-aligned axis for a thread's segment of 4 voxels (the
+ * 4 taps loaded, or with rtex gathered from layer `layer` in one texture
+ * instruction: the same values in the same order). */
 template <int G>
 __device__ __forceinline__ void fiber_back_col_view(const ViewFrame &f, const GeomConst &g, const float *Pc, float ba,
                                                     float bb, float msig, const float dg[4], const float dg2[4],
-                                                    const bool okv[4], float tmp[4], float fac[4]) {
+                                                    const bool okv[4], float tmp[4], float fac[4],
+                                                    cudaTextureObject_t rtex, int layer) {
     constexpr int A = FAx<G>::A, B = FAx<G>::B;
     const float oa = __fsub_rn(__fsub_rn(ba, f.off[A]), f.t[A]);
     const float ob = __fsub_rn(__fsub_rn(bb, f.off[B]), f.t[B]);
@@ -509,6 +514,7 @@ __device__ __forceinline__ void fiber_back_col_view(const ViewFrame &f, const Ge
     const float da2 = __fmul_rn(da, da), db2 = __fmul_rn(db, db);
     const float dab2 = __fadd_rn(da2, db2);
     const float *P = Pc + (size_t)f.view * g.Nd * g.Nd + iu;
+    const float xu = __int2float_rn(iu + 1);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         if (!okv[q]) continue;
@@ -524,11 +530,24 @@ __device__ __forceinline__ void fiber_back_col_view(const ViewFrame &f, const Ge
             const float len = __fsqrt_rn(l2);
             w0 = len > 1e-8f ? fabsf(__fdiv_rn(db, len)) : 0.f;
         }
-        const float *Pq = P + (size_t)g.Nd * iv;
-        float nb = __fmul_rn(__fmul_rn(w0, __fmul_rn(gu, fv)), __ldg(Pq + g.Nd));
-        nb = __fadd_rn(nb, __fmul_rn(__fmul_rn(w0, __fmul_rn(fu, fv)), __ldg(Pq + g.Nd + 1)));
-        nb = __fadd_rn(nb, __fmul_rn(__fmul_rn(w0, __fmul_rn(fu, gv)), __ldg(Pq + 1)));
-        nb = __fadd_rn(nb, __fmul_rn(__fmul_rn(w0, __fmul_rn(gu, gv)), __ldg(Pq)));
+        float r0, r1, r2, r3;   /* P[iv+1][iu], P[iv+1][iu+1], P[iv][iu+1], P[iv][iu] */
+        if (rtex) {
+            const float4 t = gather_a2d(rtex, layer, xu, __fadd_rn(fiv, 1.0f));
+            r0 = t.x;
+            r1 = t.y;
+            r2 = t.z;
+            r3 = t.w;
+        } else {
+            const float *Pq = P + (size_t)g.Nd * iv;
+            r0 = __ldg(Pq + g.Nd);
+            r1 = __ldg(Pq + g.Nd + 1);
+            r2 = __ldg(Pq + 1);
+            r3 = __ldg(Pq);
+        }
+        float nb = __fmul_rn(__fmul_rn(w0, __fmul_rn(gu, fv)), r0);
+        nb = __fadd_rn(nb, __fmul_rn(__fmul_rn(w0, __fmul_rn(fu, fv)), r1));
+        nb = __fadd_rn(nb, __fmul_rn(__fmul_rn(w0, __fmul_rn(fu, gv)), r2));
+        nb = __fadd_rn(nb, __fmul_rn(__fmul_rn(w0, __fmul_rn(gu, gv)), r3));
         tmp[q] = __fadd_rn(tmp[q], nb);
         fac[q] = __fadd_rn(fac[q], w0);
     }
@@ -570,7 +589,8 @@ __device__ __forceinline__ void fiber_back_axis(const FiberBackColArgs &a, ViewF
         for (int jj = 0; jj < nv; jj++) {
             const ViewFrame &f = sfr[jj];
             if (G >= 0) {
-                fiber_back_col_view<GG>(f, g, Pc, ba, bb, msig, dg, dg2, okv, tmp, fac);
+                fiber_back_col_view<GG>(f, g, Pc, ba, bb, msig, dg, dg2, okv, tmp, fac, a.rtex,
+                                        cond * a.n_views + j0 + jj);
             } else {
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
@@ -745,7 +765,7 @@ cudaError_t launch_fiber_forward_col(const GeomConst &g, const ViewFrame *frames
 
 cudaError_t launch_fiber_back(const GeomConst &g, const ViewFrame *frames, const int *view_list, int n_views,
                               int n_cond, const int *d_axis_g, const float *d_magsig, const float *proj, float *vol,
-                              int art, float alpha, int *d_nonfinite, cudaStream_t s) {
+                              int art, float alpha, int *d_nonfinite, cudaStream_t s, cudaTextureObject_t rtex) {
     if (n_views <= 0 || n_cond <= 0) return cudaSuccess;
     {   /* the ratio images the back-projection reads: any inf or NaN? */
         const dim3 grid((unsigned)((g.Nd * g.Nd + 255) / 256 < 8 ? (g.Nd * g.Nd + 255) / 256 : 8),
@@ -763,6 +783,7 @@ cudaError_t launch_fiber_back(const GeomConst &g, const ViewFrame *frames, const
     a.proj = proj;
     a.vol = vol;
     a.nonfinite = d_nonfinite;
+    a.rtex = rtex;
     a.art = art;
     a.alpha = alpha;
     a.nb = (g.N + 7) / 8;

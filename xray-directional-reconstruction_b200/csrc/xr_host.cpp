@@ -599,7 +599,8 @@ static xr_status issue_epoch(xr_ctx *c, const std::vector<int> &orders) {
                 if (s.fiber) {
                     const ColInfo *ci = dcol(c);
                     e = launch_fiber_back(c->gc, fr, vl, s.subset_size, c->C, ci->axis_g, ci->magsig, proj,
-                                          (float *)s.d_vol, s.art, alpha, (int *)c->fiber_flag.p, str);
+                                          (float *)s.d_vol, s.art, alpha, (int *)c->fiber_flag.p, str,
+                                          s.rtex ? c->rtex : 0);
                 } else if (c->all_aligned) {
                     const ColInfo *ci = dcol(c);
                     const float *sens =
@@ -981,52 +982,64 @@ xr_status xr_reset_timings(xr_ctx *c) {
 
 /* ------------------------------------------------------------- sessions */
 
-static void free_ratio_texture(xr_ctx *c) {
-    if (c->rtex) cudaDestroyTextureObject(c->rtex);
-    if (c->rsurf) cudaDestroySurfaceObject(c->rsurf);
-    if (c->rarr) cudaFreeArray(c->rarr);
-    c->rtex = 0;
-    c->rsurf = 0;
-    c->rarr = nullptr;
-    c->rlayers = c->rnd = 0;
+static void free_layered(cudaArray_t &arr, cudaTextureObject_t &tex, cudaSurfaceObject_t &surf, int &layers,
+                         int &nd) {
+    if (tex) cudaDestroyTextureObject(tex);
+    if (surf) cudaDestroySurfaceObject(surf);
+    if (arr) cudaFreeArray(arr);
+    tex = 0;
+    surf = 0;
+    arr = nullptr;
+    layers = nd = 0;
 }
 
-/* The 2D-layered array of a subset's ratio images (Nd x Nd floats, `layers`
- * layers) with its texture (point sampling, clamped, unnormalised
- * coordinates) and surface objects; kept while the shape stays.  Leaves
- * c->rtex = 0 (the back kernel then loads from the linear images) when the
- * device cannot hold that many layers. */
-static xr_status ensure_ratio_texture(xr_ctx *c, int layers) {
-    if (c->rarr && c->rlayers == layers && c->rnd == c->Nd) return XR_OK;
-    free_ratio_texture(c);
+static void free_ratio_texture(xr_ctx *c) {
+    free_layered(c->rarr, c->rtex, c->rsurf, c->rlayers, c->rnd);
+    free_layered(c->farr, c->ftex, c->fsurf, c->flayers, c->fnd);
+}
+
+/* A 2D-layered array of Nd x Nd float images (`layers` layers) with its
+ * texture (point sampling, clamped, unnormalised coordinates) and surface
+ * objects; kept while the shape stays.  Leaves tex = 0 (the kernels then load
+ * from the linear images) when the device cannot hold that many layers. */
+static xr_status ensure_layered(xr_ctx *c, int want, cudaArray_t &arr, cudaTextureObject_t &tex,
+                                cudaSurfaceObject_t &surf, int &layers, int &nd, const char *what) {
+    if (arr && layers == want && nd == c->Nd) return XR_OK;
+    free_layered(arr, tex, surf, layers, nd);
     int max_layers = 0, max_wh = 0;
     cudaDeviceGetAttribute(&max_layers, cudaDevAttrMaxSurface2DLayeredLayers, c->device);
     cudaDeviceGetAttribute(&max_wh, cudaDevAttrMaxSurface2DLayeredWidth, c->device);
-    if (layers < 1 || layers > max_layers || c->Nd > max_wh) return XR_OK;
+    if (want < 1 || want > max_layers || c->Nd > max_wh) return XR_OK;
     const cudaChannelFormatDesc fd = cudaCreateChannelDesc<float>();
-    xr_status st = cuda_check(c, cudaMalloc3DArray(&c->rarr, &fd, make_cudaExtent(c->Nd, c->Nd, layers),
+    xr_status st = cuda_check(c, cudaMalloc3DArray(&arr, &fd, make_cudaExtent(c->Nd, c->Nd, want),
                                                    cudaArrayLayered | cudaArraySurfaceLoadStore),
-                              "ratio image array");
+                              what);
     if (st) {
-        c->rarr = nullptr;
+        arr = nullptr;
         return st;
     }
     cudaResourceDesc rd{};
     rd.resType = cudaResourceTypeArray;
-    rd.res.array.array = c->rarr;
+    rd.res.array.array = arr;
     cudaTextureDesc td{};
     td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
     td.filterMode = cudaFilterModePoint;
     td.readMode = cudaReadModeElementType;
     td.normalizedCoords = 0;
-    if ((st = cuda_check(c, cudaCreateTextureObject(&c->rtex, &rd, &td, nullptr), "ratio texture")) ||
-        (st = cuda_check(c, cudaCreateSurfaceObject(&c->rsurf, &rd), "ratio surface"))) {
-        free_ratio_texture(c);
+    if ((st = cuda_check(c, cudaCreateTextureObject(&tex, &rd, &td, nullptr), what)) ||
+        (st = cuda_check(c, cudaCreateSurfaceObject(&surf, &rd), what))) {
+        free_layered(arr, tex, surf, layers, nd);
         return st;
     }
-    c->rlayers = layers;
-    c->rnd = c->Nd;
+    layers = want;
+    nd = c->Nd;
     return XR_OK;
+}
+
+/* The subset's ratio images for the back-projections (layer = axis * subset
+ * size + list position). */
+static xr_status ensure_ratio_texture(xr_ctx *c, int layers) {
+    return ensure_layered(c, layers, c->rarr, c->rtex, c->rsurf, c->rlayers, c->rnd, "ratio image array");
 }
 
 
@@ -1077,9 +1090,9 @@ static xr_status session_begin_impl(xr_ctx *c, const void *d_sino, void *d_vol, 
     const size_t npx = (size_t)c->C * c->V * c->Nd * c->Nd;
     if ((st = ensure(c, c->proj, npx * sizeof(float), "projections"))) return st;
     s.rtex = false;
-    if (!fiber && c->ratio_texture && (s.xtt ? c->all_aligned : true)) {
-        /* XTT: every axis's subset views; IR: one axis at a time */
-        if ((st = ensure_ratio_texture(c, (s.xtt ? c->C : 1) * s.subset_size))) return st;
+    if (c->ratio_texture && (fiber || (s.xtt ? c->all_aligned : true))) {
+        /* XTT and fiber: every axis's subset views; IR: one axis at a time */
+        if ((st = ensure_ratio_texture(c, (s.xtt || fiber ? c->C : 1) * s.subset_size))) return st;
         s.rtex = c->rtex != 0;
     }
     if (fiber) {
@@ -1873,13 +1886,17 @@ xr_status xr_fdk_reconstruct(xr_ctx *c, float *const *sino, float *const *voxel,
     if ((st = upload_planes(c, c->scratch_sino, (const float *const *)sino, c->C, blk, "sinogram"))) return st;
     if ((st = ensure(c, x.fdk_sf, c->C * blk * sizeof(float), "filtered"))) return st;
     if ((st = ensure(c, c->scratch_vol, c->C * N3 * sizeof(float), "volume"))) return st;
+    if (c->ratio_texture &&
+        (st = ensure_layered(c, c->C * c->V, x.farr, x.ftex, x.fsurf, x.flayers, x.fnd, "filtered projection array")))
+        return st;
     {
         Timed t(c, XR_T_FDK);
         st = cuda_check(c, launch_fdk(c->gc, (const ViewFrame *)x.fdk_frames.p, c->C,
                                       (const float *)c->scratch_sino.p, (float *)x.fdk_sf.p,
                                       (float *)c->scratch_vol.p, (const float *)x.fdk_filt.p,
                                       (float *)x.fdk_weight.p, c->fdk_axis_blocks, c->stream,
-                                      x.fdk_axis_g.data(), x.fdk_magsig.data()), "fdk");
+                                      x.fdk_axis_g.data(), x.fdk_magsig.data(), c->ratio_texture ? x.fsurf : 0,
+                                      c->ratio_texture ? x.ftex : 0), "fdk");
     }
     if (st) return st;
     if ((st = download_planes(c, (const float *)c->scratch_vol.p, voxel, c->C, N3, "volume"))) return st;

@@ -164,6 +164,11 @@ struct xr_ctx {
     cudaTextureObject_t rtex = 0;
     cudaSurfaceObject_t rsurf = 0;
     int rlayers = 0, rnd = 0;
+    /* FDK: the filtered projections as a 2D-layered array (layer = axis * V + view) */
+    cudaArray_t farr = nullptr;
+    cudaTextureObject_t ftex = 0;
+    cudaSurfaceObject_t fsurf = 0;
+    int flayers = 0, fnd = 0;
     bool ratio_texture = true;        /* XR_OPT_RATIO_TEXTURE */
     xr::DevBuf scratch_vol, scratch_sino, scratch_md, stage;
     xr::DevBuf basis_dev;              /* BasisConst                                */
@@ -298,17 +303,22 @@ cudaError_t launch_fiber_forward_col(const GeomConst &g, const ViewFrame *frames
  * of channel 0 (voxelProduct, or voxelPlus with step alpha when art).
  * d_axis_g / d_magsig: per axis the column axis (-1: general) and
  * sign(ev[g]) * mag; *d_nonfinite (a device int the caller clears once per
- * session) is set when a ratio image read holds an infinity or a NaN. */
+ * session) is set when a ratio image read holds an infinity or a NaN; rtex
+ * (non-zero): the ratio images as a 2D-layered array (layer = axis * n_views
+ * + list position), gathered by the column axes. */
 cudaError_t launch_fiber_back(const GeomConst &g, const ViewFrame *frames, const int *view_list, int n_views,
                               int n_cond, const int *d_axis_g, const float *d_magsig, const float *proj, float *vol,
-                              int art, float alpha, int *d_nonfinite, cudaStream_t s);
+                              int art, float alpha, int *d_nonfinite, cudaStream_t s, cudaTextureObject_t rtex = 0);
 
 /* ---- xr_fdk.cu ---- */
 /* h_axis_g / h_magsig (host arrays, may be null): per axis the column axis of
- * its FDK frames (-1: general) and ev[g] * mag. */
+ * its FDK frames (-1: general) and ev[g] * mag.  fsurf / ftex (non-zero): a
+ * 2D-layered array of C * V layers the filtered projections also go to, and
+ * the column back-projection gathers its taps from. */
 cudaError_t launch_fdk(const GeomConst &g, const ViewFrame *fdk_frames, int n_cond, const float *sino,
                        float *sino_filt, float *vol, const float *filt, float *weight, int axis_blocks,
-                       cudaStream_t s, const int *h_axis_g = nullptr, const float *h_magsig = nullptr);
+                       cudaStream_t s, const int *h_axis_g = nullptr, const float *h_magsig = nullptr,
+                       cudaSurfaceObject_t fsurf = 0, cudaTextureObject_t ftex = 0);
 
 }  // namespace xr
 
