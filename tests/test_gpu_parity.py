@@ -275,6 +275,38 @@ def test_session_api_matches_host_call(oracle):
     assert rel_err(dmd.cpu().numpy(), md_h) <= 1e-4
 
 
+def test_host_call_slab_tail_matches_session(oracle):
+    """xr_xtt_reconstruct back-projects its last subset in z-slabs, each slab
+    then voxelSqrt'ed, its orientation computed and its planes downloaded while
+    the next slab runs.  At N = 70 (9 brick rows of 8: 5 slabs, the last
+    ragged) the volume, the main directions and the eigenvalues equal the
+    device session's, which applies voxelSqrt and the orientation to the
+    whole volume at its end."""
+    torch = pytest.importorskip("torch")
+    xr = load_xr()
+    s, ctx = make(70, 96, 10, C=3, K=13, seed=23)
+    truth = np.random.default_rng(24).uniform(0, 1, (s.K, s.N, s.N, s.N)).astype(np.float32)
+    db = torch.from_numpy(truth).cuda()
+    b = torch.empty((s.C, s.V, s.Nd, s.Nd), dtype=torch.float32, device="cuda")
+    ctx.dev_forward(db.data_ptr(), b.data_ptr(), True)
+    v0 = np.full((s.K, s.N, s.N, s.N), 0.01, np.float32)
+    mu_h, _, md_h, ev_h, _ = ctx.xtt_reconstruct(b.cpu().numpy(), v0, 1, 2)
+    dv = torch.from_numpy(v0).cuda()
+    dmd = torch.zeros((3, s.N, s.N, s.N), device="cuda")
+    dev = torch.zeros((3, s.N, s.N, s.N), device="cuda")
+    torch.cuda.synchronize()
+    ctx.dev_session_begin(b.data_ptr(), dv.data_ptr(), True, 1, 2)
+    ctx.dev_session_epoch()
+    ctx.dev_session_end(dmd.data_ptr(), dev.data_ptr())
+    md_d, ev_d = dmd.cpu().numpy(), dev.cpu().numpy()
+    assert rel_err(mu_h, dv.cpu().numpy()) <= TOL
+    assert rel_err(ev_h, ev_d) <= 1e-4
+    mask = np.abs(ev_d[1] - ev_d[0]) > 1e-3 * np.abs(ev_d).max()   # non-degenerate smallest eigenvalue
+    assert mask.sum() > 0
+    assert np.allclose(md_h[:, mask], md_d[:, mask], atol=1e-4 * np.abs(md_d).max())
+    ctx.close()
+
+
 def test_art_zero_step_is_identity(oracle):
     """ART with lambda = 0 (voxelPlus, ir.cu:1682-1693) leaves mu bit-for-bit
     unchanged whatever the residual images hold."""
