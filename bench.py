@@ -503,7 +503,8 @@ def run_c4(args, local):
     (seed 4), 3 axes x U{90..180} views, 256^2 detector, K = 13; BF16
     volumes and sinograms with stochastic rounding, FP32 arithmetic, FP64
     residual norms.  One batched epoch (all specimens forked onto their
-    streams, replayed as one CUDA graph, views-per-CTA autotuned) against the
+    streams, replayed as one CUDA graph, views per CTA and the forward's launch
+    shape autotuned) against the
     same epochs run specimen after specimen; per specimen the BF16 result's
     error against an FP32 run of the same epochs."""
     import torch
@@ -570,7 +571,7 @@ def run_c4(args, local):
     bat = fresh(1)
     batch = xr.Batch([sp["ctx"] for sp in specs])
     batch.session_begin([sp["b16"].data_ptr() for sp in specs], [v.data_ptr() for v in bat], True, E + 1, 5)
-    chosen = batch.autotune()
+    chosen, shapes = batch.autotune_shapes()
     batch.epoch()                                              # warm-up (graph capture)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -580,12 +581,13 @@ def run_c4(args, local):
     batch.session_end()                                        # XTT_SQRT 0: the iterates stay
     batch.close()
     per = []
-    for sp, v, r, vpc in zip(specs, bat, ref, chosen):
+    for sp, v, r, vpc, shape in zip(specs, bat, ref, chosen, shapes):
         c = sp["ctx"]
         c.set_option(xr.Option.SINO_STORAGE, 0)                # residual against the FP32 data
         res, _ = c.dev_residual(v.data_ptr(), sp["b32"].data_ptr(), True)
         err = float((v.float() - r).abs().max() / r.abs().max())
-        per.append({"N": sp["N"], "views": sp["V"], "views_per_cta": vpc, "residual_rel_l2": res,
+        per.append({"N": sp["N"], "views": sp["V"], "views_per_cta": vpc, "axes_one_launch": shape,
+                    "residual_rel_l2": res,
                     "bf16_vs_fp32_max_rel": err})
     vox_views = sum(3 * sp["V"] * sp["N"] ** 3 for sp in specs)
     line = {"mode": "uneven_batch", "specimens": per, "epochs_timed": E, "storage": "bf16 volumes and sinograms, "

@@ -387,6 +387,13 @@ xr_status xr_batch_session_end(xr_batch *batch);
  * for each candidate views-per-CTA chunk and keeps the fastest
  * (XR_OPT_VIEWS_PER_CTA of that context); chosen[i] receives it (may be NULL). */
 xr_status xr_batch_autotune(xr_batch *batch, int *chosen);
+/* The same over views-per-CTA chunk x launch shape: when a specimen's axes
+ * are all grid-aligned with more than one column axis, each chunk is timed
+ * both as one launch per column axis and as one launch for all axes, and the
+ * fastest pair is kept (XR_OPT_VIEWS_PER_CTA and XR_OPT_AXES_ONE_LAUNCH 0 / 1
+ * of that context); views_per_cta[i], axes_one_launch[i] receive them (either
+ * may be NULL). */
+xr_status xr_batch_autotune_shapes(xr_batch *batch, int *views_per_cta, int *axes_one_launch);
 
 /* The raw forward splat of xr_forward_proj_only on device buffers, for
  * callers that cannot allocate device memory: code whose device memory is

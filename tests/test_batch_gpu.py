@@ -1,6 +1,6 @@
 """Several uneven specimens in one batch (xr_batch_*): each specimen's result
 equals its own session's, with and without the multi-specimen CUDA graph and
-after the views-per-CTA autotuner; with BF16 storage, each specimen's error
+after the autotuner (views per CTA and forward launch shape); with BF16 storage, each specimen's error
 against the FP64 oracle is stated and bounded."""
 from __future__ import annotations
 
@@ -69,6 +69,10 @@ def test_batch_equals_individual_sessions(oracle, graphs):
     batch.close()
 
 
+def ctx_shape(ctx, shapes, spec):
+    return shapes[[c for _, c, _ in spec].index(ctx)]
+
+
 def test_batch_autotune_and_bf16_error_vs_fp64(oracle):
     xr = load_xr()
     spec = _specimens(oracle)
@@ -81,8 +85,9 @@ def test_batch_autotune_and_bf16_error_vs_fp64(oracle):
     torch.cuda.synchronize()
     epochs, subsets = 3, 3
     batch.session_begin([d.data_ptr() for d in dbs], [d.data_ptr() for d in dvs], True, epochs, subsets)
-    chosen = batch.autotune()
+    chosen, shapes = batch.autotune_shapes()
     assert all(v >= 0 for v in chosen)
+    assert all(sh in (0, 1) for sh in shapes)   # three column axes: both launch shapes timed
     for _ in range(epochs):
         batch.epoch()
     batch.session_end()
@@ -90,6 +95,7 @@ def test_batch_autotune_and_bf16_error_vs_fp64(oracle):
         v0 = np.full((13, s.N, s.N, s.N), 0.01, np.float64)
         ref64, _, _ = oracle.xtt_reconstruct(s, b.astype(np.float64), v0, epochs, subsets, dt=np.float64)
         err = rel_err(dv.float().cpu().numpy(), ref64)
-        print(f"specimen N={s.N} V={s.V}: views/CTA {vpc}, BF16 vs FP64 {err:.3e}")
+        print(f"specimen N={s.N} V={s.V}: views/CTA {vpc}, axes one launch {ctx_shape(ctx, shapes, spec)}, "
+              f"BF16 vs FP64 {err:.3e}")
         assert err <= 3e-2
     batch.close()

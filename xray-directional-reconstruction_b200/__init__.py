@@ -188,6 +188,8 @@ _SIGS = {
     "xr_batch_epoch": ([ctypes.c_void_p, _D], ctypes.c_int),
     "xr_batch_session_end": ([ctypes.c_void_p], ctypes.c_int),
     "xr_batch_autotune": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "xr_batch_autotune_shapes": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+                                 ctypes.c_int),
     # include/xr_learn.h
     "xr_net_create": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
                        ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
@@ -796,6 +798,13 @@ class Batch:
         out = (ctypes.c_int * len(self.contexts))()
         self._check(lib().xr_batch_autotune(self._h, out))
         return list(out)
+
+    def autotune_shapes(self):
+        """(views per CTA, axes in one launch 0 / 1) chosen per specimen."""
+        vpc = (ctypes.c_int * len(self.contexts))()
+        shape = (ctypes.c_int * len(self.contexts))()
+        self._check(lib().xr_batch_autotune_shapes(self._h, vpc, shape))
+        return list(vpc), list(shape)
 
 
 # ---------------------------------------------------------------------------

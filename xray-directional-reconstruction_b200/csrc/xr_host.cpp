@@ -2063,7 +2063,7 @@ xr_status xr_batch_session_end(xr_batch *b) {
     return first;
 }
 
-xr_status xr_batch_autotune(xr_batch *b, int *chosen) {
+xr_status xr_batch_autotune_shapes(xr_batch *b, int *chosen, int *shape) {
     if (!b) return XR_ERR_ARG;
     cudaSetDevice(b->device);
     batch_drop_graphs(b);
@@ -2089,39 +2089,60 @@ xr_status xr_batch_autotune(xr_batch *b, int *chosen) {
         std::vector<int> cand = {0, ss, (ss + 1) / 2, (ss + 3) / 4, 8, 4};
         std::sort(cand.begin(), cand.end());
         cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-        const int saved = c->views_per_cta;
-        int best = saved;
-        float best_ms = 1e30f;
-        for (int v : cand) {
-            if (v > 64 || (v > ss && v != 0)) continue;
-            c->views_per_cta = v;
-            float total = 0.f;
-            for (int rep = 0; rep < 3 && !st; rep++) {
-                cudaEventRecord(e0, c->stream);
-                st = cuda_check(c, forward_dispatch(c, (const int *)c->subsets.p, ss, all_conds(c), s.d_vol,
-                                                    (float *)c->scratch_sino.p, 1, s.storage),
-                                "autotune forward");
-                cudaEventRecord(e1, c->stream);
-                if (!st) st = cuda_check(c, cudaEventSynchronize(e1), "autotune");
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (rep > 0) total += ms;   /* first run warms up */
-            }
-            if (st) {
-                st = bspec(b, (int)i, st);
-                break;
-            }
-            if (total < best_ms) {
-                best_ms = total;
-                best = v;
-            }
+        /* launch shapes worth timing: both when several column axes exist */
+        int groups = 0;
+        for (int g = 0; g < 3; g++) {
+            bool any = false;
+            for (int cond = 0; cond < c->C; cond++) any = any || c->axis_g[cond] == g;
+            groups += any;
         }
-        c->views_per_cta = st ? saved : best;
+        std::vector<int> shapes = {c->axes_one_launch};
+        if (shape && c->all_aligned && groups > 1) shapes = {0, 1};
+        const int saved = c->views_per_cta, saved_shape = c->axes_one_launch;
+        int best = saved, best_shape = saved_shape;
+        float best_ms = 1e30f;
+        for (int sh : shapes) {
+            c->axes_one_launch = sh;
+            for (int v : cand) {
+                if (v > 64 || (v > ss && v != 0)) continue;
+                c->views_per_cta = v;
+                float total = 0.f;
+                for (int rep = 0; rep < 3 && !st; rep++) {
+                    cudaEventRecord(e0, c->stream);
+                    st = cuda_check(c, forward_dispatch(c, (const int *)c->subsets.p, ss, all_conds(c), s.d_vol,
+                                                        (float *)c->scratch_sino.p, 1, s.storage),
+                                    "autotune forward");
+                    cudaEventRecord(e1, c->stream);
+                    if (!st) st = cuda_check(c, cudaEventSynchronize(e1), "autotune");
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (rep > 0) total += ms;   /* first run warms up */
+                }
+                if (st) break;
+                if (total < best_ms) {
+                    best_ms = total;
+                    best = v;
+                    best_shape = sh;
+                }
+            }
+            if (st) break;
+        }
+        if (st) {
+            st = bspec(b, (int)i, st);
+            c->views_per_cta = saved;
+            c->axes_one_launch = saved_shape;
+            break;
+        }
+        c->views_per_cta = best;
+        c->axes_one_launch = best_shape;
         if (chosen) chosen[i] = c->views_per_cta;
+        if (shape) shape[i] = c->axes_one_launch;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return st;
 }
+
+xr_status xr_batch_autotune(xr_batch *b, int *chosen) { return xr_batch_autotune_shapes(b, chosen, nullptr); }
 
 }  // extern "C"
