@@ -734,6 +734,48 @@ __global__ void __launch_bounds__(kBackThreads, 6) k_back_col(BackColArgs a) {
         __syncthreads();
     }
     if (b_plain(MODE)) return;
+    if (MODE != B_SENS && (N & 1) == 0) {
+        /* even N: voxel pairs along x (x even, so both in range and the pair
+         * aligned), one 2-element access per channel; the same arithmetic,
+         * keys and results as the loop below */
+        for (int lp = tid; lp < 256; lp += kBackThreads) {
+            const int lv = 2 * lp;
+            const int x = bx0 + (lv & 7), y = by0 + ((lv >> 3) & 7), z = bz0 + (lv >> 6);
+            if (x >= N || y >= N || z >= N) continue;
+            const size_t idx = (size_t)x + (size_t)N * y + NN * z;
+            const int s0 = sacc_slot(lv), s1 = sacc_slot(lv + 1);
+            for (int k0 = 0; k0 < K; k0 += 8) {
+                float2 mu[8], f[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const int k = k0 + j;
+                    if (k < K) {
+                        mu[j] = ld2<T>(reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3);
+                        f[j] = a.art ? make_float2(0.f, 0.f)
+                                     : __ldg(reinterpret_cast<const float2 *>(a.fac_in + idx + (size_t)k * N3));
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const int k = k0 + j;
+                    if (k >= K) break;
+                    const float t0 = sacc[k * 512 + s0], t1 = sacc[k * 512 + s1];
+                    T *vp = reinterpret_cast<T *>(a.vol) + idx + (size_t)k * N3;
+                    const uint32_t key = (uint32_t)(idx + (size_t)k * N3);
+                    float v0, v1;
+                    if (a.art) {
+                        v0 = __fadd_rn(mu[j].x, __fmul_rn(a.alpha, t0));
+                        v1 = __fadd_rn(mu[j].y, __fmul_rn(a.alpha, t1));
+                    } else {
+                        v0 = (f[j].x == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu[j].x, t0), f[j].x);
+                        v1 = (f[j].y == 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(mu[j].y, t1), f[j].y);
+                    }
+                    stu2<T>(vp, v0, v1, key, key + 1u, a.sr);
+                }
+            }
+        }
+        return;
+    }
     /* home layout: brick-linear voxel order */
     for (int lv = tid; lv < 512; lv += kBackThreads) {
         const int x = bx0 + (lv & 7), y = by0 + ((lv >> 3) & 7), z = bz0 + (lv >> 6);

@@ -88,6 +88,38 @@ __device__ __forceinline__ void stu<__half>(__half *p, float v, uint32_t key, in
     *p = (fhi != flo && t * (fhi - flo) < (v - flo)) ? hi : lo;
 }
 
+/* Pairs of consecutive elements (the first at an even index): one 64-bit
+ * (FP32) or 32-bit (16-bit types) access. */
+template <typename T>
+__device__ __forceinline__ float2 ld2(const T *p);
+template <>
+__device__ __forceinline__ float2 ld2<float>(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+template <>
+__device__ __forceinline__ float2 ld2<__nv_bfloat16>(const __nv_bfloat16 *p) {
+    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(p));
+}
+template <>
+__device__ __forceinline__ float2 ld2<__half>(const __half *p) {
+    return __half22float2(*reinterpret_cast<const __half2 *>(p));
+}
+
+/* stu of two consecutive elements with their own keys, one store. */
+template <typename T>
+__device__ __forceinline__ void stu2(T *p, float v0, float v1, uint32_t k0, uint32_t k1, int sr);
+template <>
+__device__ __forceinline__ void stu2<float>(float *p, float v0, float v1, uint32_t, uint32_t, int) {
+    *reinterpret_cast<float2 *>(p) = make_float2(v0, v1);
+}
+template <typename T>
+__device__ __forceinline__ void stu2(T *p, float v0, float v1, uint32_t k0, uint32_t k1, int sr) {
+    T r[2];
+    stu<T>(&r[0], v0, k0, sr);
+    stu<T>(&r[1], v1, k1, sr);
+    uint32_t w;
+    memcpy(&w, r, sizeof(w));
+    *reinterpret_cast<uint32_t *>(p) = w;
+}
+
 }  // namespace xr
 
 #endif
