@@ -372,7 +372,23 @@ __device__ __forceinline__ void fwd_col_brick(const FwdColArgs &a, const int con
                     const float c1 = __fmul_rn(gu, fv), c2 = __fmul_rn(fu, fv);
                     const float c3 = __fmul_rn(fu, gv), c4 = __fmul_rn(gu, gv);
                     const int lv = iv - bb4.y;
-                    if (col_tile && lv >= 0 && lv + 1 < bb4.w) {
+                    if ((MODE == 1 || MODE == 3) && col_tile && lv >= 0 && lv + 1 < bb4.w) {
+                        /* the four taps as two packed pairs: (g_u, f_u) pvs times f_v
+                         * (row iv + 1) and times g_v (row iv), split in FP32x2 */
+                        int *t0 = tcol + W * lv;
+                        const float2 up = __fmul2_rn(make_float2(gu, fu), bc2(pvs));
+                        int2 h, l;
+                        fix_split2(__fmul2_rn(up, bc2(fv)), h, l);
+                        atomicAdd(t0 + W, h.x);
+                        atomicAdd(t0 + W + kTileCap, l.x);
+                        atomicAdd(t0 + W + 1, h.y);
+                        atomicAdd(t0 + W + 1 + kTileCap, l.y);
+                        fix_split2(__fmul2_rn(up, bc2(gv)), h, l);
+                        atomicAdd(t0, h.x);
+                        atomicAdd(t0 + kTileCap, l.x);
+                        atomicAdd(t0 + 1, h.y);
+                        atomicAdd(t0 + 1 + kTileCap, l.y);
+                    } else if (col_tile && lv >= 0 && lv + 1 < bb4.w) {
                         int *t0 = tcol + W * lv;
                         auto tap = [&](float c, int *adr) {
                             float xs;
