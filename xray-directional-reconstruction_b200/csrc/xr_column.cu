@@ -345,12 +345,25 @@ __device__ __forceinline__ void fwd_col_brick(const FwdColArgs &a, const int con
                 const float2 dab2 = bc2(fmaf(da, da, db * db));
                 const float2 daa = bc2(da * da), dbb = bc2(db * db), dab = bc2(da * db);
                 const float2 da2 = bc2(da), db2 = bc2(db);
+                /* v of the 4 voxels in two packed pairs, each lane rounded as div_det */
+                float2 vp[2];
+#pragma unroll
+                for (int p = 0; p < 2; p++) {
+                    const float2 av = __fmul2_rn(__fmul2_rn(bc2(coeff), dgp[p]), bc2(magsig));
+                    if (g.exact_rdet) {
+                        const float2 qd = __fmul2_rn(av, bc2(g.rdet));
+                        const float2 rd = __ffma2_rn(qd, bc2(-g.det), av);
+                        vp[p] = __fadd2_rn(__ffma2_rn(rd, bc2(g.rdet), qd), bc2(g.half));
+                    } else {
+                        vp[p] = make_float2(__fadd_rn(__fdiv_rn(av.x, g.det), g.half),
+                                            __fadd_rn(__fdiv_rn(av.y, g.det), g.half));
+                    }
+                }
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     if (!okv[q]) continue;
                     const float dgs = (q & 1) ? dgp[q >> 1].y : dgp[q >> 1].x;
-                    const float av = __fmul_rn(__fmul_rn(coeff, dgs), magsig);
-                    const float v = __fadd_rn(div_det(av, g), g.half);
+                    const float v = (q & 1) ? vp[q >> 1].y : vp[q >> 1].x;
                     int iv;
                     float fv, gv;
                     if (!tap1(g, v, iv, fv, gv)) continue;
