@@ -190,6 +190,26 @@ def issue_roofline(kernel: str, launch_s: float, vox_views: float, n_vox: float,
             "source": os.path.relpath(PROFILE_JSON, ROOT) + " (" + figs.get("case", "") + ")"}
 
 
+def l1_roofline(kernel: str, launch_s: float, vox_views: float, sm_mhz: float):
+    """Roofline of a projector kernel against the L1 data pipe (one LSU
+    wavefront per cycle per SM: the shared-memory atomics of the forward
+    splat's tiles, the gathers of the back-projection).  achieved = captured
+    wavefronts per voxel-view x this launch's voxel-views / launch time; peak =
+    148 SMs x the SM clock sampled during the timed region."""
+    figs = profile_figures()
+    if not figs or kernel not in figs.get("kernels", {}):
+        return None
+    k = figs["kernels"][kernel]
+    if "l1_wavefronts_per_launch" not in k:
+        return None
+    per_vv = k["l1_wavefronts_per_launch"] / k["voxel_views_per_launch"]
+    peak = 148 * sm_mhz * 1e6
+    ach = per_vv * vox_views / launch_s
+    return {"bound": "l1", "kernel": kernel, "achieved": ach / 1e9, "peak": peak / 1e9, "unit": "G wavefronts/s",
+            "frac": ach / peak, "wavefronts_per_voxel_view": per_vv, "sm_mhz": sm_mhz,
+            "source": os.path.relpath(PROFILE_JSON, ROOT) + " (" + figs.get("case", "") + ")"}
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
@@ -1051,6 +1071,7 @@ def main():
                               sm_mhz, peak)
     if roofline is None:           # no captured instruction counts: the HBM view alone
         roofline = dict(hbm, traffic=None)
+    roofline_l1 = l1_roofline(dom, avg_launch_s, float(N) ** 3 * units, sm_mhz)
     roofline.update({"avg_launch_ms": avg_launch_s * 1e3, "units_per_launch": units, "peak_kind": "sampled SM clock"
                      if roofline["bound"] == "issue" else peak_kind})
     # kernels in the timed region: per subset n_groups forward launches, one
@@ -1158,7 +1179,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": bench_config(args, world), "residual_rel_l2_after": rel,
-            "e2e": e2e, "roofline": roofline, "roofline_hbm": hbm, "effective_projector": effective,
+            "e2e": e2e, "roofline": roofline, "roofline_l1": roofline_l1, "roofline_hbm": hbm,
+            "effective_projector": effective,
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in tim.items() if v[1]},
             "variants_ms_per_step": variants, "time_to_residual": ttr, "roofline_conv": conv,

@@ -60,3 +60,18 @@ def test_issue_roofline_scales_the_captured_counts():
     assert abs(r["traffic"] - exp_traffic) < 1e-6 * exp_traffic
     assert 0 < r["frac"] == r["achieved"] / r["peak"]
     assert bench.issue_roofline("no_such_kernel", 1e-3, 1.0, 1.0, 1.0, 1965.0, 6452.2) is None
+
+
+def test_l1_roofline_scales_the_captured_wavefronts():
+    """The L1 data-pipe roofline: captured LSU wavefronts per voxel-view times
+    this launch's voxel-views, over the launch time, against one wavefront per
+    cycle on each of 148 SMs at the sampled clock."""
+    bench = _bench()
+    k = bench.profile_figures()["kernels"]["k_fwd_col<1,g,float>"]
+    per_vv = k["l1_wavefronts_per_launch"] / k["voxel_views_per_launch"]
+    r = bench.l1_roofline("k_fwd_col<1,g,float>", 2e-3, 1e9, 1965.0)
+    assert r["bound"] == "l1"
+    assert abs(r["achieved"] - per_vv * 1e9 / 2e-3 / 1e9) < 1e-6 * r["achieved"]
+    assert abs(r["peak"] - 148 * 1965e6 / 1e9) < 1e-9
+    assert 0 < r["frac"] == r["achieved"] / r["peak"]
+    assert bench.l1_roofline("no_such_kernel", 1e-3, 1.0, 1965.0) is None
