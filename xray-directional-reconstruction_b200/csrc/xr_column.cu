@@ -385,31 +385,32 @@ __device__ __forceinline__ void fwd_col_brick(const FwdColArgs &a, const int con
                     const float c1 = __fmul_rn(gu, fv), c2 = __fmul_rn(fu, fv);
                     const float c3 = __fmul_rn(fu, gv), c4 = __fmul_rn(gu, gv);
                     const int lv = iv - bb4.y;
-                    if ((MODE == 1 || MODE == 3) && col_tile && lv >= 0 && lv + 1 < bb4.w) {
-                        /* the four taps as two packed pairs: (g_u, f_u) pvs times f_v
-                         * (row iv + 1) and times g_v (row iv), split in FP32x2 */
+                    if (col_tile && lv >= 0 && lv + 1 < bb4.w) {
+                        /* the four taps as two packed pairs, row iv + 1 (times f_v) and
+                         * row iv (times g_v), split in FP32x2.  XTT: (g_u, f_u) pvs times
+                         * f_v / g_v; plain and weights: each lane rounded as the scalar
+                         * tap ((c ratio) pvs) fscale / c pvs with c = g_u f_v etc. */
                         int *t0 = tcol + W * lv;
-                        const float2 up = __fmul2_rn(make_float2(gu, fu), bc2(pvs));
+                        const float2 guf = make_float2(gu, fu);
+                        const float2 up = (MODE == 1 || MODE == 3) ? __fmul2_rn(guf, bc2(pvs)) : guf;
+                        auto xs2 = [&](float w) {
+                            if (MODE == 1 || MODE == 3) return __fmul2_rn(up, bc2(w));
+                            const float2 c = __fmul2_rn(guf, bc2(w));
+                            if (MODE == 0)
+                                return __fmul2_rn(__fmul2_rn(__fmul2_rn(c, bc2(g.ratio)), bc2(pvs)), bc2(fscale));
+                            return __fmul2_rn(c, bc2(pvs));
+                        };
                         int2 h, l;
-                        fix_split2(__fmul2_rn(up, bc2(fv)), h, l);
+                        fix_split2(xs2(fv), h, l);
                         atomicAdd(t0 + W, h.x);
                         atomicAdd(t0 + W + kTileCap, l.x);
                         atomicAdd(t0 + W + 1, h.y);
                         atomicAdd(t0 + W + 1 + kTileCap, l.y);
-                        fix_split2(__fmul2_rn(up, bc2(gv)), h, l);
+                        fix_split2(xs2(gv), h, l);
                         atomicAdd(t0, h.x);
                         atomicAdd(t0 + kTileCap, l.x);
                         atomicAdd(t0 + 1, h.y);
                         atomicAdd(t0 + 1 + kTileCap, l.y);
-                    } else if (col_tile && lv >= 0 && lv + 1 < bb4.w) {
-                        int *t0 = tcol + W * lv;
-                        auto tap = [&](float c, int *adr) {
-                            float xs;
-                            if (MODE == 0) xs = __fmul_rn(__fmul_rn(c, g.ratio), pvs) * fscale;
-                            else xs = c * pvs;
-                            fix_add(adr, kTileCap, xs);
-                        };
-                        tap(c1, t0 + W); tap(c2, t0 + W + 1); tap(c3, t0 + 1); tap(c4, t0);
                     } else {
                         float *p0 = pcol + (size_t)Nd * iv;
                         auto tapg = [&](float c, float *adr) {
