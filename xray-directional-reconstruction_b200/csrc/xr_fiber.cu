@@ -424,12 +424,21 @@ __global__ void __launch_bounds__(kColThreads, 2) k_fiber_fwd_col(FiberFwdArgs a
                     const float c3 = __fmul_rn(fu, gv), c4 = __fmul_rn(gu, gv);
                     const int lv = iv - bb4.y;
                     if (col_tile && lv >= 0 && lv + 1 < bb4.w) {
+                        /* the taps as two packed FP32x2 pairs (rows iv + 1 and iv) */
                         const float pw = fabsf(ps) * wsc * fscale;
                         int *t0 = T + lu + W * lv;
-                        fix_add(t0 + W, kColTileCap, c1 * pw);
-                        fix_add(t0 + W + 1, kColTileCap, c2 * pw);
-                        fix_add(t0 + 1, kColTileCap, c3 * pw);
-                        fix_add(t0, kColTileCap, c4 * pw);
+                        const float2 up = make_float2(gu * pw, fu * pw);
+                        int2 h, l;
+                        fix_split2(make_float2(up.x * fv, up.y * fv), h, l);
+                        atomicAdd(t0 + W, h.x);
+                        atomicAdd(t0 + W + kColTileCap, l.x);
+                        atomicAdd(t0 + W + 1, h.y);
+                        atomicAdd(t0 + W + 1 + kColTileCap, l.y);
+                        fix_split2(make_float2(up.x * gv, up.y * gv), h, l);
+                        atomicAdd(t0, h.x);
+                        atomicAdd(t0 + kColTileCap, l.x);
+                        atomicAdd(t0 + 1, h.y);
+                        atomicAdd(t0 + 1 + kColTileCap, l.y);
                     } else {
                         const float pw = fabsf(ps) * wsc;
                         float *p0 = P + iu + (size_t)Nd * iv;
