@@ -213,15 +213,14 @@ __device__ __forceinline__ void fwd_col_brick(const FwdColArgs &a, const int con
      * the source-to-voxel vector): off_g and t_g are the same for every view
      * of a column-aligned axis (checked on the host), so this is per voxel */
     float2 dgp[2];
-    bool okv[4];
+    /* the thread's voxels q < nqv lie in the volume (a count, not a mask:
+     * four predicates held over the view loop cost the XTT form spills) */
+    const int nqv = col_ok ? max(0, min(4, g1 - igb + 1)) : 0;
     {
         const float offg = fr[0].off[G], tg = fr[0].t[G];
         float dgq[4];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            dgq[q] = __fsub_rn(__fsub_rn(vox_base(igb + q, N, g.vs), offg), tg);
-            okv[q] = col_ok && (igb + q <= g1);
-        }
+        for (int q = 0; q < 4; q++) dgq[q] = __fsub_rn(__fsub_rn(vox_base(igb + q, N, g.vs), offg), tg);
         dgp[0] = make_float2(dgq[0], dgq[1]);
         dgp[1] = make_float2(dgq[2], dgq[3]);
     }
@@ -245,7 +244,7 @@ __device__ __forceinline__ void fwd_col_brick(const FwdColArgs &a, const int con
             val[q] = 0.f;
 #pragma unroll
             for (int e = 0; e < 6; e++) m[q][e] = 0.f;
-            if (!okv[q]) continue;
+            if (q >= nqv) continue;
             const size_t iq = idx0 + (size_t)q * sgs;
             if (MODE == 0) {
                 val[q] = ldgf<T>(vol + iq);
@@ -271,7 +270,7 @@ __device__ __forceinline__ void fwd_col_brick(const FwdColArgs &a, const int con
 #pragma unroll
                 const T *vk = vol + (size_t)k * N3 + idx0;
 #pragma unroll
-                for (int q = 0; q < 4; q++) mu[q] = okv[q] ? ldgf<T>(vk + (size_t)q * sgs) * gk : 0.f;
+                for (int q = 0; q < 4; q++) mu[q] = q < nqv ? ldgf<T>(vk + (size_t)q * sgs) * gk : 0.f;
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     val[q] = fmaf(s2k, mu[q], val[q]);
@@ -288,7 +287,7 @@ __device__ __forceinline__ void fwd_col_brick(const FwdColArgs &a, const int con
         float bound = 0.f;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            if (!okv[q]) continue;
+            if (q >= nqv) continue;
             float bq = (MODE == 0) ? fabsf(val[q]) * g.ratio : (MODE == 2 ? 1.0f : fabsf(val[q]));
             if (MODE == 1 || MODE == 3)
 #pragma unroll
@@ -361,7 +360,7 @@ __device__ __forceinline__ void fwd_col_brick(const FwdColArgs &a, const int con
                 }
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    if (!okv[q]) continue;
+                    if (q >= nqv) continue;
                     const float dgs = (q & 1) ? dgp[q >> 1].y : dgp[q >> 1].x;
                     const float v = (q & 1) ? vp[q >> 1].y : vp[q >> 1].x;
                     int iv;
