@@ -55,6 +55,12 @@ xr_status xr_net_infer(xr_net *net, const void *d_in, void *d_out, int storage, 
 xr_status xr_net_loss_grad(xr_net *net, const float *d_in, const float *d_target, int nx, int ny, int nz,
                            float in_scale, double *loss, float *host_grad);
 xr_status xr_net_adam_step(xr_net *net, float lr, float beta1, float beta2, float eps);
+/* Orientation term of the training loss (0 = off, the default): xr_net_loss_grad
+ * then minimises sum_c (pred - target)_c^2 + weight * ||T(pred) - T(target)||_F^2
+ * per voxel (over K * voxels), T(mu) = sum_k mu_k S_k S_k^T the tensor whose
+ * smallest-eigenvalue eigenvector is the voxel's main direction (calcEigenVector,
+ * direction/src/pca.cu:12-55, on sqrt|mu|); basis: K rows of S_k (host). */
+xr_status xr_net_set_tensor_loss(xr_net *net, const float *basis, float weight);
 
 /* Layer-level tensor-core operators on device buffers (BF16 as uint16 bits,
  * channels-last: element [v][c], v = x + nx*(y + ny*z)); cin, cout in {16, 32}.

@@ -95,10 +95,20 @@ def flatten(params) -> np.ndarray:
     return np.concatenate([np.concatenate([W.ravel(), b.ravel()]) for W, b in params])
 
 
+def tensor_components(basis: np.ndarray) -> np.ndarray:
+    """E[k] = (xx, yy, zz, xy, xz, yz) of S_k S_k^T, [K, 6]."""
+    S = np.asarray(basis, np.float64).reshape(-1, 3)
+    x, y, z = S[:, 0], S[:, 1], S[:, 2]
+    return np.stack([x * x, y * y, z * z, x * y, x * z, y * z], axis=1)
+
+
 def net_loss_grad(p: np.ndarray, x: np.ndarray, target: np.ndarray, channels: int, width: int, depth: int,
-                  in_scale: float = 1.0, bf16_emulation: bool = True):
+                  in_scale: float = 1.0, bf16_emulation: bool = True, tensor_basis=None, tensor_weight: float = 0.0):
     """Loss and flat gradient of the network on planar volumes x, target
-    [K, nz, ny, nx].  Returns (loss, grad, pred)."""
+    [K, nz, ny, nx].  Returns (loss, grad, pred).  With tensor_weight > 0 the
+    loss adds tensor_weight * ||T(pred) - T(target)||_F^2 per voxel, T(mu) =
+    sum_k mu_k S_k S_k^T (the tensor of calcEigenVector, pca.cu:12-55, on
+    sqrt|mu|), over the same K * voxels."""
     R = bf16 if bf16_emulation else (lambda a: np.asarray(a, np.float64))
     params = unflatten(p, channels, width, depth)
     xs = np.moveaxis(np.asarray(x, np.float64), 0, -1)          # [nz, ny, nx, K]
@@ -121,7 +131,14 @@ def net_loss_grad(p: np.ndarray, x: np.ndarray, target: np.ndarray, channels: in
     n = pred.size
     diff = pred - ts
     loss = float((diff ** 2).sum() / n)
-    g = R(2.0 * diff / n / in_scale)
+    gd = diff
+    if tensor_weight > 0:
+        E = tensor_components(tensor_basis)[:diff.shape[-1]]
+        w = np.array([1.0, 1.0, 1.0, 2.0, 2.0, 2.0])
+        dT = diff @ E                                   # [..., 6]
+        loss += float(tensor_weight * (w * dT ** 2).sum() / n)
+        gd = diff + tensor_weight * (dT * w) @ E.T
+    g = R(2.0 * gd / n / in_scale)
     grads = [None] * depth
     for l in range(depth - 1, -1, -1):
         W, b = params[l]

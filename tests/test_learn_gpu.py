@@ -142,6 +142,36 @@ def test_net_loss_and_gradient_match_oracle():
     net.close()
 
 
+def test_net_tensor_loss_matches_oracle():
+    """The orientation term of the training loss: loss and gradient against
+    the oracle with the XTT basis; weight 0 restores the plain MSE."""
+    xr = load_xr()
+    K, x, t = _net_case(seed=4)
+    basis = np.array([[1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 0], [1, -1, 0], [1, 0, 1], [1, 0, -1], [0, 1, 1],
+                      [0, 1, -1], [1, 1, 1], [1, 1, -1], [1, -1, 1], [-1, 1, 1]], np.float64)
+    basis /= np.linalg.norm(basis, axis=1, keepdims=True)
+    net = xr.Net(K, 32, 4, seed=6)
+    p = net.get_params()
+    dx = torch.from_numpy(x).cuda()
+    dt = torch.from_numpy(t).cuda()
+    l_plain, _ = net.loss_grad(dx.data_ptr(), dt.data_ptr(), x.shape[1:])
+    net.set_tensor_loss(basis, 3.0)
+    loss, g = net.loss_grad(dx.data_ptr(), dt.data_ptr(), x.shape[1:], want_grad=True)
+    rl, rg, _ = ws.net_loss_grad(p.astype(np.float64), x, t, K, 32, 4, tensor_basis=basis, tensor_weight=3.0)
+    assert loss > 1.5 * l_plain
+    assert abs(loss - rl) <= 1e-3 * rl
+    rel = np.linalg.norm(g - rg) / np.linalg.norm(rg)
+    cos = float(g @ rg / (np.linalg.norm(g) * np.linalg.norm(rg)))
+    print(f"tensor-loss gradient: rel L2 {rel:.3e}, cosine {cos:.6f}")
+    assert rel <= 2e-2 and cos >= 0.999
+    net.set_tensor_loss(None, 0.0)
+    l_off, _ = net.loss_grad(dx.data_ptr(), dt.data_ptr(), x.shape[1:])
+    assert l_off == l_plain
+    with pytest.raises(xr.XRError):
+        net.set_tensor_loss(basis, -1.0)
+    net.close()
+
+
 @pytest.mark.parametrize("storage", [0, 1])
 def test_net_infer_matches_oracle(storage):
     xr = load_xr()

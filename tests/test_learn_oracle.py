@@ -66,3 +66,35 @@ def test_net_gradient_matches_finite_differences():
         fd = (lp - lm) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(fd), (i, fd, g[i])
     assert loss > 0
+
+
+def test_tensor_loss_is_the_frobenius_error_of_the_direction_tensor():
+    """The oracle's orientation term equals weight * ||sum_k d_k S_k S_k^T||_F^2
+    summed over voxels (/ K voxels), and its gradient matches finite
+    differences."""
+    rng = np.random.default_rng(3)
+    C, Wd, D = 3, 3, 2
+    basis = rng.normal(0, 1, (C, 3))
+    shapes = ws.layer_shapes(C, Wd, D)
+    n = sum(27 * ci * co + co for ci, co in shapes)
+    p = rng.normal(0, 0.2, n)
+    x = rng.uniform(0, 1, (C, 3, 4, 4))
+    t = rng.uniform(0, 1, (C, 3, 4, 4))
+    w = 2.5
+    l0, _, pred = ws.net_loss_grad(p, x, t, C, Wd, D, bf16_emulation=False)
+    loss, g, _ = ws.net_loss_grad(p, x, t, C, Wd, D, bf16_emulation=False, tensor_basis=basis, tensor_weight=w)
+    d = pred - t                                              # [C, nz, ny, nx]
+    SS = np.einsum("ki,kj->kij", basis, basis)
+    dT = np.einsum("kzyx,kij->zyxij", d, SS)
+    assert abs(loss - (l0 + w * (dT ** 2).sum() / d.size)) <= 1e-12 * loss
+    idx = rng.choice(n, 30, replace=False)
+    h = 1e-6
+    for i in idx:
+        e = np.zeros(n)
+        e[i] = h
+        lp, _, _ = ws.net_loss_grad(p + e, x, t, C, Wd, D, bf16_emulation=False, tensor_basis=basis,
+                                    tensor_weight=w)
+        lm, _, _ = ws.net_loss_grad(p - e, x, t, C, Wd, D, bf16_emulation=False, tensor_basis=basis,
+                                    tensor_weight=w)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(fd), (i, fd, g[i])

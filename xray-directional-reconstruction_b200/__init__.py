@@ -207,6 +207,7 @@ _SIGS = {
                           ctypes.c_int, ctypes.c_float, _D, _F], ctypes.c_int),
     "xr_net_adam_step": ([ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float],
                          ctypes.c_int),
+    "xr_net_set_tensor_loss": ([ctypes.c_void_p, _F, ctypes.c_float], ctypes.c_int),
     "xr_conv3d_fprop": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                          ctypes.c_int], ctypes.c_int),
@@ -884,6 +885,15 @@ class Net:
 
     def adam_step(self, lr: float, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8) -> None:
         self._check(lib().xr_net_adam_step(self._h, float(lr), float(beta1), float(beta2), float(eps)))
+
+    def set_tensor_loss(self, basis, weight: float) -> None:
+        """Adds weight * ||T(pred) - T(target)||_F^2 per voxel to the training
+        loss, T(mu) = sum_k mu_k S_k S_k^T (the tensor of the main direction);
+        basis: K x 3 scattering vectors; weight 0 turns it off."""
+        b = _f32(np.zeros((0, 3)) if basis is None else basis).reshape(-1, 3)
+        if basis is not None and b.shape[0] < self.channels:
+            raise ValueError("the tensor loss needs one basis vector per channel")
+        self._check(lib().xr_net_set_tensor_loss(self._h, b.ctypes.data_as(_F) if b.size else None, float(weight)))
 
 
 def conv3d_fprop(x: int, cin: int, w: int, bias: int, mask: int, y: int, cout: int, shape, epilogue: int,

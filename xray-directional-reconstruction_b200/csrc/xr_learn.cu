@@ -600,21 +600,48 @@ __global__ void k_pack_in(const T *x, int K, long nvox, float scale, bf16 *out) 
     }
 }
 
-/* g[v][c] = bf16(gscale * (pred - target)) (zero for c >= K); loss += sum (pred - target)^2 */
+/* Orientation term of the training loss.  A voxel's main direction is the
+ * smallest-eigenvalue eigenvector of T(mu) = (1/K) sum_k mu_k S_k S_k^T
+ * (calcEigenVector on sqrt|mu|, whose squares are mu for mu >= 0), a linear
+ * map of the channels: the term weight * ||T(pred) - T(target)||_F^2 (without
+ * the 1/K) adds sum_j w_j (sum_k d_k E_kj)^2 per voxel, E_k = (xx, yy, zz, xy,
+ * xz, yz) of S_k S_k^T and w = (1, 1, 1, 2, 2, 2) (the off-diagonal pairs). */
+struct TensorLoss {
+    float weight;        /* 0: plain MSE */
+    float E[16][6];
+};
+
+/* g[v][c] = bf16(gscale * dL/dpred_c / 2) (zero for c >= K), with d = pred -
+ * target and L = sum_c d_c^2 + weight * sum_j w_j dT_j^2, dT_j = sum_c d_c E_cj;
+ * loss += L */
 __global__ void k_loss_grad(const float *pred, const float *target, int K, long nvox, float gscale, bf16 *g,
-                            double *loss) {
+                            double *loss, const TensorLoss tl) {
+    constexpr float wj[6] = {1.f, 1.f, 1.f, 2.f, 2.f, 2.f};
     double s = 0.0;
     for (long v = (long)blockIdx.x * blockDim.x + threadIdx.x; v < nvox; v += (long)gridDim.x * blockDim.x) {
+        float d[16];
+#pragma unroll
+        for (int c = 0; c < 16; c++) d[c] = (c < K) ? pred[(size_t)c * nvox + v] - target[(size_t)c * nvox + v] : 0.f;
         float f[16];
 #pragma unroll
         for (int c = 0; c < 16; c++) {
-            f[c] = 0.f;
-            if (c < K) {
-                const float d = pred[(size_t)c * nvox + v] - target[(size_t)c * nvox + v];
-                s += (double)d * d;
-                f[c] = gscale * d;
+            s += (double)d[c] * d[c];
+            f[c] = d[c];
+        }
+        if (tl.weight > 0.f) {
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                float dt = 0.f;
+#pragma unroll
+                for (int c = 0; c < 16; c++) dt = fmaf(d[c], tl.E[c][j], dt);
+                s += (double)(tl.weight * wj[j]) * dt * dt;
+                const float a = tl.weight * wj[j] * dt;
+#pragma unroll
+                for (int c = 0; c < 16; c++) f[c] = fmaf(a, tl.E[c][j], f[c]);
             }
         }
+#pragma unroll
+        for (int c = 0; c < 16; c++) f[c] = (c < K) ? gscale * f[c] : 0.f;
         uint4 *o = reinterpret_cast<uint4 *>(g + (size_t)v * 16);
         o[0] = make_uint4(pack2(f[0], f[1]), pack2(f[2], f[3]), pack2(f[4], f[5]), pack2(f[6], f[7]));
         o[1] = make_uint4(pack2(f[8], f[9]), pack2(f[10], f[11]), pack2(f[12], f[13]), pack2(f[14], f[15]));
@@ -901,6 +928,7 @@ struct xr_net {
     float *pred = nullptr;              /* [K][cap] FP32           */
     double *loss = nullptr;
     int *err = nullptr;
+    TensorLoss tloss{};                 /* orientation term of the training loss */
     std::string msg;
 };
 
@@ -1108,6 +1136,24 @@ xr_status xr_net_set_stream(xr_net *n, void *stream) {
     return XR_OK;
 }
 
+xr_status xr_net_set_tensor_loss(xr_net *n, const float *basis, float weight) {
+    if (!n) return XR_ERR_ARG;
+    if (!(weight >= 0.f) || !std::isfinite(weight)) return net_fail(n, XR_ERR_ARG, "tensor loss weight must be >= 0");
+    if (weight > 0.f && !basis) return net_fail(n, XR_ERR_ARG, "tensor loss needs the K basis vectors");
+    TensorLoss t{};
+    t.weight = weight;
+    if (weight > 0.f)
+        for (int k = 0; k < n->K; k++) {
+            const float x = basis[3 * k], y = basis[3 * k + 1], z = basis[3 * k + 2];
+            if (!std::isfinite(x) || !std::isfinite(y) || !std::isfinite(z))
+                return net_fail(n, XR_ERR_ARG, "non-finite basis vector");
+            const float e[6] = {x * x, y * y, z * z, x * y, x * z, y * z};
+            for (int j = 0; j < 6; j++) t.E[k][j] = e[j];
+        }
+    n->tloss = t;
+    return XR_OK;
+}
+
 size_t xr_net_num_params(const xr_net *n) { return n ? n->n_params : 0; }
 
 xr_status xr_net_get_params(xr_net *n, float *host, size_t count) {
@@ -1203,7 +1249,8 @@ xr_status xr_net_loss_grad(xr_net *n, const float *d_in, const float *d_target, 
     const int D = n->depth;
     /* dL/d(last conv) = 2 (y - t) / (K nvox) / s */
     k_loss_grad<<<grid1d(nvox, 256), 256, 0, s>>>(n->pred, d_target, n->K, nvox,
-                                                  2.0f / ((float)n->K * (float)nvox) / in_scale, n->grd[D - 1], n->loss);
+                                                  2.0f / ((float)n->K * (float)nvox) / in_scale, n->grd[D - 1], n->loss,
+                                                  n->tloss);
     if ((st = net_cuda(n, cudaGetLastError(), "loss"))) return st;
     for (int l = D - 1; l >= 0; l--) {
         const XrLayer &L = n->layers[l];

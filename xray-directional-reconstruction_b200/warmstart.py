@@ -283,6 +283,9 @@ def main(argv=None):
     ap.add_argument("--crop", type=int, default=64)
     ap.add_argument("--early", type=int, default=5)
     ap.add_argument("--depths", default="4", help="comma-separated network depths, each trained on the same pool")
+    ap.add_argument("--tensor-loss", default="0",
+                    help="comma-separated weights of the loss's direction-tensor term (0: plain MSE), each trained "
+                         "on the same pool")
     ap.add_argument("--target", default="converged", choices=["converged", "truth"])
     ap.add_argument("--target-residual", type=float, default=1e-3)
     ap.add_argument("--steps", type=int, default=12000)
@@ -299,19 +302,27 @@ def main(argv=None):
                          storage=args.storage, target=args.target, target_residual=args.target_residual, log=tlog)
     t1 = time.time()
     depths = [int(d) for d in args.depths.split(",")]
+    tweights = [float(w) for w in args.tensor_loss.split(",")]
     recs = []
     for depth in depths:
-        t2 = time.time()
-        net = xr.Net(scan.K, 32, depth, seed=0)
-        net.set_stream(scan.stream.cuda_stream)
-        trace = train(net, xin, tgt, args.steps, args.lr)
-        torch.cuda.synchronize()
-        t3 = time.time()
-        out = args.out if len(depths) == 1 else args.out.replace(".bin", f"_d{depth}.bin")
-        os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
-        net.save(out)
-        net.close()
-        recs.append({"out": os.path.basename(out), "depth": depth, "train_s": t3 - t2, "loss_trace": trace})
+        for tw in tweights:
+            t2 = time.time()
+            net = xr.Net(scan.K, 32, depth, seed=0)
+            net.set_stream(scan.stream.cuda_stream)
+            net.set_tensor_loss(scan.basis, tw)
+            trace = train(net, xin, tgt, args.steps, args.lr)
+            torch.cuda.synchronize()
+            t3 = time.time()
+            out = args.out
+            if len(depths) > 1:
+                out = out.replace(".bin", f"_d{depth}.bin")
+            if len(tweights) > 1:
+                out = out.replace(".bin", f"_t{tw:g}.bin")
+            os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+            net.save(out)
+            net.close()
+            recs.append({"out": os.path.basename(out), "depth": depth, "tensor_loss": tw, "train_s": t3 - t2,
+                         "loss_trace": trace})
     rec = {"pairs": int(xin.shape[0]), "phantoms": args.phantoms, "seeds": [args.seed0, args.seed0 + args.phantoms - 1],
            "N": args.N, "crop": args.crop, "crops_per_phantom": args.crops, "early_epochs": args.early,
            "target": args.target, "target_residual": args.target_residual, "steps": args.steps, "lr": args.lr,
