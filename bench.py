@@ -511,6 +511,20 @@ def run_ttr(args, local):
         line["orientation_gate"] = {"learned_median_deg": lo["median_deg"], "plain_median_deg": po["median_deg"],
                                     "allowed_excess_deg": 0.25,
                                     "pass": bool(lo["median_deg"] <= po["median_deg"] + 0.25)}
+    # plain FP32 after as many epochs as the learned arm ran (not timed): the
+    # direction at equal epochs, beside the gate's comparison at equal residual
+    le = arms.get("learned_bf16", {}).get("epochs")
+    if md_true is not None and le and arms.get("learned_bf16", {}).get("reached"):
+        try:
+            vol = torch.full((K, N, N, N), 0.01, dtype=torch.float32, device="cuda")
+            scan.osem(b, vol, int(le), W["batch"], 0, 0, final_sqrt=False)
+            eq = angle_stats(orientation_of(scan, vol), md_true, fiber_mask)
+            eq["epochs"] = int(le)
+            eq["residual"] = scan.residual(vol, b, 0, 0)
+            line["orientation_plain_f32_at_learned_epochs"] = eq
+            del vol
+        except Exception as ex:
+            line["orientation_plain_f32_at_learned_epochs"] = {"error": f"{type(ex).__name__}: {ex}"}
     line["orientation_note"] = ("angle between per-voxel main directions (calcEigenVector of sqrt|mu|) over the "
                                 "fiber voxels of the phantom; the truth is the orientation of the true volume")
     del md_arm, md_true
@@ -1163,6 +1177,7 @@ def main():
                "same data b = A mu_true (held-out phantom)",
                "orientation_learned_bf16_vs_plain_f32": t["orientation_learned_bf16_vs_plain_f32"],
                "orientation_note": t["orientation_note"], "orientation_gate": t.get("orientation_gate"),
+               "orientation_plain_f32_at_learned_epochs": t.get("orientation_plain_f32_at_learned_epochs"),
                "network": t.get("network")}
         for k, a in t["arms"].items():
             ttr[k] = {x: a.get(x) for x in ("seconds", "epochs", "reached", "residual_final", "storage",

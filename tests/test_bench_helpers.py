@@ -58,7 +58,7 @@ def test_issue_roofline_scales_the_captured_counts():
     exp_traffic = (k["dram_read_bytes_per_launch"] * 2e7 / k["voxels_per_launch"] +
                    k["dram_write_bytes_per_launch"] * 1e6 / k["pixel_views_per_launch"])
     assert abs(r["traffic"] - exp_traffic) < 1e-6 * exp_traffic
-    assert 0 < r["frac"] == r["achieved"] / r["peak"]
+    assert r["frac"] > 0 and abs(r["frac"] - r["achieved"] / r["peak"]) <= 1e-12 * r["frac"]
     assert bench.issue_roofline("no_such_kernel", 1e-3, 1.0, 1.0, 1.0, 1965.0, 6452.2) is None
 
 
