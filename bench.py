@@ -1007,8 +1007,10 @@ def main():
     def epoch_ms(storage, graphs, steps, split=None):
         """Mean epoch time of a fresh session (same inputs) with the given
         storage type and graph replay; warm-up epochs untimed.  split: a dict
-        that receives the per-class device times per epoch (direct epochs
-        only: timing events are not recorded inside graphs)."""
+        that receives the per-class device times per epoch, averaged over the
+        timed epochs, which then run with the per-class timing events on, as
+        the FP32 epochs of the headline do (direct epochs only: timing events
+        are not recorded inside graphs)."""
         ctx.set_option(xr.Option.STORAGE, storage)
         ctx.set_option(xr.Option.GRAPHS, graphs)
         dt = {0: torch.float32, 1: torch.bfloat16, 2: torch.float16}[storage]
@@ -1018,6 +1020,10 @@ def main():
         ctx.dev_session_begin(db.data_ptr(), dv.data_ptr(), True, args.warmup + steps, W["batch"])
         for _ in range(args.warmup):
             ctx.dev_session_epoch()
+        torch.cuda.synchronize()
+        if split is not None:
+            ctx.set_option(xr.Option.TIMING, 1)
+            ctx.reset_timings()
         a0 = torch.cuda.Event(enable_timing=True)
         a1 = torch.cuda.Event(enable_timing=True)
         a0.record(stream)
@@ -1027,11 +1033,7 @@ def main():
         torch.cuda.synchronize()
         ms = a0.elapsed_time(a1) / steps
         if split is not None:
-            ctx.set_option(xr.Option.TIMING, 1)
-            ctx.reset_timings()
-            ctx.dev_session_epoch()
-            torch.cuda.synchronize()
-            split.update({k: v[0] for k, v in ctx.timings().items() if v[1]})
+            split.update({k: v[0] / steps for k, v in ctx.timings().items() if v[1]})
             ctx.set_option(xr.Option.TIMING, 0)
         ctx.dev_session_end(0, 0)
         ctx.set_option(xr.Option.GRAPHS, 0)
