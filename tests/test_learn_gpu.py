@@ -166,7 +166,7 @@ def test_net_tensor_loss_matches_oracle():
     assert rel <= 2e-2 and cos >= 0.999
     net.set_tensor_loss(None, 0.0)
     l_off, _ = net.loss_grad(dx.data_ptr(), dt.data_ptr(), x.shape[1:])
-    assert l_off == l_plain
+    assert abs(l_off - l_plain) <= 1e-9 * l_plain   # the loss sums per-block partials by atomics, in any order
     with pytest.raises(xr.XRError):
         net.set_tensor_loss(basis, -1.0)
     net.close()
