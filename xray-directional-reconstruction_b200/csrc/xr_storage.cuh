@@ -119,6 +119,28 @@ __device__ __forceinline__ void stu2(T *p, float v0, float v1, uint32_t k0, uint
     memcpy(&w, r, sizeof(w));
     *reinterpret_cast<uint32_t *>(p) = w;
 }
+/* BF16 pairs draw once: one hash of the first element's index and both FP32
+ * values gives 32 uniform bits, the top 16 rounding the first element and
+ * the bottom 16 the second (each added below the kept half, as in stu), so
+ * the pair costs one mixer instead of two.  Infinities and NaNs take the
+ * per-element path. */
+template <>
+__device__ __forceinline__ void stu2<__nv_bfloat16>(__nv_bfloat16 *p, float v0, float v1, uint32_t k0, uint32_t k1,
+                                                    int sr) {
+    const uint32_t b0 = __float_as_uint(v0), b1 = __float_as_uint(v1);
+    if (!sr || (b0 & 0x7F800000u) == 0x7F800000u || (b1 & 0x7F800000u) == 0x7F800000u) {
+        __nv_bfloat16 r[2];
+        stu<__nv_bfloat16>(&r[0], v0, k0, sr);
+        stu<__nv_bfloat16>(&r[1], v1, k1, sr);
+        uint32_t w;
+        memcpy(&w, r, sizeof(w));
+        *reinterpret_cast<uint32_t *>(p) = w;
+        return;
+    }
+    const uint32_t h = mix32(b0 ^ ((b1 << 16) | (b1 >> 16)) ^ (k0 * 0x9E3779B9u));
+    const uint32_t w0 = (b0 + (h >> 16)) >> 16, w1 = (b1 + (h & 0xFFFFu)) >> 16;
+    *reinterpret_cast<uint32_t *>(p) = (w0 & 0xFFFFu) | (w1 << 16);
+}
 
 }  // namespace xr
 
